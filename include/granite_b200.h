@@ -1,0 +1,186 @@
+/*
+ * granite_b200.h — C ABI of the B200 trajectory engine (libgranite_b200.so).
+ *
+ * This is the boundary under pygranite's Python surface.  The reference binds its C++
+ * classes directly with pybind11 (source/pygranite.cpp:41-152); it has no C ABI.  Each
+ * entry point below states which reference interface it replaces.  The pybind11 module
+ * pygranite_b200/_pygranite (same class, method and enum names as the reference) is one
+ * caller; ctypes, cgo or JNI callers bind the same symbols.
+ *
+ * Conventions: every call returns GR_OK (0) or a negative status; no call exits the
+ * process or throws.  gr_last_error() returns the message of the last failure on the
+ * calling thread, prefixed like the reference's exceptions ("ERROR < USER INPUT | ..." for
+ * bad input, "ERROR < RUNTIME | ..." for CUDA or internal faults).  Host buffers belong to
+ * the caller and are copied before the call returns; device memory belongs to the engine.
+ * One engine is driven by one host thread at a time.
+ */
+#ifndef GRANITE_B200_H
+#define GRANITE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GR_OK 0
+#define GR_ERR_USER (-1)      /* invalid input; the reference throws MY_USER_ERROR */
+#define GR_ERR_RUNTIME (-2)   /* CUDA or internal failure; the reference calls exit(1) */
+#define GR_ERR_CALLBACK (-3)  /* the loader callback reported a failure */
+
+#define GR_MAX_VOLUMES 8      /* MAX_ADDITIONAL_VOLUMES, source/granite/Constants.hpp:9 */
+#define GR_MAX_EXPRESSIONS 4  /* MAX_ADDITIONAL_COMPUTE, Constants.hpp:10 */
+#define GR_MAX_CONSTANTS 4    /* MAX_CONSTANT_ADDITIONAL_COMPUTE, Constants.hpp:12 */
+
+/* Wind storage type of the device snapshot ring. */
+#define GR_STORE_F32 0
+#define GR_STORE_BF16 1
+#define GR_STORE_F16 2
+
+/* Settings.  Enum fields take the reference's values (IntegratorSettings.hpp:16-76);
+ * float/int fields mirror IntegratorSettings.hpp:83-181.  GridScale/Offset keep the
+ * reference's 1..3-entry lists (grid_scale_len / offset_len). */
+typedef struct gr_settings {
+    int32_t space;                 /* Space: 0 Space3D, 1 Space2D */
+    int32_t integrator;            /* Integrator: 0 ExplicitEuler, 1 ClassicRungeKutta */
+    int32_t windfield_mode;        /* WindfieldMode: 0 Constant, 1 Dynamic */
+    int32_t constants_mode;        /* ConstantsMode: 0 Off, 1 Constant, 2 Dynamic */
+    int32_t volume_mode;           /* AdditionalVolumeMode: 0 Off, 1 Constant, 2 Dynamic */
+    int32_t uplift_mode;           /* UpLiftMode: 0 Off, 1 Constant, 2 Dynamic */
+    int32_t border_mode;           /* BorderMode: 0 Block, 1 LoopX, 2 LoopY, 3 LoopXY */
+    int32_t curvature_mode;        /* CurvatureMode: 0 Off, 1 Total, 2 FastTotal, 3 IndividualAndTotal */
+    int32_t abort_mode;            /* AbortMode: 0 Time, 1 Length, 2 FitLength */
+    int32_t reverse;               /* Reverse */
+    int32_t minimum_alive;         /* MinimumAliveParticles */
+    int32_t grid_scale_len;        /* entries used in grid_scale (1..3) */
+    int32_t offset_len;            /* entries used in offset (1..3) */
+    float sphere_radius;           /* SphereRadius */
+    float delta_t;                 /* DeltaT */
+    float data_time_distance;      /* DataTimeDistance */
+    float maximum_length;          /* MaximumLength */
+    float maximum_simulation_time; /* MaximumSimulationTime */
+    float grid_scale[3];           /* GridScale */
+    float offset[3];               /* Offset */
+    int64_t save_interval;         /* SaveInterval */
+    /* engine options beyond the reference (0 = reference behaviour) */
+    int32_t storage;               /* GR_STORE_*: wind storage in the device ring */
+    int32_t time_mode;             /* 0: time weights from the float32 accumulator the reference
+                                      keeps; 1: from a float64 accumulator */
+    int32_t compensated;           /* 1: Kahan-compensated float32 position update */
+    int32_t ring_slots;            /* device ring depth (>= 3); 0 = 3 */
+    int32_t steps_per_launch;      /* steps fused into one launch; 0 = one snapshot window */
+    int32_t sort_interval;         /* launches between Morton re-sorts / compactions; 0 = off */
+    int32_t block_size;            /* threads per block; 0 = autotuned default */
+    int32_t device;                /* CUDA device ordinal */
+} gr_settings;
+
+/* Fills *s with the reference's IntegratorSettings defaults (IntegratorSettings.hpp:89-181). */
+void gr_settings_default(gr_settings *s);
+
+typedef struct gr_engine gr_engine;
+
+/* Loader callback: called with the snapshot index the run needs next (the reference's
+ * `_loader.step()` followed by updateData, TrajectoryIntegrator.tpp:887-889,
+ * TrajectoryIntegrator.cpp:261-360).  It must push that snapshot's dynamic quantities
+ * with gr_load_* and return 1, return 0 when the loader is exhausted (step() == False),
+ * or a negative value on failure.  Called on the thread that called gr_run. */
+typedef int (*gr_loader_fn)(void *user, gr_engine *engine, int64_t snapshot);
+
+/* Result sizes after gr_run. */
+typedef struct gr_result_info {
+    int64_t n;                   /* particles */
+    int32_t dim;                 /* 2 or 3 */
+    int64_t records;             /* position records incl. the seed record (lengthTrajectories) */
+    int64_t curvature_records;   /* per-step curvature records (IndividualAndTotalCurvature) */
+    int64_t info_records;        /* volume / compute records */
+    int64_t steps;               /* integrator steps run */
+    int64_t windows;             /* snapshot windows run */
+    int64_t particle_steps;      /* alive particles advanced, summed over steps */
+    int32_t n_volumes;
+    int32_t n_expressions;
+} gr_result_info;
+
+/* Timing and traffic counters of the last gr_run. */
+typedef struct gr_stats {
+    double kernel_ms;            /* summed device time of the step launches (CUDA events) */
+    double run_ms;               /* device time from first upload to last result byte */
+    int64_t launches;            /* step-kernel launches */
+    int64_t aux_launches;        /* pack / sort / save kernels */
+    int64_t particle_steps;
+    int64_t h2d_bytes;
+    int64_t d2h_bytes;
+} gr_stats;
+
+/* Create / destroy.  Replaces the TrajectoryIntegrator constructor's resource setup
+ * (TrajectoryIntegrator.hpp:138-147) and destructor (TrajectoryIntegrator.cpp:362-422). */
+int gr_create(const gr_settings *settings, gr_engine **out);
+void gr_destroy(gr_engine *engine);
+
+/* Message of the last failure on this thread ("" if none). */
+const char *gr_last_error(void);
+
+/* Snapshot loads.  Replace loadTexture3D / loadTexture2D (TrajectoryIntegrator.cpp:444-609)
+ * and the constants / uplift uploads (cpp:195-245, 305-359).  `snapshot` is the loader
+ * step the data belongs to (0 = the data present at construction).  Planes are C-order
+ * (z, y, x) for 3D and (y, x) for 2D, float32.  The first wind load fixes the grid. */
+int gr_load_windfield(gr_engine *engine, int64_t snapshot, const float *const *components,
+                      int32_t n_components, int64_t nz, int64_t ny, int64_t nx);
+int gr_load_volume(gr_engine *engine, int64_t snapshot, int32_t index, const float *data,
+                   int64_t nz, int64_t ny, int64_t nx);
+int gr_load_constant(gr_engine *engine, int64_t snapshot, int32_t index, const float *data,
+                     int64_t n);
+int gr_load_uplift(gr_engine *engine, int64_t snapshot, const float *data, int64_t n, int32_t dim);
+/* Topography (IntegratorSettings.Topography; initializeTopography, cpp:635-663). */
+int gr_set_topography(gr_engine *engine, const float *data, int64_t ny, int64_t nx);
+
+/* Compiles one AdditionalCompute expression to device bytecode.  Replaces parse /
+ * replace_environment / contains / flatten (TrajectoryIntegrator.cpp:4-144, 744-798,
+ * TrajectoryIntegrator.tpp:647-712).  volume_names[k] binds to volume index k and
+ * constant_names[k] to constant index k. */
+int gr_compile_expression(gr_engine *engine, int32_t index, const char *code,
+                          const char *const *volume_names, int32_t n_volumes,
+                          const char *const *constant_names, int32_t n_constants);
+
+/* Compiles `code` like gr_compile_expression and evaluates it on the host for one
+ * reference vector ref[19] = {x, y, z, cv, f0..f7, c0..c3, u, v, w}
+ * (TrajectoryIntegrator.tpp:381-439).  Needs no GPU; returns GR_ERR_USER with the
+ * reference's message for an invalid expression. */
+int gr_expression_evaluate(const char *code, const char *const *volume_names, int32_t n_volumes,
+                           const char *const *constant_names, int32_t n_constants, int32_t dim,
+                           int32_t curvature_mode, const float *ref, float *out);
+
+/* Seeds (the last record of the TrajectorySet handed to the constructor,
+ * TrajectoryIntegrator::initSet, cpp:424-442). */
+int gr_set_seeds(gr_engine *engine, const float *positions, int64_t n, int32_t dim);
+
+/* Runs the whole simulation.  Replaces compute() (cpp:687-693) with compute_ /
+ * computeLoop_ / computeLoopGPU_ (TrajectoryIntegrator.tpp:467-995). */
+int gr_run(gr_engine *engine, gr_loader_fn loader, void *user);
+
+int gr_result_info_get(gr_engine *engine, gr_result_info *out);
+int gr_stats_get(gr_engine *engine, gr_stats *out);
+
+/* Results, copied into caller buffers.  Shapes follow the reference's accessors
+ * (TrajectorySet.cpp:90-253): positions (n, records, dim); status (n); lengths (n);
+ * total curvature (n); curvatures (n, curvature_records); volume / compute info
+ * (n, info_records). */
+int gr_fetch_positions(gr_engine *engine, float *out, int64_t capacity_floats);
+int gr_fetch_status(gr_engine *engine, int32_t *out, int64_t capacity);
+int gr_fetch_lengths(gr_engine *engine, float *out, int64_t capacity);
+int gr_fetch_total_curvature(gr_engine *engine, float *out, int64_t capacity);
+int gr_fetch_curvatures(gr_engine *engine, float *out, int64_t capacity_floats);
+int gr_fetch_volume_info(gr_engine *engine, int32_t index, float *out, int64_t capacity_floats);
+int gr_fetch_compute_info(gr_engine *engine, int32_t index, float *out, int64_t capacity_floats);
+
+/* Device-resident variants for callers that keep data on the GPU: the same loads and
+ * seeds from device pointers (no host copy). */
+int gr_load_windfield_device(gr_engine *engine, int64_t snapshot, const float *const *components,
+                             int32_t n_components, int64_t nz, int64_t ny, int64_t nx);
+int gr_set_seeds_device(gr_engine *engine, const float *positions, int64_t n, int32_t dim);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

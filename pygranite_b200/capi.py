@@ -1,0 +1,276 @@
+"""ctypes view of the C ABI in include/granite_b200.h (libgranite_b200.so).
+
+The pybind11 module is the pygranite-compatible surface; this module is for callers that
+bind the C ABI directly (the benchmark's device-resident path, ABI tests).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgranite_b200.so")
+
+GR_OK, GR_ERR_USER, GR_ERR_RUNTIME, GR_ERR_CALLBACK = 0, -1, -2, -3
+
+# Every entry point declared in include/granite_b200.h.
+EXPORTS = [
+    "gr_settings_default", "gr_create", "gr_destroy", "gr_last_error", "gr_load_windfield",
+    "gr_load_volume", "gr_load_constant", "gr_load_uplift", "gr_set_topography",
+    "gr_compile_expression", "gr_expression_evaluate", "gr_set_seeds", "gr_run",
+    "gr_result_info_get", "gr_stats_get", "gr_fetch_positions", "gr_fetch_status",
+    "gr_fetch_lengths", "gr_fetch_total_curvature", "gr_fetch_curvatures",
+    "gr_fetch_volume_info", "gr_fetch_compute_info", "gr_load_windfield_device",
+    "gr_set_seeds_device",
+]
+
+
+class Settings(ctypes.Structure):
+    _fields_ = [
+        ("space", ctypes.c_int32), ("integrator", ctypes.c_int32), ("windfield_mode", ctypes.c_int32),
+        ("constants_mode", ctypes.c_int32), ("volume_mode", ctypes.c_int32), ("uplift_mode", ctypes.c_int32),
+        ("border_mode", ctypes.c_int32), ("curvature_mode", ctypes.c_int32), ("abort_mode", ctypes.c_int32),
+        ("reverse", ctypes.c_int32), ("minimum_alive", ctypes.c_int32), ("grid_scale_len", ctypes.c_int32),
+        ("offset_len", ctypes.c_int32), ("sphere_radius", ctypes.c_float), ("delta_t", ctypes.c_float),
+        ("data_time_distance", ctypes.c_float), ("maximum_length", ctypes.c_float),
+        ("maximum_simulation_time", ctypes.c_float), ("grid_scale", ctypes.c_float * 3),
+        ("offset", ctypes.c_float * 3), ("save_interval", ctypes.c_int64), ("storage", ctypes.c_int32),
+        ("time_mode", ctypes.c_int32), ("compensated", ctypes.c_int32), ("ring_slots", ctypes.c_int32),
+        ("steps_per_launch", ctypes.c_int32), ("sort_interval", ctypes.c_int32), ("block_size", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+    ]
+
+
+class ResultInfo(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("dim", ctypes.c_int32), ("records", ctypes.c_int64),
+                ("curvature_records", ctypes.c_int64), ("info_records", ctypes.c_int64),
+                ("steps", ctypes.c_int64), ("windows", ctypes.c_int64), ("particle_steps", ctypes.c_int64),
+                ("n_volumes", ctypes.c_int32), ("n_expressions", ctypes.c_int32)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("kernel_ms", ctypes.c_double), ("run_ms", ctypes.c_double), ("launches", ctypes.c_int64),
+                ("aux_launches", ctypes.c_int64), ("particle_steps", ctypes.c_int64),
+                ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64)]
+
+
+LOADER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64)
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing; build with `make -C pygranite_b200/csrc`")
+        L = ctypes.CDLL(LIB_PATH)
+        P, I32, I64, FP = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.POINTER(ctypes.c_float)
+        CP = ctypes.POINTER(ctypes.c_char_p)
+        sig = {
+            "gr_settings_default": (None, [ctypes.POINTER(Settings)]),
+            "gr_create": (ctypes.c_int, [ctypes.POINTER(Settings), ctypes.POINTER(P)]),
+            "gr_destroy": (None, [P]),
+            "gr_last_error": (ctypes.c_char_p, []),
+            "gr_load_windfield": (ctypes.c_int, [P, I64, ctypes.POINTER(FP), I32, I64, I64, I64]),
+            "gr_load_windfield_device": (ctypes.c_int, [P, I64, ctypes.POINTER(P), I32, I64, I64, I64]),
+            "gr_load_volume": (ctypes.c_int, [P, I64, I32, FP, I64, I64, I64]),
+            "gr_load_constant": (ctypes.c_int, [P, I64, I32, FP, I64]),
+            "gr_load_uplift": (ctypes.c_int, [P, I64, FP, I64, I32]),
+            "gr_set_topography": (ctypes.c_int, [P, FP, I64, I64]),
+            "gr_compile_expression": (ctypes.c_int, [P, I32, ctypes.c_char_p, CP, I32, CP, I32]),
+            "gr_expression_evaluate": (ctypes.c_int, [ctypes.c_char_p, CP, I32, CP, I32, I32, I32, FP, FP]),
+            "gr_set_seeds": (ctypes.c_int, [P, FP, I64, I32]),
+            "gr_set_seeds_device": (ctypes.c_int, [P, P, I64, I32]),
+            "gr_run": (ctypes.c_int, [P, LOADER_FN, P]),
+            "gr_result_info_get": (ctypes.c_int, [P, ctypes.POINTER(ResultInfo)]),
+            "gr_stats_get": (ctypes.c_int, [P, ctypes.POINTER(Stats)]),
+            "gr_fetch_positions": (ctypes.c_int, [P, FP, I64]),
+            "gr_fetch_status": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_int32), I64]),
+            "gr_fetch_lengths": (ctypes.c_int, [P, FP, I64]),
+            "gr_fetch_total_curvature": (ctypes.c_int, [P, FP, I64]),
+            "gr_fetch_curvatures": (ctypes.c_int, [P, FP, I64]),
+            "gr_fetch_volume_info": (ctypes.c_int, [P, I32, FP, I64]),
+            "gr_fetch_compute_info": (ctypes.c_int, [P, I32, FP, I64]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class GraniteError(RuntimeError):
+    pass
+
+
+def _check(rc):
+    if rc != GR_OK:
+        raise GraniteError(lib().gr_last_error().decode())
+
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def _names(names):
+    arr = (ctypes.c_char_p * max(1, len(names)))(*[n.encode() for n in names])
+    return ctypes.cast(arr, ctypes.POINTER(ctypes.c_char_p)), arr
+
+
+def default_settings(**kw) -> Settings:
+    s = Settings()
+    lib().gr_settings_default(ctypes.byref(s))
+    for k, v in kw.items():
+        if k in ("grid_scale", "offset"):
+            arr = getattr(s, k)
+            for i, x in enumerate(v):
+                arr[i] = x
+            setattr(s, k + "_len", len(v))
+        else:
+            setattr(s, k, v)
+    return s
+
+
+def settings_from_reference(d: dict, **extra) -> Settings:
+    """gr_settings from a dict of reference IntegratorSettings field names (int enums)."""
+    m = dict(space=d.get("Space", 0), integrator=d.get("Integrator", 1), windfield_mode=d.get("WindfieldMode", 1),
+             constants_mode=d.get("ConstantsMode", 0), volume_mode=d.get("AdditionalVolumeMode", 0),
+             uplift_mode=d.get("UpLiftMode", 0), border_mode=d.get("BorderMode", 0),
+             curvature_mode=d.get("CurvatureMode", 0), abort_mode=d.get("AbortMode", 0),
+             reverse=int(bool(d.get("Reverse", False))), minimum_alive=d.get("MinimumAliveParticles", 0),
+             sphere_radius=d.get("SphereRadius", 0.0), delta_t=d.get("DeltaT", 1.0),
+             data_time_distance=d.get("DataTimeDistance", 60.0), maximum_length=d.get("MaximumLength", 0.0),
+             maximum_simulation_time=d.get("MaximumSimulationTime", 100.0),
+             grid_scale=d.get("GridScale", [25.0, 25.0, 25.0]), offset=d.get("Offset", [0.0, 0.0, 0.0]),
+             save_interval=d.get("SaveInterval", 1))
+    m.update(extra)
+    return default_settings(**m)
+
+
+def evaluate_expression(code, ref, volume_names=(), constant_names=(), dim=3, curvature_mode=0):
+    """Host evaluation through gr_expression_evaluate (no GPU needed)."""
+    vn, _k1 = _names(list(volume_names))
+    cn, _k2 = _names(list(constant_names))
+    r = np.ascontiguousarray(ref, np.float32)
+    out = ctypes.c_float(0.0)
+    _check(lib().gr_expression_evaluate(code.encode(), vn, len(volume_names), cn, len(constant_names), dim,
+                                        curvature_mode, _fp(r), ctypes.byref(out)))
+    return out.value
+
+
+class Engine:
+    """Thin owner of a gr_engine*."""
+
+    def __init__(self, settings: Settings):
+        self.h = ctypes.c_void_p()
+        _check(lib().gr_create(ctypes.byref(settings), ctypes.byref(self.h)))
+        self.dim = 3 if settings.space == 0 else 2
+        self._keep = []
+
+    def close(self):
+        if self.h:
+            lib().gr_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_windfield(self, snapshot, planes):
+        planes = [np.ascontiguousarray(p, np.float32) for p in planes]
+        arr = (ctypes.POINTER(ctypes.c_float) * len(planes))(*[_fp(p) for p in planes])
+        shp = planes[0].shape
+        nz, ny, nx = (shp if len(shp) == 3 else (1,) + tuple(shp))
+        _check(lib().gr_load_windfield(self.h, snapshot, arr, len(planes), nz, ny, nx))
+
+    def load_windfield_device(self, snapshot, ptrs, shape):
+        arr = (ctypes.c_void_p * len(ptrs))(*ptrs)
+        nz, ny, nx = (shape if len(shape) == 3 else (1,) + tuple(shape))
+        _check(lib().gr_load_windfield_device(self.h, snapshot, arr, len(ptrs), nz, ny, nx))
+
+    def load_volume(self, snapshot, index, plane):
+        p = np.ascontiguousarray(plane, np.float32)
+        shp = p.shape
+        nz, ny, nx = (shp if len(shp) == 3 else (1,) + tuple(shp))
+        _check(lib().gr_load_volume(self.h, snapshot, index, _fp(p), nz, ny, nx))
+
+    def load_constant(self, snapshot, index, values):
+        v = np.ascontiguousarray(values, np.float32)
+        _check(lib().gr_load_constant(self.h, snapshot, index, _fp(v), v.size))
+
+    def load_uplift(self, snapshot, values):
+        v = np.ascontiguousarray(values, np.float32)
+        _check(lib().gr_load_uplift(self.h, snapshot, _fp(v), v.shape[0], v.shape[1]))
+
+    def set_topography(self, topo):
+        t = np.ascontiguousarray(topo, np.float32)
+        _check(lib().gr_set_topography(self.h, _fp(t), t.shape[0], t.shape[1]))
+
+    def compile_expression(self, index, code, volume_names=(), constant_names=()):
+        vn, k1 = _names(list(volume_names))
+        cn, k2 = _names(list(constant_names))
+        _check(lib().gr_compile_expression(self.h, index, code.encode(), vn, len(volume_names), cn,
+                                           len(constant_names)))
+
+    def set_seeds(self, seeds):
+        s = np.ascontiguousarray(seeds, np.float32)
+        _check(lib().gr_set_seeds(self.h, _fp(s), s.shape[0], s.shape[1]))
+
+    def run(self, loader=None):
+        """loader(snapshot) -> 1 / 0 / negative; None = the ring already holds every snapshot."""
+        def cb(user, eng, snapshot):
+            try:
+                return int(loader(snapshot)) if loader is not None else 0
+            except Exception:  # the error is reported through the status code
+                return -1
+        fn = LOADER_FN(cb)
+        self._keep.append(fn)
+        _check(lib().gr_run(self.h, fn, None))
+
+    def info(self) -> ResultInfo:
+        r = ResultInfo()
+        _check(lib().gr_result_info_get(self.h, ctypes.byref(r)))
+        return r
+
+    def stats(self) -> Stats:
+        s = Stats()
+        _check(lib().gr_stats_get(self.h, ctypes.byref(s)))
+        return s
+
+    def results(self, volumes=True, compute=True):
+        info = self.info()
+        n, L, D = info.n, info.records, info.dim
+        pos = np.empty((n, L, D), np.float32)
+        _check(lib().gr_fetch_positions(self.h, _fp(pos), pos.size))
+        st = np.empty(n, np.int32)
+        _check(lib().gr_fetch_status(self.h, st.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), n))
+        out = dict(trajectories=pos, status=st, info=info)
+        ln = np.zeros(n, np.float32)
+        _check(lib().gr_fetch_lengths(self.h, _fp(ln), n))
+        tc = np.zeros(n, np.float32)
+        _check(lib().gr_fetch_total_curvature(self.h, _fp(tc), n))
+        cv = np.zeros((n, info.curvature_records), np.float32)
+        if info.curvature_records:
+            _check(lib().gr_fetch_curvatures(self.h, _fp(cv), cv.size))
+        out.update(lengths=ln, total_curvature=tc, curvatures=cv)
+        if volumes:
+            vols = []
+            for k in range(info.n_volumes):
+                a = np.empty((n, info.info_records), np.float32)
+                _check(lib().gr_fetch_volume_info(self.h, k, _fp(a), a.size))
+                vols.append(a)
+            out["volume_info"] = vols
+        if compute:
+            cmps = []
+            for k in range(info.n_expressions):
+                a = np.empty((n, info.info_records), np.float32)
+                _check(lib().gr_fetch_compute_info(self.h, k, _fp(a), a.size))
+                cmps.append(a)
+            out["compute_info"] = cmps
+        return out

@@ -1,0 +1,1054 @@
+// engine.cu — host engine and C ABI of libgranite_b200.so (declarations: include/granite_b200.h).
+//
+// Replaces the reference's TrajectoryIntegrator host driver (source/granite/
+// TrajectoryIntegrator.tpp:467-1049, TrajectoryIntegrator.cpp:146-693):
+//  * snapshot store: a device ring of `ring_slots` snapshots per quantity (reference: a
+//    3-slot ring of cudaArray textures filled by synchronous cudaMemcpy3D).  Host data is
+//    copied into pinned staging, moved by cudaMemcpyAsync on a copy stream and packed
+//    node-major by a kernel; events order the copies against the step launches, so the
+//    loader callback and the uploads for the next window overlap the current window.
+//  * step loop: one launch advances all particles through one or more windows (the
+//    reference launches once per step, synchronises, and copies every saved step to the
+//    host); records go to a device history in the (particle, record, component) layout the
+//    Python accessors return.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/granite_b200.h"
+#include "expr.h"
+#include "granite_kernels.cuh"
+#include "schedule.h"
+
+using namespace granite_b200;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define USER_ERR(...) fail(GR_ERR_USER, "ERROR < USER INPUT | " __VA_ARGS__)
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t err_ = (call);                                                                 \
+        if (err_ != cudaSuccess)                                                                   \
+            return fail(GR_ERR_RUNTIME, "ERROR < RUNTIME | CUDA error | %s : %s, line %d >",       \
+                        cudaGetErrorString(err_), __FILE__, __LINE__);                             \
+    } while (0)
+
+// ------------------------------------------------------------------ aux kernels
+
+// Planes (ncomp x nodes, float32) -> node-major packed snapshot of storage type W.
+template <typename W>
+__global__ void pack_wind_kernel(const float *__restrict__ u, const float *__restrict__ v,
+                                 const float *__restrict__ w, void *out, int64_t nodes, int dim);
+
+template <>
+__global__ void pack_wind_kernel<float>(const float *__restrict__ u, const float *__restrict__ v,
+                                        const float *__restrict__ w, void *out, int64_t nodes, int dim) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        if (dim == 3) reinterpret_cast<float4 *>(out)[i] = make_float4(u[i], v[i], w[i], 0.f);
+        else reinterpret_cast<float2 *>(out)[i] = make_float2(u[i], v[i]);
+    }
+}
+
+template <>
+__global__ void pack_wind_kernel<__nv_bfloat16>(const float *__restrict__ u, const float *__restrict__ v,
+                                                const float *__restrict__ w, void *out, int64_t nodes, int dim) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        const __nv_bfloat162 a = __floats2bfloat162_rn(u[i], v[i]);
+        if (dim == 3) {
+            const __nv_bfloat162 b = __floats2bfloat162_rn(w[i], 0.f);
+            uint2 q;
+            q.x = *reinterpret_cast<const unsigned *>(&a);
+            q.y = *reinterpret_cast<const unsigned *>(&b);
+            reinterpret_cast<uint2 *>(out)[i] = q;
+        } else {
+            reinterpret_cast<unsigned *>(out)[i] = *reinterpret_cast<const unsigned *>(&a);
+        }
+    }
+}
+
+template <>
+__global__ void pack_wind_kernel<__half>(const float *__restrict__ u, const float *__restrict__ v,
+                                         const float *__restrict__ w, void *out, int64_t nodes, int dim) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        const __half2 a = __floats2half2_rn(u[i], v[i]);
+        if (dim == 3) {
+            const __half2 b = __floats2half2_rn(w[i], 0.f);
+            uint2 q;
+            q.x = *reinterpret_cast<const unsigned *>(&a);
+            q.y = *reinterpret_cast<const unsigned *>(&b);
+            reinterpret_cast<uint2 *>(out)[i] = q;
+        } else {
+            reinterpret_cast<unsigned *>(out)[i] = *reinterpret_cast<const unsigned *>(&a);
+        }
+    }
+}
+
+// Seeds (AoS, n x dim) -> state SoA; zeroes the per-particle accumulators.
+__global__ void seed_kernel(const float *__restrict__ seeds, int64_t n, int dim, float *px, float *py,
+                            float *pz, int32_t *status, int32_t *id) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        px[i] = seeds[i * dim];
+        py[i] = seeds[i * dim + 1];
+        if (dim == 3) pz[i] = seeds[i * dim + 2];
+        status[i] = 0;
+        id[i] = (int32_t)i;
+    }
+}
+
+// Record 0 of the history = the seeds (TrajectoryIntegrator.cpp:424-442).
+__global__ void seed_record_kernel(const float *__restrict__ seeds, int64_t n, int dim, float *hpos, int64_t L) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        for (int d = 0; d < dim; ++d) hpos[i * L * dim + d] = seeds[i * dim + d];
+}
+
+// Writes one record from the state (the SaveInterval == 0 final record, tpp:914-915).
+template <int DIM>
+__global__ void save_state_kernel(const __grid_constant__ KParams P, int32_t rec, int32_t crec, int32_t irec,
+                                  int write_curv) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pid = P.id[i];
+        float *hp = P.hpos + (pid * P.L + rec) * DIM;
+        hp[0] = P.px[i];
+        hp[1] = P.py[i];
+        if (DIM == 3) hp[2] = P.pz[i];
+        if (P.curvature_mode == 3 && write_curv) P.hcurv[pid * P.Lc + crec] = P.curv[i];
+        if (P.volume_mode != 0)
+            for (int k = 0; k < P.nvol; ++k) P.hvol[((int64_t)k * P.n_total + pid) * P.Li + irec] = P.volc[k * P.n_state + i];
+        for (int e = 0; e < P.nexpr; ++e) P.hcmp[((int64_t)e * P.n_total + pid) * P.Li + irec] = P.cmpc[e * P.n_state + i];
+    }
+}
+
+// State (slot order) -> final per-particle outputs (particle order).
+__global__ void finalize_kernel(const __grid_constant__ KParams P, int32_t *status_out, float *length_out,
+                                float *tc_out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pid = P.id[i];
+        status_out[pid] = P.status[i];
+        if (P.abort_mode != 0) length_out[pid] = P.length[i];
+        if (P.curvature_mode != 0) tc_out[pid] = P.tc[i];
+    }
+}
+
+int grid_for(int64_t n, int threads) {
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > 148 * 64) b = 148 * 64;
+    return (int)b;
+}
+
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t count = 0;
+    ~DevBuf() { reset(); }
+    void reset() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        count = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        if (n <= count && p) return cudaSuccess;
+        reset();
+        if (n == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+        if (e == cudaSuccess) count = n;
+        else p = nullptr;
+        return e;
+    }
+};
+
+struct PinnedBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    cudaEvent_t done = nullptr;
+    ~PinnedBuf() {
+        if (p) cudaFreeHost(p);
+        if (done) cudaEventDestroy(done);
+    }
+};
+
+}  // namespace
+
+struct gr_engine {
+    gr_settings s{};
+    int dim = 3;
+    bool dyn_any = false, wind_dynamic = false;
+    cudaStream_t cs = nullptr, xs = nullptr;
+    int K = 3;
+
+    // geometry
+    bool grid_set = false;
+    int64_t nx = 0, ny = 0, nz = 1, nodes = 0;
+    float scale[3]{}, off[3]{}, dom[3]{}, inv_scale[3]{};
+
+    // rings
+    DevBuf<char> wind;
+    int64_t wind_stride = 0;
+    DevBuf<float> vol, cons, lift, topo;
+    int nvol = 0, ncon = 0;
+    bool has_topo = false, has_uplift = false;
+    std::vector<int64_t> wind_holds, vol_holds, cons_holds, lift_holds;
+    std::vector<cudaEvent_t> slot_free, slot_ready;
+    std::vector<bool> slot_used;
+    DevBuf<float> raw;                 // device staging of one snapshot's planes
+    PinnedBuf pin[2];
+    int pin_next = 0;
+
+    // expressions
+    Program progs[GR_MAX_EXPR]{};
+    int nexpr = 0;
+    DevBuf<Program> d_prog;
+
+    // particles
+    int64_t n = 0;
+    DevBuf<float> seeds;               // AoS n x dim
+    DevBuf<float> px, py, pz, qx, qy, qz, kx, ky, kz, lx, ly, lz, length, tc, curv, volc, cmpc;
+    DevBuf<int32_t> status, id;
+    DevBuf<float> hpos, hcurv, hvol, hcmp;
+    DevBuf<int32_t> out_status;
+    DevBuf<float> out_length, out_tc;
+    DevBuf<unsigned long long> counters;
+    unsigned long long *h_counters = nullptr;   // pinned
+    DevBuf<StepEntry> d_sched;
+    std::vector<StepEntry> h_sched;
+    int64_t L = 0, Lc = 0, Li = 0;
+
+    // results
+    bool have_result = false;
+    gr_result_info info{};
+    gr_stats stats{};
+    std::vector<cudaEvent_t> ev_pool;
+
+    ~gr_engine() {
+        if (cs) cudaStreamSynchronize(cs);
+        if (xs) cudaStreamSynchronize(xs);
+        for (auto e : slot_free) cudaEventDestroy(e);
+        for (auto e : slot_ready) cudaEventDestroy(e);
+        for (auto e : ev_pool) cudaEventDestroy(e);
+        if (h_counters) cudaFreeHost(h_counters);
+        if (cs) cudaStreamDestroy(cs);
+        if (xs) cudaStreamDestroy(xs);
+    }
+};
+
+namespace {
+
+int set_device(gr_engine *e) {
+    CK(cudaSetDevice(e->s.device));
+    return GR_OK;
+}
+
+int ensure_pinned(gr_engine *e, size_t bytes, PinnedBuf *&out) {
+    PinnedBuf &b = e->pin[e->pin_next];
+    e->pin_next ^= 1;
+    if (b.done) CK(cudaEventSynchronize(b.done));
+    if (b.bytes < bytes) {
+        if (b.p) CK(cudaFreeHost(b.p));
+        b.p = nullptr;
+        CK(cudaMallocHost(&b.p, bytes));
+        b.bytes = bytes;
+    }
+    if (!b.done) CK(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
+    out = &b;
+    return GR_OK;
+}
+
+int setup_grid(gr_engine *e, int64_t nz, int64_t ny, int64_t nx) {
+    if (nx < 1 || ny < 1 || nz < 1) return USER_ERR("Invalid dataset was provided. Empty grid. >");
+    if (nx > (1 << 30) || ny > (1 << 30) || nz > (1 << 30) || nx * ny * nz > (int64_t(1) << 40))
+        return USER_ERR("Invalid dataset was provided. Grid too large. >");
+    e->nx = nx; e->ny = ny; e->nz = e->dim == 3 ? nz : 1;
+    e->nodes = e->nx * e->ny * e->nz;
+    const gr_settings &s = e->s;
+    // GridScale / Offset / Domain (TrajectoryIntegrator.tpp:521-574)
+    const float *gs = s.grid_scale, *of = s.offset;
+    if (s.grid_scale_len == 1) { e->scale[0] = e->scale[1] = e->scale[2] = gs[0]; }
+    else if (s.grid_scale_len == 2) { e->scale[0] = gs[0]; e->scale[1] = gs[1]; e->scale[2] = gs[0]; }
+    else if (s.grid_scale_len == 3) { e->scale[0] = gs[0]; e->scale[1] = gs[1]; e->scale[2] = gs[2]; }
+    else return USER_ERR("Invalid GridScale dimension. >");
+    if (s.offset_len == 1) { e->off[0] = e->off[1] = e->off[2] = of[0]; }
+    else if (s.grid_scale_len == 2 && s.offset_len >= 2) { e->off[0] = of[0]; e->off[1] = of[1]; e->off[2] = of[0]; }
+    else if (s.grid_scale_len == 3 && s.offset_len >= 3) { e->off[0] = of[0]; e->off[1] = of[1]; e->off[2] = of[2]; }
+    else return USER_ERR("Invalid Offset dimension. >");
+    const float g[3] = {(float)e->nx, (float)e->ny, (float)(e->dim == 3 ? nz : 0)};
+    for (int d = 0; d < 3; ++d) {
+        e->dom[d] = g[d] * e->scale[d];
+        e->inv_scale[d] = 1.0f / e->scale[d];
+    }
+    const int bytes_node = e->s.storage == GR_STORE_F32 ? (e->dim == 3 ? 16 : 8) : (e->dim == 3 ? 8 : 4);
+    e->wind_stride = ((e->nodes * bytes_node + 255) / 256) * 256;
+    CK(e->wind.alloc((size_t)e->wind_stride * e->K));
+    CK(e->raw.alloc((size_t)e->nodes * e->dim));
+    e->grid_set = true;
+    return GR_OK;
+}
+
+int wait_slot_free(gr_engine *e, int slot) {
+    if (e->slot_used[slot]) CK(cudaStreamWaitEvent(e->xs, e->slot_free[slot], 0));
+    return GR_OK;
+}
+
+int pack_launch(gr_engine *e, const float *u, const float *v, const float *w, int slot) {
+    void *dst = e->wind.p + (int64_t)slot * e->wind_stride;
+    const int threads = 256;
+    const int blocks = grid_for(e->nodes, threads);
+    switch (e->s.storage) {
+        case GR_STORE_BF16: pack_wind_kernel<__nv_bfloat16><<<blocks, threads, 0, e->xs>>>(u, v, w, dst, e->nodes, e->dim); break;
+        case GR_STORE_F16: pack_wind_kernel<__half><<<blocks, threads, 0, e->xs>>>(u, v, w, dst, e->nodes, e->dim); break;
+        default: pack_wind_kernel<float><<<blocks, threads, 0, e->xs>>>(u, v, w, dst, e->nodes, e->dim); break;
+    }
+    CK(cudaGetLastError());
+    e->stats.aux_launches++;
+    return GR_OK;
+}
+
+int check_shape(gr_engine *e, int64_t nz, int64_t ny, int64_t nx) {
+    if (e->dim == 3) {
+        if (nz != e->nz) return USER_ERR("Invalid dataset was provided. Shape does not match in z dimension (3D). >");
+        if (ny != e->ny) return USER_ERR("Invalid dataset was provided. Shape does not match in y dimension (3D). >");
+        if (nx != e->nx) return USER_ERR("Invalid dataset was provided. Shape does not match in x dimension (3D). >");
+    } else {
+        if (ny != e->ny) return USER_ERR("Invalid dataset was provided. Shape does not match in y dimension (2D). >");
+        if (nx != e->nx) return USER_ERR("Invalid dataset was provided. Shape does not match in x dimension (2D). >");
+    }
+    return GR_OK;
+}
+
+int load_wind(gr_engine *e, int64_t snapshot, const float *const *comps, int32_t ncomp, int64_t nz, int64_t ny,
+              int64_t nx, bool device_src) {
+    if (!e) return USER_ERR("null engine >");
+    if (snapshot < 0) return USER_ERR("negative snapshot index >");
+    if (ncomp != e->dim)
+        return fail(GR_ERR_USER, "%s", e->dim == 3
+                        ? "ERROR < USER INPUT | Invalid dataset was provided. Wrong amout of data (3D). >"
+                        : "ERROR < USER INPUT | Invalid dataset was provided. Wrong amout of data (2D). >");
+    for (int c = 0; c < ncomp; ++c)
+        if (!comps || !comps[c]) return USER_ERR("null windfield component >");
+    if (e->dim == 2) nz = 1;
+    int rc = set_device(e);
+    if (rc) return rc;
+    if (!e->grid_set) {
+        rc = setup_grid(e, nz, ny, nx);
+        if (rc) return rc;
+    } else {
+        rc = check_shape(e, nz, ny, nx);
+        if (rc) return rc;
+    }
+    const int slot = (int)(snapshot % e->K);
+    rc = wait_slot_free(e, slot);
+    if (rc) return rc;
+    const size_t plane = (size_t)e->nodes;
+    float *raw[3] = {e->raw.p, e->raw.p + plane, e->raw.p + 2 * plane};
+    if (device_src) {
+        for (int c = 0; c < ncomp; ++c) raw[c] = const_cast<float *>(comps[c]);
+    } else {
+        PinnedBuf *pb = nullptr;
+        rc = ensure_pinned(e, plane * ncomp * sizeof(float), pb);
+        if (rc) return rc;
+        for (int c = 0; c < ncomp; ++c)
+            std::memcpy(static_cast<float *>(pb->p) + c * plane, comps[c], plane * sizeof(float));
+        CK(cudaMemcpyAsync(e->raw.p, pb->p, plane * ncomp * sizeof(float), cudaMemcpyHostToDevice, e->xs));
+        CK(cudaEventRecord(pb->done, e->xs));
+        e->stats.h2d_bytes += (int64_t)(plane * ncomp * sizeof(float));
+    }
+    rc = pack_launch(e, raw[0], raw[1], e->dim == 3 ? raw[2] : raw[1], slot);
+    if (rc) return rc;
+    CK(cudaEventRecord(e->slot_ready[slot], e->xs));
+    if (device_src) CK(cudaStreamSynchronize(e->xs));
+    e->wind_holds[slot] = snapshot;
+    return GR_OK;
+}
+
+int ensure_particles(gr_engine *e) {
+    if (e->n <= 0) return USER_ERR("Provided TrajectorySet does not contain any data. >");
+    return GR_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+
+extern "C" {
+
+void gr_settings_default(gr_settings *s) {
+    std::memset(s, 0, sizeof *s);
+    s->space = 0;
+    s->integrator = 1;
+    s->windfield_mode = 1;
+    s->delta_t = 1.f;
+    s->data_time_distance = 60.f;
+    s->grid_scale[0] = s->grid_scale[1] = s->grid_scale[2] = 25.f;
+    s->grid_scale_len = 3;
+    s->offset_len = 3;
+    s->save_interval = 1;
+    s->maximum_simulation_time = 100.f;
+}
+
+const char *gr_last_error(void) { return g_last_error.c_str(); }
+
+int gr_create(const gr_settings *settings, gr_engine **out) {
+    g_last_error.clear();
+    if (!settings || !out) return USER_ERR("null argument >");
+    *out = nullptr;
+    const gr_settings &s = *settings;
+    if (s.space != 0 && s.space != 1) return USER_ERR("Invalid Space. >");
+    if (s.delta_t <= 0.f || !std::isfinite(s.delta_t)) return USER_ERR("DeltaT must be positive. >");
+    if (s.data_time_distance <= 0.f || !std::isfinite(s.data_time_distance))
+        return USER_ERR("DataTimeDistance must be positive. >");
+    if (!std::isfinite(s.maximum_simulation_time)) return USER_ERR("MaximumSimulationTime must be finite. >");
+    if (s.maximum_simulation_time / s.delta_t > 5.0e8f) return USER_ERR("Too many integration steps requested. >");
+    if (s.save_interval < 0) return USER_ERR("SaveInterval must not be negative. >");
+    if (s.storage < 0 || s.storage > 2) return USER_ERR("Invalid storage type. >");
+    auto e = std::make_unique<gr_engine>();
+    e->s = s;
+    e->dim = s.space == 0 ? 3 : 2;
+    if (e->dim == 2) e->s.uplift_mode = 0;   // 2D variants force uplift Off (TrajectoryIntegratorMacros.hpp:67)
+    e->wind_dynamic = s.windfield_mode == 1;
+    e->dyn_any = e->wind_dynamic || e->s.uplift_mode == 2 || s.volume_mode == 2 || s.constants_mode == 2;
+    e->K = s.ring_slots >= 3 ? s.ring_slots : 3;
+    if (e->K > 100000) return USER_ERR("ring_slots too large >");
+    CK(cudaSetDevice(s.device));
+    CK(cudaStreamCreateWithFlags(&e->cs, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&e->xs, cudaStreamNonBlocking));
+    e->slot_free.resize(e->K);
+    e->slot_ready.resize(e->K);
+    e->slot_used.assign(e->K, false);
+    for (int k = 0; k < e->K; ++k) {
+        CK(cudaEventCreateWithFlags(&e->slot_free[k], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&e->slot_ready[k], cudaEventDisableTiming));
+    }
+    e->wind_holds.assign(e->K, -1);
+    e->vol_holds.assign(e->K, -1);
+    e->cons_holds.assign(e->K, -1);
+    e->lift_holds.assign(e->K, -1);
+    CK(e->counters.alloc(4));
+    CK(cudaMallocHost(&e->h_counters, 4 * sizeof(unsigned long long)));
+    *out = e.release();
+    return GR_OK;
+}
+
+void gr_destroy(gr_engine *engine) { delete engine; }
+
+int gr_load_windfield(gr_engine *e, int64_t snapshot, const float *const *comps, int32_t ncomp, int64_t nz,
+                      int64_t ny, int64_t nx) {
+    return load_wind(e, snapshot, comps, ncomp, nz, ny, nx, false);
+}
+
+int gr_load_windfield_device(gr_engine *e, int64_t snapshot, const float *const *comps, int32_t ncomp, int64_t nz,
+                             int64_t ny, int64_t nx) {
+    return load_wind(e, snapshot, comps, ncomp, nz, ny, nx, true);
+}
+
+int gr_load_volume(gr_engine *e, int64_t snapshot, int32_t index, const float *data, int64_t nz, int64_t ny,
+                   int64_t nx) {
+    if (!e || !data) return USER_ERR("null argument >");
+    if (index < 0 || index >= GR_MAX_VOLUMES) return USER_ERR("You provided more additional volumes than supported. >");
+    if (!e->grid_set) return USER_ERR("The windfield must be loaded before additional volumes. >");
+    if (e->dim == 2) nz = 1;
+    int rc = check_shape(e, nz, ny, nx);
+    if (rc) return rc;
+    rc = set_device(e);
+    if (rc) return rc;
+    CK(e->vol.alloc((size_t)e->nodes * GR_MAX_VOLUMES * e->K));
+    const int slot = (int)(snapshot % e->K);
+    rc = wait_slot_free(e, slot);
+    if (rc) return rc;
+    PinnedBuf *pb = nullptr;
+    const size_t bytes = (size_t)e->nodes * sizeof(float);
+    rc = ensure_pinned(e, bytes, pb);
+    if (rc) return rc;
+    std::memcpy(pb->p, data, bytes);
+    float *dst = e->vol.p + ((int64_t)slot * GR_MAX_VOLUMES + index) * e->nodes;
+    CK(cudaMemcpyAsync(dst, pb->p, bytes, cudaMemcpyHostToDevice, e->xs));
+    CK(cudaEventRecord(pb->done, e->xs));
+    CK(cudaEventRecord(e->slot_ready[slot], e->xs));
+    e->stats.h2d_bytes += (int64_t)bytes;
+    if (snapshot == 0 && index + 1 > e->nvol) e->nvol = index + 1;
+    e->vol_holds[slot] = snapshot;
+    return GR_OK;
+}
+
+int gr_load_constant(gr_engine *e, int64_t snapshot, int32_t index, const float *data, int64_t n) {
+    if (!e || !data) return USER_ERR("null argument >");
+    if (index < 0 || index >= GR_MAX_CONSTANTS) return USER_ERR("You provided more constants than supported. >");
+    if (e->n <= 0) return USER_ERR("Seeds must be set before constants. >");
+    if (n != e->n) return USER_ERR("Constant dimension does not match number of particles. >");
+    int rc = set_device(e);
+    if (rc) return rc;
+    CK(e->cons.alloc((size_t)e->n * GR_MAX_CONSTANTS * e->K));
+    const int slot = (int)(snapshot % e->K);
+    rc = wait_slot_free(e, slot);
+    if (rc) return rc;
+    PinnedBuf *pb = nullptr;
+    const size_t bytes = (size_t)n * sizeof(float);
+    rc = ensure_pinned(e, bytes, pb);
+    if (rc) return rc;
+    std::memcpy(pb->p, data, bytes);
+    CK(cudaMemcpyAsync(e->cons.p + ((int64_t)slot * GR_MAX_CONSTANTS + index) * e->n, pb->p, bytes,
+                       cudaMemcpyHostToDevice, e->xs));
+    CK(cudaEventRecord(pb->done, e->xs));
+    CK(cudaEventRecord(e->slot_ready[slot], e->xs));
+    e->stats.h2d_bytes += (int64_t)bytes;
+    if (snapshot == 0 && index + 1 > e->ncon) e->ncon = index + 1;
+    e->cons_holds[slot] = snapshot;
+    return GR_OK;
+}
+
+int gr_load_uplift(gr_engine *e, int64_t snapshot, const float *data, int64_t n, int32_t dim) {
+    if (!e || !data) return USER_ERR("null argument >");
+    if (e->n <= 0) return USER_ERR("Seeds must be set before the uplift. >");
+    if (n != e->n) return USER_ERR("Uplift dimension does not match number of particles. >");
+    if (dim != e->dim) return USER_ERR("Uplift dimension does not match the integrator space. >");
+    if (e->dim == 2) return GR_OK;   // 2D variants never read the uplift
+    int rc = set_device(e);
+    if (rc) return rc;
+    CK(e->lift.alloc((size_t)e->n * 3 * e->K));
+    const int slot = (int)(snapshot % e->K);
+    rc = wait_slot_free(e, slot);
+    if (rc) return rc;
+    PinnedBuf *pb = nullptr;
+    const size_t bytes = (size_t)n * 3 * sizeof(float);
+    rc = ensure_pinned(e, bytes, pb);
+    if (rc) return rc;
+    std::memcpy(pb->p, data, bytes);
+    CK(cudaMemcpyAsync(e->lift.p + (int64_t)slot * e->n * 3, pb->p, bytes, cudaMemcpyHostToDevice, e->xs));
+    CK(cudaEventRecord(pb->done, e->xs));
+    CK(cudaEventRecord(e->slot_ready[slot], e->xs));
+    e->stats.h2d_bytes += (int64_t)bytes;
+    e->has_uplift = true;
+    e->lift_holds[slot] = snapshot;
+    return GR_OK;
+}
+
+int gr_set_topography(gr_engine *e, const float *data, int64_t ny, int64_t nx) {
+    if (!e || !data) return USER_ERR("null argument >");
+    if (!e->grid_set) return USER_ERR("The windfield must be loaded before the topography. >");
+    if (nx != e->nx || ny != e->ny) return USER_ERR("Topography dimensions does not match to provided data! >");
+    int rc = set_device(e);
+    if (rc) return rc;
+    CK(e->topo.alloc((size_t)nx * ny));
+    CK(cudaMemcpy(e->topo.p, data, (size_t)nx * ny * sizeof(float), cudaMemcpyHostToDevice));
+    e->has_topo = e->dim == 3;   // 2D variants never use the topography (Macros.hpp:71)
+    return GR_OK;
+}
+
+int gr_compile_expression(gr_engine *e, int32_t index, const char *code, const char *const *volume_names,
+                          int32_t n_volumes, const char *const *constant_names, int32_t n_constants) {
+    if (!e || !code) return USER_ERR("null argument >");
+    if (index < 0 || index >= GR_MAX_EXPRESSIONS) return USER_ERR("At most 4 AdditionalCompute expressions are supported. >");
+    std::vector<std::string> vn, cn;
+    for (int k = 0; k < n_volumes; ++k) vn.emplace_back(volume_names[k] ? volume_names[k] : "");
+    for (int k = 0; k < n_constants; ++k) cn.emplace_back(constant_names[k] ? constant_names[k] : "");
+    std::string err;
+    Program p{};
+    if (!compile_expression(code, vn, cn, e->dim, e->s.curvature_mode, p, err)) return fail(GR_ERR_USER, "%s", err.c_str());
+    e->progs[index] = p;
+    if (index + 1 > e->nexpr) e->nexpr = index + 1;
+    return GR_OK;
+}
+
+int gr_expression_evaluate(const char *code, const char *const *volume_names, int32_t n_volumes,
+                           const char *const *constant_names, int32_t n_constants, int32_t dim,
+                           int32_t curvature_mode, const float *ref, float *out) {
+    if (!code || !ref || !out) return USER_ERR("null argument >");
+    std::vector<std::string> vn, cn;
+    for (int k = 0; k < n_volumes; ++k) vn.emplace_back(volume_names[k] ? volume_names[k] : "");
+    for (int k = 0; k < n_constants; ++k) cn.emplace_back(constant_names[k] ? constant_names[k] : "");
+    std::string err;
+    Program p{};
+    if (!compile_expression(code, vn, cn, dim, curvature_mode, p, err)) return fail(GR_ERR_USER, "%s", err.c_str());
+    *out = evaluate(p, ref);
+    return GR_OK;
+}
+
+static int set_seeds(gr_engine *e, const float *pos, int64_t n, int32_t dim, bool device_src) {
+    if (!e || (!pos && n > 0)) return USER_ERR("null argument >");
+    if (dim != e->dim) return USER_ERR("Dimensions of IntegratorSettings and provided TrajectorySet do not match. >");
+    if (n <= 0) return USER_ERR("Provided TrajectorySet does not contain any data. >");
+    if (n > (int64_t(1) << 31) - 1) return USER_ERR("Too many particles. >");
+    int rc = set_device(e);
+    if (rc) return rc;
+    e->n = n;
+    CK(e->seeds.alloc((size_t)n * dim));
+    CK(cudaMemcpy(e->seeds.p, pos, (size_t)n * dim * sizeof(float),
+                  device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
+    if (!device_src) e->stats.h2d_bytes += n * dim * (int64_t)sizeof(float);
+    return GR_OK;
+}
+
+int gr_set_seeds(gr_engine *e, const float *pos, int64_t n, int32_t dim) { return set_seeds(e, pos, n, dim, false); }
+int gr_set_seeds_device(gr_engine *e, const float *pos, int64_t n, int32_t dim) { return set_seeds(e, pos, n, dim, true); }
+
+}  // extern "C"
+
+// ====================================================================== run
+
+namespace {
+
+int alloc_state(gr_engine *e) {
+    const int64_t n = e->n;
+    const size_t N = (size_t)n;
+    CK(e->px.alloc(N)); CK(e->py.alloc(N)); CK(e->pz.alloc(N));
+    CK(e->status.alloc(N)); CK(e->id.alloc(N));
+    const int cm = e->s.curvature_mode;
+    if (cm == 1 || cm == 3) { CK(e->qx.alloc(N)); CK(e->qy.alloc(N)); CK(e->qz.alloc(N)); }
+    if (e->s.compensated) {
+        CK(e->kx.alloc(N)); CK(e->ky.alloc(N)); CK(e->kz.alloc(N));
+        CK(cudaMemsetAsync(e->kx.p, 0, N * 4, e->cs)); CK(cudaMemsetAsync(e->ky.p, 0, N * 4, e->cs));
+        CK(cudaMemsetAsync(e->kz.p, 0, N * 4, e->cs));
+    }
+    if (cm == 2) {
+        CK(e->lx.alloc(N)); CK(e->ly.alloc(N)); CK(e->lz.alloc(N));
+        CK(cudaMemsetAsync(e->lx.p, 0, N * 4, e->cs)); CK(cudaMemsetAsync(e->ly.p, 0, N * 4, e->cs));
+        CK(cudaMemsetAsync(e->lz.p, 0, N * 4, e->cs));
+    }
+    CK(e->length.alloc(N)); CK(e->tc.alloc(N)); CK(e->curv.alloc(N));
+    CK(cudaMemsetAsync(e->length.p, 0, N * 4, e->cs));
+    CK(cudaMemsetAsync(e->tc.p, 0, N * 4, e->cs));
+    CK(cudaMemsetAsync(e->curv.p, 0, N * 4, e->cs));
+    const int nv = std::max(1, e->nvol), ne = std::max(1, e->nexpr);
+    CK(e->volc.alloc(N * nv)); CK(e->cmpc.alloc(N * ne));
+    CK(cudaMemsetAsync(e->volc.p, 0, N * nv * 4, e->cs));
+    CK(cudaMemsetAsync(e->cmpc.p, 0, N * ne * 4, e->cs));
+    CK(e->out_status.alloc(N)); CK(e->out_length.alloc(N)); CK(e->out_tc.alloc(N));
+    const int threads = 256;
+    seed_kernel<<<grid_for(n, threads), threads, 0, e->cs>>>(e->seeds.p, n, e->dim, e->px.p, e->py.p, e->pz.p,
+                                                             e->status.p, e->id.p);
+    CK(cudaGetLastError());
+    e->stats.aux_launches++;
+    return GR_OK;
+}
+
+KParams make_params(gr_engine *e) {
+    KParams P;
+    std::memset(&P, 0, sizeof P);
+    for (int d = 0; d < 3; ++d) {
+        P.inv_scale[d] = e->inv_scale[d];
+        P.off[d] = e->off[d];
+        P.dom[d] = e->dom[d];
+        P.scale[d] = e->scale[d];
+    }
+    P.nx = (int32_t)e->nx; P.ny = (int32_t)e->ny; P.nz = (int32_t)e->nz; P.dim = e->dim;
+    P.wind = e->wind.p; P.wind_stride = e->wind_stride;
+    P.vol = e->vol.p; P.vol_plane = e->nodes;
+    P.cons = e->cons.p; P.lift = e->lift.p; P.topo = e->topo.p;
+    P.px = e->px.p; P.py = e->py.p; P.pz = e->pz.p;
+    P.qx = e->qx.p; P.qy = e->qy.p; P.qz = e->qz.p;
+    P.kx = e->kx.p; P.ky = e->ky.p; P.kz = e->kz.p;
+    P.lx = e->lx.p; P.ly = e->ly.p; P.lz = e->lz.p;
+    P.status = e->status.p; P.length = e->length.p; P.tc = e->tc.p; P.curv = e->curv.p;
+    P.volc = e->volc.p; P.cmpc = e->cmpc.p; P.id = e->id.p;
+    P.n = e->n; P.n_state = e->n; P.n_total = e->n;
+    P.hpos = e->hpos.p; P.hcurv = e->hcurv.p; P.hvol = e->hvol.p; P.hcmp = e->hcmp.p;
+    P.L = e->L; P.Lc = e->Lc; P.Li = e->Li;
+    P.sched = e->d_sched.p;
+    const gr_settings &s = e->s;
+    P.h = s.delta_t;
+    P.hh = 0.5f * s.delta_t;
+    P.sixth = 1.0f / 6;
+    P.max_length = s.maximum_length;
+    P.sphere_radius = s.sphere_radius;
+    P.wind_dynamic = e->wind_dynamic;
+    P.dyn_any = e->dyn_any;
+    P.border_mode = e->dim == 2 ? s.border_mode : 0;
+    P.curvature_mode = s.curvature_mode;
+    P.abort_mode = s.abort_mode;
+    P.uplift_mode = e->dim == 3 && e->has_uplift ? s.uplift_mode : 0;
+    P.constants_mode = e->ncon > 0 ? s.constants_mode : 0;
+    P.volume_mode = e->nvol > 0 ? s.volume_mode : 0;
+    P.reverse = s.reverse ? 1 : 0;
+    P.sphere = e->dim == 2 && s.sphere_radius > 0.f;
+    P.topography = e->has_topo ? 1 : 0;
+    P.compensated = s.compensated ? 1 : 0;
+    P.nvol = P.volume_mode ? e->nvol : 0;
+    P.ncon = P.constants_mode ? e->ncon : 0;
+    P.nexpr = e->nexpr;
+    P.prog = e->d_prog.p;
+    P.counters = e->counters.p;
+    return P;
+}
+
+using KernelFn = void (*)(const KParams);
+
+KernelFn pick_kernel(const gr_engine *e) {
+    const bool rk4 = e->s.integrator == 1;
+    const int st = e->s.storage;
+    if (e->dim == 3) {
+        if (rk4) return st == GR_STORE_BF16 ? advance_kernel<3, true, __nv_bfloat16>
+                      : st == GR_STORE_F16 ? advance_kernel<3, true, __half> : advance_kernel<3, true, float>;
+        return st == GR_STORE_BF16 ? advance_kernel<3, false, __nv_bfloat16>
+             : st == GR_STORE_F16 ? advance_kernel<3, false, __half> : advance_kernel<3, false, float>;
+    }
+    if (rk4) return st == GR_STORE_BF16 ? advance_kernel<2, true, __nv_bfloat16>
+                  : st == GR_STORE_F16 ? advance_kernel<2, true, __half> : advance_kernel<2, true, float>;
+    return st == GR_STORE_BF16 ? advance_kernel<2, false, __nv_bfloat16>
+         : st == GR_STORE_F16 ? advance_kernel<2, false, __half> : advance_kernel<2, false, float>;
+}
+
+int block_size_for(const gr_engine *e) {
+    if (e->s.block_size > 0) return e->s.block_size;
+    // keep at least ~2 blocks per SM on small particle counts
+    int bs = 256;
+    while (bs > 32 && (e->n + bs - 1) / bs < 2 * 148) bs /= 2;
+    return bs;
+}
+
+cudaEvent_t pool_event(gr_engine *e, size_t k) {
+    while (e->ev_pool.size() <= k) {
+        cudaEvent_t ev;
+        cudaEventCreate(&ev);
+        e->ev_pool.push_back(ev);
+    }
+    return e->ev_pool[k];
+}
+
+struct RunCtx {
+    gr_engine *e;
+    KParams P;
+    KernelFn fn;
+    int threads;
+    size_t ev_used = 0;
+};
+
+int launch_steps(RunCtx &r, int64_t s0, int64_t s1) {
+    gr_engine *e = r.e;
+    KParams P = r.P;
+    P.s0 = (int32_t)s0;
+    P.s1 = (int32_t)s1;
+    CK(cudaMemsetAsync(e->counters.p + 1, 0, sizeof(unsigned long long), e->cs));
+    cudaEvent_t a = pool_event(e, r.ev_used++), b = pool_event(e, r.ev_used++);
+    CK(cudaEventRecord(a, e->cs));
+    // one thread per particle: the step kernel is not grid-strided
+    const int64_t blocks = (P.n + r.threads - 1) / r.threads;
+    r.fn<<<(unsigned)std::max<int64_t>(1, blocks), r.threads, 0, e->cs>>>(P);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(b, e->cs));
+    e->stats.launches++;
+    return GR_OK;
+}
+
+int call_loader(gr_engine *e, gr_loader_fn loader, void *user, int64_t snapshot, int &result) {
+    if (!loader) {
+        result = 0;
+        return GR_OK;
+    }
+    result = loader(user, e, snapshot);
+    if (result < 0) {
+        if (g_last_error.empty()) g_last_error = "ERROR < RUNTIME | the loader callback failed >";
+        return GR_ERR_CALLBACK;
+    }
+    if (result > 0) {
+        const int slot = (int)(snapshot % e->K);
+        if (e->wind_dynamic && e->wind_holds[slot] != snapshot)
+            return fail(GR_ERR_USER, "ERROR < USER INPUT | The loader did not provide windfield snapshot %lld. >",
+                        (long long)snapshot);
+    }
+    return GR_OK;
+}
+
+}  // namespace
+
+extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
+    if (!e) return USER_ERR("null engine >");
+    g_last_error.clear();
+    int rc = set_device(e);
+    if (rc) return rc;
+    rc = ensure_particles(e);
+    if (rc) return rc;
+    if (!e->grid_set) return USER_ERR("No windfield was loaded. >");
+    if (e->wind_holds[0] != 0)
+        return USER_ERR("Snapshot 0 is no longer resident in the ring; load the data again to run again. >");
+    if (e->dyn_any && e->wind_dynamic && e->wind_holds[1 % e->K] != 1) return USER_ERR("Cannot increment loader. >");
+    const gr_settings &s = e->s;
+    // settings combinations the reference has no kernel variant for
+    // (TrajectoryIntegrator.gen.py:52-53 and the 2D curvature axis, gen.py:184-187)
+    if (e->dim == 2 && (s.curvature_mode == 1 || s.curvature_mode == 3))
+        return USER_ERR("No kernel could be picked for your settings configuration. >");
+    if (s.constants_mode != 0 && e->nexpr == 0)
+        return USER_ERR("No kernel could be picked for your settings configuration. >");
+    e->have_result = false;
+    {
+        const int64_t h2d = e->stats.h2d_bytes, d2h = e->stats.d2h_bytes;
+        e->stats = gr_stats{};
+        e->stats.h2d_bytes = h2d;
+        e->stats.d2h_bytes = d2h;
+    }
+
+    ScheduleInput si;
+    si.dyn_any = e->dyn_any;
+    si.wind_dynamic = e->wind_dynamic;
+    si.delta_t = s.delta_t;
+    si.data_time_distance = s.data_time_distance;
+    si.maximum_simulation_time = s.maximum_simulation_time;
+    si.save_interval = s.save_interval;
+    si.time_mode = s.time_mode;
+    const Schedule sched = build_schedule(si);
+    const int64_t nsteps = (int64_t)sched.steps.size();
+    const int64_t nwin = (int64_t)sched.window_begin.size() - 1;
+
+    // records: seed + saves (+ the final record when SaveInterval == 0)
+    int64_t nsaves = 0;
+    for (const auto &st : sched.steps) nsaves += st.save;
+    e->L = 1 + nsaves + (s.save_interval == 0 ? 1 : 0);
+    e->Li = e->L - 1;
+    e->Lc = s.curvature_mode == 3 ? e->L - 1 : 0;
+
+    // device schedule
+    e->h_sched.resize(std::max<int64_t>(1, nsteps));
+    {
+        int64_t rec = 1, crec = 0, irec = 0;
+        for (int64_t k = 0; k < nsteps; ++k) {
+            const HostStep &h = sched.steps[k];
+            StepEntry E{};
+            E.t0 = h.t0; E.t1 = h.t1; E.t2 = h.t2;
+            E.flags = (h.save ? SF_SAVE : 0) | (h.time_pos ? SF_TIME_POS : 0) |
+                      (h.save && h.time_pos ? SF_CURV_REC : 0);
+            E.rec = (int32_t)rec; E.crec = (int32_t)crec; E.irec = (int32_t)irec;
+            E.slot_back = (int32_t)(h.window % e->K);
+            E.slot_front = (int32_t)((h.window + 1) % e->K);
+            if (h.save) {
+                ++rec;
+                ++irec;
+                if (h.time_pos) ++crec;
+            }
+            e->h_sched[k] = E;
+        }
+    }
+    CK(e->d_sched.alloc(e->h_sched.size()));
+    CK(cudaMemcpyAsync(e->d_sched.p, e->h_sched.data(), e->h_sched.size() * sizeof(StepEntry), cudaMemcpyHostToDevice, e->cs));
+    CK(e->d_prog.alloc(GR_MAX_EXPR));
+    CK(cudaMemcpyAsync(e->d_prog.p, e->progs, sizeof(e->progs), cudaMemcpyHostToDevice, e->cs));
+
+    rc = alloc_state(e);
+    if (rc) return rc;
+    const size_t N = (size_t)e->n;
+    CK(e->hpos.alloc(N * e->L * e->dim));
+    if (e->Lc > 0) CK(e->hcurv.alloc(N * e->Lc));
+    if (e->nvol > 0 && s.volume_mode != 0 && e->Li > 0) CK(e->hvol.alloc(N * e->Li * e->nvol));
+    if (e->nexpr > 0 && e->Li > 0) CK(e->hcmp.alloc(N * e->Li * e->nexpr));
+    seed_record_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(e->seeds.p, e->n, e->dim, e->hpos.p, e->L);
+    CK(cudaGetLastError());
+    CK(cudaMemsetAsync(e->counters.p, 0, 4 * sizeof(unsigned long long), e->cs));
+
+    cudaEvent_t run_a = pool_event(e, 0), run_b = pool_event(e, 1);
+    RunCtx r{e, make_params(e), pick_kernel(e), block_size_for(e), 2};
+    CK(cudaEventRecord(run_a, e->cs));
+    // the first windows read snapshots already uploaded
+    for (int k = 0; k < e->K; ++k)
+        if (e->wind_holds[k] >= 0 || e->vol_holds[k] >= 0 || e->cons_holds[k] >= 0 || e->lift_holds[k] >= 0)
+            CK(cudaStreamWaitEvent(e->cs, e->slot_ready[k], 0));
+
+    const int64_t spl = s.steps_per_launch > 0 ? s.steps_per_launch : (int64_t)1 << 40;
+    const int64_t gmax = std::max(1, e->K - 1);
+    int64_t executed = 0, windows_run = 0;
+    bool stop = false;
+    int64_t w = 0;
+    auto launch_range = [&](int64_t b, int64_t t) -> int {
+        if (s.minimum_alive > 0) {
+            for (int64_t k = b; k < t; ++k) {
+                // alive() before every step (tpp:973-975)
+                unsigned long long alive = e->n;
+                if (k > 0 || executed > 0) {
+                    CK(cudaMemcpyAsync(e->h_counters, e->counters.p, 2 * sizeof(unsigned long long),
+                                       cudaMemcpyDeviceToHost, e->cs));
+                    CK(cudaStreamSynchronize(e->cs));
+                    alive = e->h_counters[1];
+                }
+                if ((long long)alive < (long long)s.minimum_alive) return 1;
+                int q = launch_steps(r, k, k + 1);
+                if (q) return q;
+                ++executed;
+            }
+            return 0;
+        }
+        for (int64_t k = b; k < t; k += spl) {
+            int q = launch_steps(r, k, std::min(t, k + spl));
+            if (q) return q;
+        }
+        executed += t - b;
+        return 0;
+    };
+
+    while (w < nwin && !stop) {
+        int64_t g_end = w + 1;
+        bool exhausted = false;
+        // windows w .. g_end-1 run in one group; their snapshots must all fit in the ring
+        while (g_end < nwin && g_end - w < gmax && s.minimum_alive == 0 && e->dyn_any) {
+            int res = 0;
+            rc = call_loader(e, loader, user, g_end + 1, res);   // the loader step after window g_end-1
+            if (rc) return rc;
+            if (res == 0) { exhausted = true; break; }
+            CK(cudaStreamWaitEvent(e->cs, e->slot_ready[(g_end + 1) % e->K], 0));
+            ++g_end;
+        }
+        for (int64_t k = w; k < g_end + (e->dyn_any ? 1 : 0) && k <= w + e->K; ++k)
+            CK(cudaStreamWaitEvent(e->cs, e->slot_ready[k % e->K], 0));
+        const int q = launch_range(sched.window_begin[w], sched.window_begin[g_end]);
+        if (q < 0) return q;
+        windows_run = g_end;
+        // slots read by this group become free once it has run
+        for (int64_t k = w; k <= g_end && k - w < e->K; ++k) {
+            CK(cudaEventRecord(e->slot_free[k % e->K], e->cs));
+            e->slot_used[k % e->K] = true;
+        }
+        const bool alive_abort = q == 1;
+        if (exhausted) break;
+        if (e->dyn_any) {
+            int res = 0;
+            rc = call_loader(e, loader, user, g_end + 1, res);   // loader step after window g_end-1
+            if (rc) return rc;
+            if (res == 0 || alive_abort) break;
+            CK(cudaStreamWaitEvent(e->cs, e->slot_ready[(g_end + 1) % e->K], 0));
+        } else {
+            break;
+        }
+        if (alive_abort) stop = true;
+        w = g_end;
+    }
+
+    // number of records written so far
+    int64_t rec_done = 1, crec_done = 0, irec_done = 0;
+    for (int64_t k = 0; k < executed; ++k)
+        if (sched.steps[k].save) {
+            ++rec_done;
+            ++irec_done;
+            if (sched.steps[k].time_pos) ++crec_done;
+        }
+    KParams P = r.P;
+    if (s.save_interval == 0) {
+        const bool tpos = executed > 0;   // data.Time > 0 after at least one step
+        if (e->dim == 3)
+            save_state_kernel<3><<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, (int32_t)rec_done, (int32_t)crec_done, (int32_t)irec_done, tpos);
+        else
+            save_state_kernel<2><<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, (int32_t)rec_done, (int32_t)crec_done, (int32_t)irec_done, tpos);
+        CK(cudaGetLastError());
+        ++rec_done;
+        ++irec_done;
+        if (tpos) ++crec_done;
+        e->stats.aux_launches++;
+    }
+    finalize_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, e->out_status.p, e->out_length.p, e->out_tc.p);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(run_b, e->cs));
+    CK(cudaMemcpyAsync(e->h_counters, e->counters.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->cs));
+    CK(cudaStreamSynchronize(e->cs));
+
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, run_a, run_b));
+    e->stats.run_ms = ms;
+    double kms = 0.0;
+    for (size_t k = 2; k + 1 < r.ev_used; k += 2) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, e->ev_pool[k], e->ev_pool[k + 1]));
+        kms += t;
+    }
+    e->stats.kernel_ms = kms;
+    e->stats.particle_steps = (int64_t)e->h_counters[0];
+
+    e->info.n = e->n;
+    e->info.dim = e->dim;
+    e->info.records = rec_done;
+    e->info.curvature_records = s.curvature_mode == 3 ? crec_done : 0;
+    e->info.info_records = irec_done;
+    e->info.steps = executed;
+    e->info.windows = windows_run;
+    e->info.particle_steps = (int64_t)e->h_counters[0];
+    e->info.n_volumes = s.volume_mode != 0 ? e->nvol : 0;
+    e->info.n_expressions = e->nexpr;
+    e->have_result = true;
+    return GR_OK;
+}
+
+extern "C" {
+
+int gr_result_info_get(gr_engine *e, gr_result_info *out) {
+    if (!e || !out) return USER_ERR("null argument >");
+    if (!e->have_result) return USER_ERR("No result: run() has not completed. >");
+    *out = e->info;
+    return GR_OK;
+}
+
+int gr_stats_get(gr_engine *e, gr_stats *out) {
+    if (!e || !out) return USER_ERR("null argument >");
+    *out = e->stats;
+    return GR_OK;
+}
+
+static int fetch_rows(gr_engine *e, void *out, int64_t capacity, const void *src, int64_t rows, int64_t row_used,
+                      int64_t row_stride, size_t elem) {
+    if (!e || !out) return USER_ERR("null argument >");
+    if (!e->have_result) return USER_ERR("No result: run() has not completed. >");
+    if (capacity < rows * row_used) return USER_ERR("Output buffer too small. >");
+    if (rows == 0 || row_used == 0) return GR_OK;
+    int rc = set_device(e);
+    if (rc) return rc;
+    CK(cudaMemcpy2D(out, row_used * elem, src, row_stride * elem, row_used * elem, rows, cudaMemcpyDeviceToHost));
+    e->stats.d2h_bytes += rows * row_used * (int64_t)elem;
+    return GR_OK;
+}
+
+int gr_fetch_positions(gr_engine *e, float *out, int64_t cap) {
+    if (!e) return USER_ERR("null engine >");
+    return fetch_rows(e, out, cap, e->hpos.p, e->n, e->info.records * e->dim, e->L * e->dim, sizeof(float));
+}
+
+int gr_fetch_status(gr_engine *e, int32_t *out, int64_t cap) {
+    if (!e) return USER_ERR("null engine >");
+    return fetch_rows(e, out, cap, e->out_status.p, 1, e->n, e->n, sizeof(int32_t));
+}
+
+int gr_fetch_lengths(gr_engine *e, float *out, int64_t cap) {
+    if (!e) return USER_ERR("null engine >");
+    if (e->s.abort_mode == 0) return GR_OK;
+    return fetch_rows(e, out, cap, e->out_length.p, 1, e->n, e->n, sizeof(float));
+}
+
+int gr_fetch_total_curvature(gr_engine *e, float *out, int64_t cap) {
+    if (!e) return USER_ERR("null engine >");
+    if (e->s.curvature_mode == 0) return GR_OK;
+    return fetch_rows(e, out, cap, e->out_tc.p, 1, e->n, e->n, sizeof(float));
+}
+
+int gr_fetch_curvatures(gr_engine *e, float *out, int64_t cap) {
+    if (!e) return USER_ERR("null engine >");
+    if (e->info.curvature_records == 0) return GR_OK;
+    return fetch_rows(e, out, cap, e->hcurv.p, e->n, e->info.curvature_records, e->Lc, sizeof(float));
+}
+
+int gr_fetch_volume_info(gr_engine *e, int32_t index, float *out, int64_t cap) {
+    if (!e) return USER_ERR("null engine >");
+    if (index < 0 || index >= e->info.n_volumes) return USER_ERR("TrajectorySet: Volume with given key does not exist! >");
+    if (e->info.info_records == 0) return GR_OK;
+    return fetch_rows(e, out, cap, e->hvol.p + (int64_t)index * e->n * e->Li, e->n, e->info.info_records, e->Li,
+                      sizeof(float));
+}
+
+int gr_fetch_compute_info(gr_engine *e, int32_t index, float *out, int64_t cap) {
+    if (!e) return USER_ERR("null engine >");
+    if (index < 0 || index >= e->info.n_expressions) return USER_ERR("TrajectorySet: Volume with given id does not exist! >");
+    if (e->info.info_records == 0) return GR_OK;
+    return fetch_rows(e, out, cap, e->hcmp.p + (int64_t)index * e->n * e->Li, e->n, e->info.info_records, e->Li,
+                      sizeof(float));
+}
+
+}  // extern "C"

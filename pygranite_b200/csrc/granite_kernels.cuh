@@ -1,0 +1,677 @@
+// granite_kernels.cuh — sm_100a device code of the trajectory step path.
+//
+// One thread owns one particle.  A launch advances its particle through a range of steps
+// (one or more snapshot windows) with the particle state in registers; the reference
+// instead launches `integrate` once per step on a single 512-thread block and
+// double-buffers AoS positions through global memory (TrajectoryIntegrator.tpp:108-457,
+// 790-796, 978-984).  Per step the uniform data (time weights, save slots, ring slots)
+// comes from a small device schedule.
+//
+// Arithmetic follows one fixed operation order, spelled out with __fmaf_rn and compiled
+// with --fmad=false, so the float32 oracle build reproduces it bit for bit.  Wind is
+// stored node-major: float4 {u,v,w,0} (3D) or float2 {u,v} (2D) per node for float32,
+// four / two 16-bit values per node for bf16 / fp16.  Hardware texture filtering (8-bit
+// weights, TrajectoryIntegrator.cpp:503-505) is replaced by float32 interpolation.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cstdint>
+
+#include "expr.h"
+
+namespace granite_b200 {
+
+constexpr int GR_MAX_VOL = 8;
+constexpr int GR_MAX_EXPR = 4;
+constexpr int GR_MAX_CON = 4;
+
+// Step-schedule flags.
+constexpr int SF_SAVE = 1;       // position / info record after this step
+constexpr int SF_TIME_POS = 2;   // data.Time > 0 at the start of the step
+constexpr int SF_CURV_REC = 4;   // curvature record after this step (IndividualAndTotal)
+
+struct StepEntry {
+    float t0, t1, t2;      // time weights of the RK4 stages (t1 also for k3)
+    int32_t flags;
+    int32_t rec, crec, irec;
+    int32_t slot_back, slot_front;   // ring slots of the window's snapshots
+    int32_t pad[3];
+};
+
+struct KParams {
+    // geometry (TrajectoryIntegrator.tpp:521-574)
+    float inv_scale[3], off[3], dom[3], scale[3];
+    int32_t nx, ny, nz, dim;
+    // ring buffers: slot s of quantity q starts at base + s * stride
+    const void *wind;
+    int64_t wind_stride;          // bytes per slot
+    const float *vol;             // [slot][8][plane]
+    int64_t vol_plane;            // floats per plane
+    const float *cons;            // [slot][4][n_total]
+    const float *lift;            // [slot][n_total * dim]
+    const float *topo;            // (ny, nx)
+    // particle state, slot order
+    float *px, *py, *pz;          // position
+    float *qx, *qy, *qz;          // previous position (curvature pm1)
+    float *kx, *ky, *kz;          // Kahan compensation
+    float *lx, *ly, *lz;          // last direction (FastTotal curvature)
+    int32_t *status;
+    float *length, *tc, *curv;
+    float *volc;                  // [8][n_state]
+    float *cmpc;                  // [4][n_state]
+    const int32_t *id;            // original particle index
+    int64_t n;                    // particles in this launch (prefix of the state arrays)
+    int64_t n_state;              // stride of volc / cmpc
+    int64_t n_total;              // original particle count (history / constants stride)
+    // history, particle-major
+    float *hpos;                  // [(id * L + rec) * dim + d]
+    float *hcurv;                 // [id * Lc + crec]
+    float *hvol;                  // [(k * n_total + id) * Li + irec]
+    float *hcmp;                  // [(e * n_total + id) * Li + irec]
+    int64_t L, Lc, Li;
+    // schedule
+    const StepEntry *sched;
+    int32_t s0, s1;
+    // options (runtime-uniform)
+    float h, hh, sixth, max_length, sphere_radius;
+    int32_t wind_dynamic, dyn_any, border_mode, curvature_mode, abort_mode, uplift_mode;
+    int32_t constants_mode, volume_mode, reverse, sphere, topography, compensated;
+    int32_t nvol, ncon, nexpr;
+    const Program *prog;          // [4]
+    unsigned long long *counters; // [0] particle-steps, [1] alive at the end of the launch
+};
+
+// ------------------------------------------------------------------ helpers
+
+__device__ __forceinline__ float lerp_(float a, float b, float t) { return __fmaf_rn(t, b - a, a); }
+
+// Texture coordinate -> cell index and fraction.  Coordinates are clamped to [-2, n+1]
+// first; every corner outside the grid is border (3D) or clamped (2D), so the clamp never
+// changes a value and keeps the integer conversion in range.
+__device__ __forceinline__ void cell(float a, int n, int &i, float &f) {
+    a = fminf(fmaxf(a, -2.0f), (float)(n + 1));
+    const float fl = floorf(a);
+    i = (int)fl;
+    f = a - fl;
+}
+
+template <typename W> struct Store;
+
+template <> struct Store<float> {
+    // 3D node {u, v, w, 0}
+    static __device__ __forceinline__ void load3(const void *base, int64_t idx, float &u, float &v, float &w) {
+        const float4 q = __ldg(reinterpret_cast<const float4 *>(base) + idx);
+        u = q.x; v = q.y; w = q.z;
+    }
+    static __device__ __forceinline__ void load2(const void *base, int64_t idx, float &u, float &v) {
+        const float2 q = __ldg(reinterpret_cast<const float2 *>(base) + idx);
+        u = q.x; v = q.y;
+    }
+    static constexpr int bytes3 = 16, bytes2 = 8;
+};
+
+template <> struct Store<__nv_bfloat16> {
+    static __device__ __forceinline__ void load3(const void *base, int64_t idx, float &u, float &v, float &w) {
+        const uint2 q = __ldg(reinterpret_cast<const uint2 *>(base) + idx);
+        const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&q.x));
+        const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&q.y));
+        u = a.x; v = a.y; w = b.x;
+    }
+    static __device__ __forceinline__ void load2(const void *base, int64_t idx, float &u, float &v) {
+        const unsigned q = __ldg(reinterpret_cast<const unsigned *>(base) + idx);
+        const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&q));
+        u = a.x; v = a.y;
+    }
+    static constexpr int bytes3 = 8, bytes2 = 4;
+};
+
+template <> struct Store<__half> {
+    static __device__ __forceinline__ void load3(const void *base, int64_t idx, float &u, float &v, float &w) {
+        const uint2 q = __ldg(reinterpret_cast<const uint2 *>(base) + idx);
+        const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&q.x));
+        const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&q.y));
+        u = a.x; v = a.y; w = b.x;
+    }
+    static __device__ __forceinline__ void load2(const void *base, int64_t idx, float &u, float &v) {
+        const unsigned q = __ldg(reinterpret_cast<const unsigned *>(base) + idx);
+        const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&q));
+        u = a.x; v = a.y;
+    }
+    static constexpr int bytes3 = 8, bytes2 = 4;
+};
+
+// Trilinear corner weights of one sample: indices and border validity.
+struct Cell3 {
+    int64_t base;        // node index of corner (ix, iy, iz), clamped into the grid
+    int64_t sx, sy, sz;  // strides to the +x / +y / +z corner (0 where that corner is clamped)
+    float fx, fy, fz;
+    unsigned valid;      // bit (dz*4 + dy*2 + dx): corner inside the grid
+};
+
+__device__ __forceinline__ Cell3 make_cell3(const KParams &P, float ax, float ay, float az) {
+    int ix, iy, iz;
+    Cell3 c;
+    cell(ax, P.nx, ix, c.fx);
+    cell(ay, P.ny, iy, c.fy);
+    cell(az, P.nz, iz, c.fz);
+    const bool x0 = (unsigned)ix < (unsigned)P.nx, x1 = (unsigned)(ix + 1) < (unsigned)P.nx;
+    const bool y0 = (unsigned)iy < (unsigned)P.ny, y1 = (unsigned)(iy + 1) < (unsigned)P.ny;
+    const bool z0 = (unsigned)iz < (unsigned)P.nz, z1 = (unsigned)(iz + 1) < (unsigned)P.nz;
+    c.valid = 0;
+    c.valid |= (x0 && y0 && z0) << 0;
+    c.valid |= (x1 && y0 && z0) << 1;
+    c.valid |= (x0 && y1 && z0) << 2;
+    c.valid |= (x1 && y1 && z0) << 3;
+    c.valid |= (x0 && y0 && z1) << 4;
+    c.valid |= (x1 && y0 && z1) << 5;
+    c.valid |= (x0 && y1 && z1) << 6;
+    c.valid |= (x1 && y1 && z1) << 7;
+    const int cx = min(max(ix, 0), P.nx - 1), cy = min(max(iy, 0), P.ny - 1), cz = min(max(iz, 0), P.nz - 1);
+    c.base = ((int64_t)cz * P.ny + cy) * P.nx + cx;
+    c.sx = (ix + 1 >= 0 && ix + 1 < P.nx && ix >= 0) ? 1 : 0;
+    c.sy = (iy + 1 >= 0 && iy + 1 < P.ny && iy >= 0) ? (int64_t)P.nx : 0;
+    c.sz = (iz + 1 >= 0 && iz + 1 < P.nz && iz >= 0) ? (int64_t)P.nx * P.ny : 0;
+    return c;
+}
+
+// Trilinear interpolation of the three wind components of one snapshot (border = 0).
+template <typename W>
+__device__ __forceinline__ void tri3(const void *slot, const Cell3 &c, float &ou, float &ov, float &ow) {
+    float u[8], v[8], w[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
+        const int64_t idx = c.base + (dx ? c.sx : 0) + (dy ? c.sy : 0) + (dz ? c.sz : 0);
+        u[k] = 0.f; v[k] = 0.f; w[k] = 0.f;
+        if (c.valid & (1u << k)) Store<W>::load3(slot, idx, u[k], v[k], w[k]);
+    }
+    float a00 = lerp_(u[0], u[1], c.fx), a10 = lerp_(u[2], u[3], c.fx);
+    float a01 = lerp_(u[4], u[5], c.fx), a11 = lerp_(u[6], u[7], c.fx);
+    ou = lerp_(lerp_(a00, a10, c.fy), lerp_(a01, a11, c.fy), c.fz);
+    a00 = lerp_(v[0], v[1], c.fx); a10 = lerp_(v[2], v[3], c.fx);
+    a01 = lerp_(v[4], v[5], c.fx); a11 = lerp_(v[6], v[7], c.fx);
+    ov = lerp_(lerp_(a00, a10, c.fy), lerp_(a01, a11, c.fy), c.fz);
+    a00 = lerp_(w[0], w[1], c.fx); a10 = lerp_(w[2], w[3], c.fx);
+    a01 = lerp_(w[4], w[5], c.fx); a11 = lerp_(w[6], w[7], c.fx);
+    ow = lerp_(lerp_(a00, a10, c.fy), lerp_(a01, a11, c.fy), c.fz);
+}
+
+// Trilinear interpolation of one scalar float32 plane.
+__device__ __forceinline__ float tri1(const float *plane, const Cell3 &c) {
+    float s[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
+        const int64_t idx = c.base + (dx ? c.sx : 0) + (dy ? c.sy : 0) + (dz ? c.sz : 0);
+        s[k] = (c.valid & (1u << k)) ? __ldg(plane + idx) : 0.f;
+    }
+    const float a00 = lerp_(s[0], s[1], c.fx), a10 = lerp_(s[2], s[3], c.fx);
+    const float a01 = lerp_(s[4], s[5], c.fx), a11 = lerp_(s[6], s[7], c.fx);
+    return lerp_(lerp_(a00, a10, c.fy), lerp_(a01, a11, c.fy), c.fz);
+}
+
+// Bilinear footprint with clamped indices (2D pitch textures sample as clamp).
+struct Cell2 {
+    int64_t i00, i10, i01, i11;
+    float fx, fy;
+};
+
+__device__ __forceinline__ Cell2 make_cell2(int nx, int ny, float ax, float ay) {
+    int ix, iy;
+    Cell2 c;
+    cell(ax, nx, ix, c.fx);
+    cell(ay, ny, iy, c.fy);
+    const int x0 = min(max(ix, 0), nx - 1), x1 = min(max(ix + 1, 0), nx - 1);
+    const int y0 = min(max(iy, 0), ny - 1), y1 = min(max(iy + 1, 0), ny - 1);
+    c.i00 = (int64_t)y0 * nx + x0;
+    c.i10 = (int64_t)y0 * nx + x1;
+    c.i01 = (int64_t)y1 * nx + x0;
+    c.i11 = (int64_t)y1 * nx + x1;
+    return c;
+}
+
+template <typename W>
+__device__ __forceinline__ void bil2(const void *slot, const Cell2 &c, float &ou, float &ov) {
+    float u0, v0, u1, v1, u2, v2, u3, v3;
+    Store<W>::load2(slot, c.i00, u0, v0);
+    Store<W>::load2(slot, c.i10, u1, v1);
+    Store<W>::load2(slot, c.i01, u2, v2);
+    Store<W>::load2(slot, c.i11, u3, v3);
+    ou = lerp_(lerp_(u0, u1, c.fx), lerp_(u2, u3, c.fx), c.fy);
+    ov = lerp_(lerp_(v0, v1, c.fx), lerp_(v2, v3, c.fx), c.fy);
+}
+
+__device__ __forceinline__ float bil1(const float *plane, const Cell2 &c) {
+    return lerp_(lerp_(__ldg(plane + c.i00), __ldg(plane + c.i10), c.fx),
+                 lerp_(__ldg(plane + c.i01), __ldg(plane + c.i11), c.fx), c.fy);
+}
+
+struct V3 {
+    float x, y, z;
+};
+
+__device__ __forceinline__ float dot3(const V3 &a, const V3 &b, int dim) {
+    float s = a.x * b.x;
+    s = __fmaf_rn(a.y, b.y, s);
+    if (dim == 3) s = __fmaf_rn(a.z, b.z, s);
+    return s;
+}
+
+// Wind at world position p, time weight t: interpolate() of TrajectoryIntegrator.icc:42-110.
+template <int DIM, typename W>
+__device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, const void *wb, const void *wf) {
+    V3 r{0.f, 0.f, 0.f};
+    const float ax = (p.x - P.off[0]) * P.inv_scale[0];
+    const float ay = (p.y - P.off[1]) * P.inv_scale[1];
+    if (DIM == 3) {
+        const float az = (p.z - P.off[2]) * P.inv_scale[2];
+        const Cell3 c = make_cell3(P, ax, ay, az);
+        float bu, bv, bw;
+        tri3<W>(wb, c, bu, bv, bw);
+        if (P.wind_dynamic) {
+            float fu, fv, fw;
+            tri3<W>(wf, c, fu, fv, fw);
+            r.x = lerp_(bu, fu, t); r.y = lerp_(bv, fv, t); r.z = lerp_(bw, fw, t);
+        } else {
+            r.x = bu; r.y = bv; r.z = bw;
+        }
+    } else {
+        const Cell2 c = make_cell2(P.nx, P.ny, ax, ay);
+        float bu, bv;
+        bil2<W>(wb, c, bu, bv);
+        if (P.wind_dynamic) {
+            float fu, fv;
+            bil2<W>(wf, c, fu, fv);
+            r.x = lerp_(bu, fu, t); r.y = lerp_(bv, fv, t);
+        } else {
+            r.x = bu; r.y = bv;
+        }
+    }
+    return r;
+}
+
+// sphere_coordinates (TrajectoryIntegrator.tpp:98-104).
+__device__ __forceinline__ V3 sphere_(const KParams &P, float py, V3 v) {
+    const float pi = 3.14159265358979323846f;
+    V3 r{0.f, 0.f, 0.f};
+    r.x = (v.x * 180.f) / (P.sphere_radius * cosf(py * (pi * 2.f) / 360.f) * pi);
+    r.y = (v.y * 180.f) / (pi * P.sphere_radius);
+    return r;
+}
+
+__device__ __forceinline__ float ref_at(const float (&ref)[19], int i) {
+    switch (i) {
+        case 0: return ref[0]; case 1: return ref[1]; case 2: return ref[2]; case 3: return ref[3];
+        case 4: return ref[4]; case 5: return ref[5]; case 6: return ref[6]; case 7: return ref[7];
+        case 8: return ref[8]; case 9: return ref[9]; case 10: return ref[10]; case 11: return ref[11];
+        case 12: return ref[12]; case 13: return ref[13]; case 14: return ref[14]; case 15: return ref[15];
+        case 16: return ref[16]; case 17: return ref[17]; default: return ref[18];
+    }
+}
+
+// Postfix evaluation with an 8-register rotating stack (s0 = top); the program is uniform
+// across the grid, so every branch here is uniform.
+__device__ __forceinline__ float eval_program(const Program *prog, const float (&ref)[19]) {
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f, s4 = 0.f, s5 = 0.f, s6 = 0.f, s7 = 0.f;
+    const int len = prog->len;
+    for (int k = 0; k < len; ++k) {
+        const Instr in = prog->code[k];
+        float r;
+        bool binary = false, push = false;
+        switch (in.op) {
+            case OP_REF: r = ref_at(ref, in.arg); push = true; break;
+            case OP_CONST: r = in.value; push = true; break;
+            case OP_ADD: r = s1 + s0; binary = true; break;
+            case OP_SUB: r = s1 - s0; binary = true; break;
+            case OP_MUL: r = s1 * s0; binary = true; break;
+            case OP_DIV: r = s1 / s0; binary = true; break;
+            case OP_RSUB: r = s0 - s1; binary = true; break;
+            case OP_RDIV: r = s0 / s1; binary = true; break;
+            case OP_ATAN2: r = atan2f(s1, s0); binary = true; break;
+            case OP_RATAN2: r = atan2f(s0, s1); binary = true; break;
+            case OP_SQRT: r = sqrtf(s0); break;
+            case OP_EXP: r = expf(s0); break;
+            case OP_LOG: r = logf(s0); break;
+            case OP_SIN: r = sinf(s0); break;
+            case OP_COS: r = cosf(s0); break;
+            case OP_TAN: r = tanf(s0); break;
+            case OP_ASIN: r = asinf(s0); break;
+            case OP_ACOS: r = acosf(s0); break;
+            case OP_ATAN: r = atanf(s0); break;
+            default: r = s0; break;
+        }
+        if (push) {
+            s7 = s6; s6 = s5; s5 = s4; s4 = s3; s3 = s2; s2 = s1; s1 = s0; s0 = r;
+        } else if (binary) {
+            s0 = r; s1 = s2; s2 = s3; s3 = s4; s4 = s5; s5 = s6; s6 = s7;
+        } else {
+            s0 = r;
+        }
+    }
+    return s0;
+}
+
+// ------------------------------------------------------------------ the step kernel
+
+template <int DIM, bool RK4, typename W>
+__global__ void __launch_bounds__(256) advance_kernel(const __grid_constant__ KParams P) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < P.n;
+    int32_t st = valid ? P.status[i] : 1;
+    bool alive = st == 0;
+    const int64_t pid = valid ? (int64_t)P.id[i] : 0;
+
+    V3 p{0.f, 0.f, 0.f}, q{0.f, 0.f, 0.f}, comp{0.f, 0.f, 0.f}, ld{0.f, 0.f, 0.f};
+    float len = 0.f, tc = 0.f, cv = 0.f;
+    float vol[GR_MAX_VOL], cmp[GR_MAX_EXPR];
+#pragma unroll
+    for (int k = 0; k < GR_MAX_VOL; ++k) vol[k] = 0.f;
+#pragma unroll
+    for (int k = 0; k < GR_MAX_EXPR; ++k) cmp[k] = 0.f;
+
+    const bool curv_prev = P.curvature_mode == 1 || P.curvature_mode == 3;
+    if (valid) {
+        p.x = P.px[i]; p.y = P.py[i];
+        if (DIM == 3) p.z = P.pz[i];
+        if (curv_prev) { q.x = P.qx[i]; q.y = P.qy[i]; if (DIM == 3) q.z = P.qz[i]; }
+        if (P.compensated) { comp.x = P.kx[i]; comp.y = P.ky[i]; if (DIM == 3) comp.z = P.kz[i]; }
+        if (P.curvature_mode == 2) { ld.x = P.lx[i]; ld.y = P.ly[i]; if (DIM == 3) ld.z = P.lz[i]; }
+        if (P.abort_mode != 0) len = P.length[i];
+        if (P.curvature_mode != 0) tc = P.tc[i];
+        if (P.curvature_mode == 3) cv = P.curv[i];
+#pragma unroll
+        for (int k = 0; k < GR_MAX_VOL; ++k)
+            if (k < P.nvol) vol[k] = P.volc[k * P.n_state + i];
+#pragma unroll
+        for (int k = 0; k < GR_MAX_EXPR; ++k)
+            if (k < P.nexpr) cmp[k] = P.cmpc[k * P.n_state + i];
+    }
+    const bool was_alive = alive;
+    unsigned long long my_steps = 0;
+    const int sph = P.sphere && DIM == 2;
+
+    for (int s = P.s0; s < P.s1; ++s) {
+        const StepEntry E = P.sched[s];
+        if (alive) {
+            ++my_steps;
+            const int sb = P.wind_dynamic ? E.slot_back : 0, sf = P.wind_dynamic ? E.slot_front : 0;
+            const void *wb = reinterpret_cast<const char *>(P.wind) + (int64_t)sb * P.wind_stride;
+            const void *wf = reinterpret_cast<const char *>(P.wind) + (int64_t)sf * P.wind_stride;
+            const float t0 = P.dyn_any ? E.t0 : 0.f;
+
+            // integrator (tpp:135-231)
+            V3 v, vc;
+            if (RK4) {
+                const float t1 = E.t1, t2 = E.t2;
+                const V3 k1c = wind_at<DIM, W>(P, p, t0, wb, wf);
+                const V3 k1 = sph ? sphere_(P, p.y, k1c) : k1c;
+                V3 a{__fmaf_rn(k1.x, P.hh, p.x), __fmaf_rn(k1.y, P.hh, p.y), DIM == 3 ? __fmaf_rn(k1.z, P.hh, p.z) : 0.f};
+                const V3 k2c = wind_at<DIM, W>(P, a, t1, wb, wf);
+                const V3 k2 = sph ? sphere_(P, a.y, k2c) : k2c;
+                a = V3{__fmaf_rn(k2.x, P.hh, p.x), __fmaf_rn(k2.y, P.hh, p.y), DIM == 3 ? __fmaf_rn(k2.z, P.hh, p.z) : 0.f};
+                const V3 k3c = wind_at<DIM, W>(P, a, t1, wb, wf);
+                const V3 k3 = sph ? sphere_(P, a.y, k3c) : k3c;
+                a = V3{__fmaf_rn(k3.x, P.h, p.x), __fmaf_rn(k3.y, P.h, p.y), DIM == 3 ? __fmaf_rn(k3.z, P.h, p.z) : 0.f};
+                const V3 k4c = wind_at<DIM, W>(P, a, t2, wb, wf);
+                const V3 k4 = sph ? sphere_(P, a.y, k4c) : k4c;
+                v.x = (((k1.x + 2.f * k2.x) + 2.f * k3.x) + k4.x) * P.sixth;
+                v.y = (((k1.y + 2.f * k2.y) + 2.f * k3.y) + k4.y) * P.sixth;
+                v.z = DIM == 3 ? (((k1.z + 2.f * k2.z) + 2.f * k3.z) + k4.z) * P.sixth : 0.f;
+                if (sph) {
+                    vc.x = (((k1c.x + 2.f * k2c.x) + 2.f * k3c.x) + k4c.x) * P.sixth;
+                    vc.y = (((k1c.y + 2.f * k2c.y) + 2.f * k3c.y) + k4c.y) * P.sixth;
+                    vc.z = 0.f;
+                } else {
+                    vc = v;
+                }
+            } else {
+                vc = wind_at<DIM, W>(P, p, t0, wb, wf);
+                v = sph ? sphere_(P, p.y, vc) : vc;
+            }
+
+            // displacement, reverse and uplift (tpp:233-250)
+            V3 dp{v.x * P.h, v.y * P.h, DIM == 3 ? v.z * P.h : 0.f};
+            if (P.reverse) { dp.x = -dp.x; dp.y = -dp.y; dp.z = -dp.z; }
+            if (DIM == 3 && P.uplift_mode != 0) {
+                const int lb = P.uplift_mode == 2 ? E.slot_back : 0, lf = P.uplift_mode == 2 ? E.slot_front : 0;
+                const float *LB = P.lift + (int64_t)lb * P.n_total * 3 + pid * 3;
+                const float *LF = P.lift + (int64_t)lf * P.n_total * 3 + pid * 3;
+                if (P.uplift_mode == 1) {
+                    dp.x = dp.x + LB[0]; dp.y = dp.y + LB[1]; dp.z = dp.z + LB[2];
+                } else {
+                    dp.x = dp.x + lerp_(LB[0], LF[0], t0);
+                    dp.y = dp.y + lerp_(LB[1], LF[1], t0);
+                    dp.z = dp.z + lerp_(LB[2], LF[2], t0);
+                }
+            }
+
+            // length abort (tpp:252-280)
+            int32_t abort = 0;
+            if (P.abort_mode != 0) {
+                const float dpl = sqrtf(dot3(dp, dp, DIM));
+                const float nl = len + dpl;
+                if (P.abort_mode == 2) {
+                    if (nl > P.max_length) {
+                        const float sc = (P.max_length - len) / dpl;
+                        dp.x = sc * dp.x; dp.y = sc * dp.y; dp.z = sc * dp.z;
+                        len = P.max_length;
+                        abort = 1;
+                    } else {
+                        len = nl;
+                    }
+                } else {
+                    if (nl > P.max_length) abort = 1;
+                    len = nl;
+                }
+            }
+
+            // new position (tpp:282); Kahan-compensated in the precision form
+            V3 np;
+            if (P.compensated) {
+                const V3 sd{P.reverse ? -dp.x : dp.x, P.reverse ? -dp.y : dp.y, P.reverse ? -dp.z : dp.z};
+                float y = sd.x - comp.x, t = p.x + y;
+                np.x = t; comp.x = (t - p.x) - y;
+                y = sd.y - comp.y; t = p.y + y;
+                np.y = t; comp.y = (t - p.y) - y;
+                if (DIM == 3) { y = sd.z - comp.z; t = p.z + y; np.z = t; comp.z = (t - p.z) - y; }
+                else np.z = 0.f;
+            } else {
+                np.x = P.reverse ? p.x - dp.x : p.x + dp.x;
+                np.y = P.reverse ? p.y - dp.y : p.y + dp.y;
+                np.z = DIM == 3 ? (P.reverse ? p.z - dp.z : p.z + dp.z) : 0.f;
+            }
+
+            // border and abort checks (tpp:284-323, icc:7-20, tpp:13-96)
+            if (abort == 0) {
+                const float dp2 = dot3(dp, dp, DIM);
+                const int bm = DIM == 3 ? 0 : P.border_mode;
+                if (bm == 0) {
+                    bool topo = false;
+                    if (DIM == 3 && P.topography) {
+                        const Cell2 c = make_cell2(P.nx, P.ny, np.x / P.scale[0], np.y / P.scale[1]);
+                        topo = bil1(P.topo, c) > np.z;
+                    }
+                    if (topo) abort = 3;
+                    else if (dp2 < 1e-9f) abort = 4;
+                    else {
+                        bool out = np.x - P.off[0] > P.dom[0] || np.x - P.off[0] < 0.f ||
+                                   np.y - P.off[1] > P.dom[1] || np.y - P.off[1] < 0.f;
+                        if (DIM == 3) out = out || np.z - P.off[2] > P.dom[2] || np.z - P.off[2] < 0.f;
+                        if (out) abort = 2;
+                    }
+                } else if (dp2 < 1e-9f) {
+                    abort = 4;
+                } else {
+                    const float ox = P.off[0], oy = P.off[1], DX = P.dom[0], DY = P.dom[1];
+                    if (bm == 1) {
+                        np.x = fmodf(np.x - ox + DX, DX) + ox;
+                        if (np.y - oy > DY || np.y - oy < 0.f) abort = 2;
+                    } else if (bm == 2) {
+                        if (sph) {
+                            if (np.x - ox > DX || np.x - ox < 0.f || np.y - oy > DY || np.y - oy < 0.f) abort = 2;
+                        } else {
+                            np.y = fmodf(np.y - oy + DY, DY) + oy;
+                            if (np.x - ox > DX || np.x - ox < 0.f) abort = 2;
+                        }
+                    } else {
+                        if (sph) {
+                            const float nx_ = np.x - ox, ny_ = np.y - oy, px_ = p.x - ox, py_ = p.y - oy;
+                            if (ny_ < 0.f) {
+                                const float tx = (-py_) / (ny_ - py_) * (nx_ - px_) + px_;
+                                np.y = -ny_ + oy;
+                                np.x = fmodf(DX + 180.0f - nx_ + 2.f * tx, DX) + ox;
+                            } else if (ny_ >= DY) {
+                                const float tx = (DY - py_) / (ny_ - py_) * (nx_ - px_) + px_;
+                                np.y = (ny_ - DY) + oy;
+                                np.x = fmodf(DX + 180.0f - nx_ + 2.f * tx, DX) + ox;
+                            }
+                        } else {
+                            np.y = fmodf(np.y - oy + DY, DY) + oy;
+                        }
+                        np.x = fmodf(np.x - ox + DX, DX) + ox;
+                    }
+                }
+            }
+
+            st = abort;
+            if (abort == 2 || abort == 3 || abort == 4) {
+                // old position kept, total curvature flagged (tpp:327-332)
+                if (P.curvature_mode != 0) tc = -1.f;
+                alive = false;
+            } else {
+                // curvature (tpp:335-361)
+                if (P.curvature_mode == 2) {
+                    const float inv = 1.0f / sqrtf(dot3(v, v, DIM));
+                    const V3 u{v.x * inv, v.y * inv, v.z * inv};
+                    if (E.flags & SF_TIME_POS) {
+                        const float k = acosf(dot3(ld, u, DIM));
+                        if (!isnan(k)) tc += k;
+                    }
+                    ld = u;
+                } else if (curv_prev && (E.flags & SF_TIME_POS)) {
+                    float k = 0.f;
+                    if (DIM == 3) {
+                        const float two_dt = 2.f * P.h, dt2 = P.h * P.h;
+                        const V3 d1{(np.x - q.x) / two_dt, (np.y - q.y) / two_dt, (np.z - q.z) / two_dt};
+                        const V3 d2{((q.x + np.x) - 2.f * p.x) / dt2, ((q.y + np.y) - 2.f * p.y) / dt2,
+                                    ((q.z + np.z) - 2.f * p.z) / dt2};
+                        const V3 x{d1.y * d2.z - d1.z * d2.y, d1.z * d2.x - d1.x * d2.z, d1.x * d2.y - d1.y * d2.x};
+                        const float l = sqrtf(dot3(d1, d1, 3));
+                        k = fabsf(sqrtf(dot3(x, x, 3)) / (l * l * l));
+                    }
+                    const V3 a{p.x - q.x, p.y - q.y, p.z - q.z}, b{np.x - p.x, np.y - p.y, np.z - p.z};
+                    const float ds = 0.5f * (sqrtf(dot3(a, a, DIM)) + sqrtf(dot3(b, b, DIM)));
+                    if (P.curvature_mode == 3) cv = k;
+                    if (!isnan(k)) tc += k * ds;
+                }
+
+                // additional volumes at the new position (tpp:363-377)
+                if (P.volume_mode != 0 && P.nvol > 0) {
+                    const int vb = P.volume_mode == 2 ? E.slot_back : 0, vf = P.volume_mode == 2 ? E.slot_front : 0;
+                    const float ax = (np.x - P.off[0]) * P.inv_scale[0];
+                    const float ay = (np.y - P.off[1]) * P.inv_scale[1];
+                    if (DIM == 3) {
+                        const float az = (np.z - P.off[2]) * P.inv_scale[2];
+                        const Cell3 c = make_cell3(P, ax, ay, az);
+#pragma unroll
+                        for (int k = 0; k < GR_MAX_VOL; ++k) {
+                            if (k < P.nvol) {
+                                const float b = tri1(P.vol + ((int64_t)vb * GR_MAX_VOL + k) * P.vol_plane, c);
+                                vol[k] = P.volume_mode == 2
+                                             ? lerp_(b, tri1(P.vol + ((int64_t)vf * GR_MAX_VOL + k) * P.vol_plane, c), t0)
+                                             : b;
+                            }
+                        }
+                    } else {
+                        const Cell2 c = make_cell2(P.nx, P.ny, ax, ay);
+#pragma unroll
+                        for (int k = 0; k < GR_MAX_VOL; ++k) {
+                            if (k < P.nvol) {
+                                const float b = bil1(P.vol + ((int64_t)vb * GR_MAX_VOL + k) * P.vol_plane, c);
+                                vol[k] = P.volume_mode == 2
+                                             ? lerp_(b, bil1(P.vol + ((int64_t)vf * GR_MAX_VOL + k) * P.vol_plane, c), t0)
+                                             : b;
+                            }
+                        }
+                    }
+                }
+
+                // expressions (tpp:379-447)
+                if (P.nexpr > 0) {
+                    float ref[19];
+                    ref[0] = np.x; ref[1] = np.y; ref[2] = DIM == 3 ? np.z : 0.f;
+                    ref[3] = P.curvature_mode == 3 ? cv : 0.f;
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) ref[4 + k] = k < P.nvol ? vol[k] : 0.f;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        float c = 0.f;
+                        if (k < P.ncon && P.constants_mode != 0) {
+                            const int cb = P.constants_mode == 2 ? E.slot_back : 0;
+                            const float b = __ldg(P.cons + ((int64_t)cb * GR_MAX_CON + k) * P.n_total + pid);
+                            if (P.constants_mode == 2) {
+                                const float f = __ldg(P.cons + ((int64_t)E.slot_front * GR_MAX_CON + k) * P.n_total + pid);
+                                c = lerp_(b, f, t0);
+                            } else {
+                                c = b;
+                            }
+                        }
+                        ref[12 + k] = c;
+                    }
+                    ref[16] = vc.x; ref[17] = vc.y; ref[18] = DIM == 3 ? vc.z : 0.f;
+#pragma unroll
+                    for (int e = 0; e < GR_MAX_EXPR; ++e)
+                        if (e < P.nexpr) cmp[e] = eval_program(P.prog + e, ref);
+                }
+
+                q = p;
+                p = np;
+                if (abort != 0) alive = false;
+            }
+        }
+
+        if (valid && (E.flags & SF_SAVE)) {
+            float *hp = P.hpos + (pid * P.L + E.rec) * DIM;
+            hp[0] = p.x; hp[1] = p.y;
+            if (DIM == 3) hp[2] = p.z;
+            if (P.curvature_mode == 3 && (E.flags & SF_CURV_REC)) P.hcurv[pid * P.Lc + E.crec] = cv;
+            if (P.volume_mode != 0) {
+#pragma unroll
+                for (int k = 0; k < GR_MAX_VOL; ++k)
+                    if (k < P.nvol) P.hvol[((int64_t)k * P.n_total + pid) * P.Li + E.irec] = vol[k];
+            }
+#pragma unroll
+            for (int e = 0; e < GR_MAX_EXPR; ++e)
+                if (e < P.nexpr) P.hcmp[((int64_t)e * P.n_total + pid) * P.Li + E.irec] = cmp[e];
+        }
+    }
+
+    if (valid && was_alive) {
+        P.status[i] = st;
+        P.px[i] = p.x; P.py[i] = p.y;
+        if (DIM == 3) P.pz[i] = p.z;
+        if (curv_prev) { P.qx[i] = q.x; P.qy[i] = q.y; if (DIM == 3) P.qz[i] = q.z; }
+        if (P.compensated) { P.kx[i] = comp.x; P.ky[i] = comp.y; if (DIM == 3) P.kz[i] = comp.z; }
+        if (P.curvature_mode == 2) { P.lx[i] = ld.x; P.ly[i] = ld.y; if (DIM == 3) P.lz[i] = ld.z; }
+        if (P.abort_mode != 0) P.length[i] = len;
+        if (P.curvature_mode != 0) P.tc[i] = tc;
+        if (P.curvature_mode == 3) P.curv[i] = cv;
+#pragma unroll
+        for (int k = 0; k < GR_MAX_VOL; ++k)
+            if (k < P.nvol) P.volc[k * P.n_state + i] = vol[k];
+#pragma unroll
+        for (int k = 0; k < GR_MAX_EXPR; ++k)
+            if (k < P.nexpr) P.cmpc[k * P.n_state + i] = cmp[k];
+    }
+
+    // counters: particle-steps and the alive count after the launch (warp-aggregated)
+    const unsigned long long warp_steps = __reduce_add_sync(0xffffffffu, (unsigned)my_steps);
+    const unsigned alive_mask = __ballot_sync(0xffffffffu, valid && alive);
+    if ((threadIdx.x & 31) == 0) {
+        if (warp_steps) atomicAdd(P.counters, warp_steps);
+        if (alive_mask) atomicAdd(P.counters + 1, (unsigned long long)__popc(alive_mask));
+    }
+}
+
+}  // namespace granite_b200

@@ -1,0 +1,199 @@
+"""Seeded synthetic wind fields and seed sets for the benchmark configurations.
+
+No public dataset is involved: every field is generated from a fixed seed.
+  * double gyre (2D, analytic) on [0,2] x [0,1];
+  * Fourier-mode fields (2D / 3D): a sum of seeded random modes with a k^(-5/3) amplitude
+    spectrum, scaled to a target RMS, phases advected linearly in time;
+  * a temperature volume T = 290 K - 6.5 K/km * z + 2 K seeded noise.
+`SnapshotLoader` serves precomputed snapshots through pygranite's DataLoader interface
+(source/granite/DataLoader.hpp:26-81): windfield() returns snapshot k, step() advances k.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+# ----------------------------------------------------------------- double gyre (config 1)
+
+def double_gyre(nx=256, ny=128, n_snapshots=16, A=0.1, eps=0.25, omega=2 * math.pi / 10, dt=1.0,
+                lx=2.0, ly=1.0):
+    """u = -dpsi/dy, v = dpsi/dx with psi = A sin(pi f(x,t)) sin(pi y),
+    f = eps sin(wt) x^2 + (1 - 2 eps sin(wt)) x; nodes x_i = i*lx/nx, y_j = j*ly/ny."""
+    x = np.arange(nx, dtype=np.float64) * (lx / nx)
+    y = np.arange(ny, dtype=np.float64) * (ly / ny)
+    X, Y = np.meshgrid(x, y)  # (ny, nx)
+    snaps = []
+    for k in range(n_snapshots):
+        t = k * dt
+        a = eps * math.sin(omega * t)
+        b = 1.0 - 2.0 * eps * math.sin(omega * t)
+        f = a * X * X + b * X
+        dfdx = 2.0 * a * X + b
+        u = -math.pi * A * np.sin(math.pi * f) * np.cos(math.pi * Y)
+        v = math.pi * A * np.cos(math.pi * f) * np.sin(math.pi * Y) * dfdx
+        snaps.append([u.astype(np.float32), v.astype(np.float32)])
+    return snaps
+
+
+def uniform_seeds(n, seed, lo, hi):
+    """n points uniform in the box [lo, hi) (numpy PCG64 generator with the given seed)."""
+    rng = np.random.default_rng(seed)
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    return (lo + rng.random((n, lo.size)) * (hi - lo)).astype(np.float32)
+
+
+# ----------------------------------------------------------------- Fourier-mode fields
+
+class FourierField:
+    """Sum of `n_modes` random plane waves per component, amplitude ~ |k|^(-5/3).
+
+    shape = (nz, ny, nx) for 3D or (ny, nx) for 2D; spacing in metres per axis (same order).
+    |k| is log-uniform between 2*pi/L_max and 2*pi/(4*dx); phases advance as -k.U t with
+    U = `advect` (m/s).  Each component is scaled so its RMS over the grid at t = 0 equals
+    `rms[c]`.  Snapshots are evaluated as a rank-n_modes separable product, so a snapshot
+    costs one small complex matrix product per component.
+    """
+
+    def __init__(self, shape, spacing, n_modes=32, seed=0, rms=(7.0710678, 7.0710678, 0.1),
+                 advect=(5.0, 3.0, 0.0), dtype=np.float32):
+        self.shape = tuple(shape)
+        self.dim = len(shape)
+        self.spacing = tuple(float(s) for s in spacing)
+        self.dtype = dtype
+        rng = np.random.default_rng(seed)
+        axes = [np.arange(n) * d for n, d in zip(self.shape, self.spacing)]  # z,y,x order
+        extent = max(n * d for n, d in zip(self.shape, self.spacing))
+        dmin = min(d for d in self.spacing[-2:])
+        kmin, kmax = 2 * math.pi / extent, 2 * math.pi / (4 * dmin)
+        adv = np.asarray(advect[: self.dim][::-1] if self.dim == 3 else advect[:2][::-1], np.float64)
+        self.comps = []
+        for c in range(self.dim):
+            kmag = np.exp(rng.uniform(math.log(kmin), math.log(kmax), n_modes))
+            direction = rng.normal(size=(n_modes, self.dim))
+            if self.dim == 3:
+                direction[:, 0] *= 0.25  # flatter modes in the vertical
+            direction /= np.linalg.norm(direction, axis=1, keepdims=True)
+            kvec = direction * kmag[:, None]           # (modes, dim) in axis order (z,y,x)
+            amp = kmag ** (-5.0 / 3.0)
+            phase0 = rng.uniform(0, 2 * math.pi, n_modes)
+            omega = kvec @ adv
+            factors = [np.exp(1j * np.outer(kvec[:, a], axes[a])) for a in range(self.dim)]
+            self.comps.append(dict(amp=amp, phase0=phase0, omega=omega, factors=factors, scale=1.0))
+        for c in range(self.dim):
+            r = float(np.sqrt(np.mean(self._eval(c, 0.0).astype(np.float64) ** 2)))
+            self.comps[c]["scale"] = (rms[c] / r) if r > 0 else 0.0
+
+    def _eval(self, c, t):
+        m = self.comps[c]
+        coef = m["amp"] * np.exp(1j * (m["phase0"] - m["omega"] * t))  # (modes,)
+        f = m["factors"]
+        if self.dim == 3:
+            fz, fy, fx = f
+            a = (coef[:, None] * fz).T                     # (nz, modes)
+            b = (fy[:, :, None] * fx[:, None, :]).reshape(len(coef), -1)   # (modes, ny*nx)
+            val = (a @ b).real.reshape(self.shape)
+        else:
+            fy, fx = f
+            a = (coef[:, None] * fy).T                     # (ny, modes)
+            val = (a @ fx).real
+        return (val * m.get("scale", 1.0)).astype(self.dtype)
+
+    def snapshot(self, t):
+        return [self._eval(c, t) for c in range(self.dim)]
+
+
+def temperature(shape, spacing_z, seed=1):
+    """T = 290 - 6.5e-3 * z + 2 * N(0,1) noise, z = iz * spacing_z (metres)."""
+    nz = shape[0]
+    rng = np.random.default_rng(seed)
+    z = (np.arange(nz, dtype=np.float64) * spacing_z)[:, None, None]
+    return (290.0 - 6.5e-3 * z + 2.0 * rng.standard_normal(shape)).astype(np.float32)
+
+
+# ----------------------------------------------------------------- loader
+
+class SnapshotSource:
+    """Precomputed snapshots plus optional volumes / constants / uplift per snapshot."""
+
+    def __init__(self, wind, volumes=None, constants=None, uplift=None):
+        self.wind = wind
+        self.volumes = volumes or []
+        self.constants = constants or []
+        self.uplift = uplift or []
+
+
+def make_loader(base_cls, source: SnapshotSource):
+    """A DataLoader subclass of `base_cls` (pygranite's DataLoader) serving `source`."""
+
+    class SnapshotLoader(base_cls):
+        def __init__(self):
+            base_cls.__init__(self)
+            self.k = 0
+            self.calls = 0
+
+        def step(self):
+            self.calls += 1
+            if self.k + 1 < len(source.wind):
+                self.k += 1
+                return True
+            return False
+
+        def windfield(self):
+            return source.wind[self.k]
+
+        def additionalVolumes(self):
+            if not source.volumes:
+                return {}
+            return source.volumes[min(self.k, len(source.volumes) - 1)]
+
+        def constants(self):
+            if not source.constants:
+                return {}
+            return source.constants[min(self.k, len(source.constants) - 1)]
+
+        def uplift(self):
+            if not source.uplift:
+                return np.zeros((0,), np.float32)
+            return source.uplift[min(self.k, len(source.uplift) - 1)]
+
+    return SnapshotLoader()
+
+
+# ----------------------------------------------------------------- benchmark configurations
+
+def config1(n_particles=10_000, n_snapshots=16):
+    """Plain 2D Euler FP32: double gyre on 256 x 128 over [0,2] x [0,1], h = 0.01 x 1000 steps."""
+    settings = dict(Space=1, Integrator=0, WindfieldMode=1, DeltaT=0.01, DataTimeDistance=1.0,
+                    GridScale=[2.0 / 256, 1.0 / 128], Offset=[0.0, 0.0], SaveInterval=1,
+                    BorderMode=0, CurvatureMode=0, MaximumSimulationTime=10.0)
+    src = SnapshotSource(double_gyre(256, 128, n_snapshots))
+    seeds = uniform_seeds(n_particles, 0, [0.0, 0.0], [2.0, 1.0])
+    return settings, src, seeds
+
+
+def config2(n_particles=1_000_000, n_snapshots=201, grid=(64, 192, 192), steps=2000, seed=0):
+    """Plain 3D RK4 FP32 on a Fourier field (1 km x 1 km x 250 m), 600 s snapshots, h = 60 s,
+    TotalCurvature, a constant temperature volume and the expression sqrt(u*u+v*v)*T."""
+    nz, ny, nx = grid
+    field = FourierField(grid, (250.0, 1000.0, 1000.0), n_modes=32, seed=seed)
+    wind = [field.snapshot(600.0 * k) for k in range(n_snapshots)]
+    T = temperature(grid, 250.0, seed=seed + 1)
+    settings = dict(Space=0, Integrator=1, WindfieldMode=1, DeltaT=60.0, DataTimeDistance=600.0,
+                    GridScale=[1000.0, 1000.0, 250.0], Offset=[0.0, 0.0, 0.0], SaveInterval=10,
+                    BorderMode=0, CurvatureMode=1, MaximumSimulationTime=60.0 * steps,
+                    AdditionalVolumeMode=1, AdditionalCompute=["sqrt(u*u+v*v)*T"])
+    src = SnapshotSource(wind, volumes=[{"T": T}])
+    seeds = uniform_seeds(n_particles, seed, [0.0, 0.0, 0.0], [nx * 1000.0, ny * 1000.0, nz * 250.0 / 2])
+    return settings, src, seeds
+
+
+def apply_settings(obj, settings: dict, enums=None):
+    """Sets reference-named fields on a pygranite IntegratorSettings instance."""
+    for k, v in settings.items():
+        if enums is not None and k in enums:
+            v = enums[k](v)
+        setattr(obj, k, v)
+    return obj
