@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--sim-steps", type=int, default=2000)
     p.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
     p.add_argument("--steps-per-launch", type=int, default=0)
+    p.add_argument("--sort-interval", type=int, default=1,
+                   help="launches between compaction / Morton re-sorts of the live particles (0 = off)")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -198,7 +200,7 @@ def main():
 
     # ---------------- device-resident engine: every snapshot in the ring before timing
     cs = capi.settings_from_reference(settings, ring_slots=n_snap, storage=storage, device=local,
-                                      steps_per_launch=args.steps_per_launch)
+                                      steps_per_launch=args.steps_per_launch, sort_interval=args.sort_interval)
     eng = capi.Engine(cs)
     eng.set_seeds(seeds)
     for k, snap in enumerate(src.wind):
@@ -254,6 +256,8 @@ def main():
         s = W.apply_settings(pg.IntegratorSettings(), settings, enums)
         s.WindStorage = [pg.WindStorage.Float32, pg.WindStorage.BFloat16, pg.WindStorage.Float16][storage]
         s.Device = local
+        s.SortInterval = args.sort_interval
+        s.StepsPerLaunch = args.steps_per_launch
         h2d = seeds.nbytes + sum(p.nbytes for snap in src.wind for p in snap) + src.volumes[0]["T"].nbytes
         e_ps, e_s, d2h = 0, 0.0, 0
         for k in range(1 + args.e2e_steps):
@@ -312,7 +316,8 @@ def main():
         "config": {"workload": WORKLOAD, "particles_per_gpu": args.particles, "sim_steps": args.sim_steps,
                    "snapshots": n_snap, "grid": [192, 192, 64], "storage": args.storage,
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (201 snapshots, 7.6 GB ring)",
-                   "records": int(info.records), "steps_run": int(info.steps)},
+                   "records": int(info.records), "steps_run": int(info.steps),
+                   "sort_interval": args.sort_interval, "steps_per_launch": args.steps_per_launch},
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
         "gpu_launches": int(launches + aux), "wall_s": wall,
     }

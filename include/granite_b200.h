@@ -112,6 +112,22 @@ typedef struct gr_stats {
     int64_t d2h_bytes;
 } gr_stats;
 
+/* Step plan of a run whose loader never runs dry: counts and, if the arrays are non-null,
+ * per step the window index, flags (1 = record after the step, 2 = data.Time > 0 at its
+ * start) and the three float32 time weights.  Restates the bookkeeping of computeLoop_ /
+ * computeLoopGPU_ (TrajectoryIntegrator.tpp:778-995); needs no GPU, so callers can size
+ * result buffers before a run. */
+typedef struct gr_plan_info {
+    int64_t steps;
+    int64_t windows;
+    int64_t records;             /* position records incl. the seed record */
+    int64_t curvature_records;
+    int64_t info_records;
+} gr_plan_info;
+
+int gr_plan(const gr_settings *settings, gr_plan_info *out, int64_t capacity, int64_t *window,
+            int32_t *flags, float *weights);
+
 /* Create / destroy.  Replaces the TrajectoryIntegrator constructor's resource setup
  * (TrajectoryIntegrator.hpp:138-147) and destructor (TrajectoryIntegrator.cpp:362-422). */
 int gr_create(const gr_settings *settings, gr_engine **out);

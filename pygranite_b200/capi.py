@@ -23,7 +23,7 @@ EXPORTS = [
     "gr_result_info_get", "gr_stats_get", "gr_fetch_positions", "gr_fetch_status",
     "gr_fetch_lengths", "gr_fetch_total_curvature", "gr_fetch_curvatures",
     "gr_fetch_volume_info", "gr_fetch_compute_info", "gr_load_windfield_device",
-    "gr_set_seeds_device",
+    "gr_set_seeds_device", "gr_plan",
 ]
 
 
@@ -54,6 +54,11 @@ class Stats(ctypes.Structure):
     _fields_ = [("kernel_ms", ctypes.c_double), ("run_ms", ctypes.c_double), ("launches", ctypes.c_int64),
                 ("aux_launches", ctypes.c_int64), ("particle_steps", ctypes.c_int64),
                 ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64)]
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int64), ("windows", ctypes.c_int64), ("records", ctypes.c_int64),
+                ("curvature_records", ctypes.c_int64), ("info_records", ctypes.c_int64)]
 
 
 LOADER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64)
@@ -94,6 +99,8 @@ def lib():
             "gr_fetch_curvatures": (ctypes.c_int, [P, FP, I64]),
             "gr_fetch_volume_info": (ctypes.c_int, [P, I32, FP, I64]),
             "gr_fetch_compute_info": (ctypes.c_int, [P, I32, FP, I64]),
+            "gr_plan": (ctypes.c_int, [ctypes.POINTER(Settings), ctypes.POINTER(PlanInfo), I64,
+                                       ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32), FP]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -149,6 +156,22 @@ def settings_from_reference(d: dict, **extra) -> Settings:
              save_interval=d.get("SaveInterval", 1))
     m.update(extra)
     return default_settings(**m)
+
+
+def plan(settings: Settings, with_steps=True):
+    """gr_plan: counts and (optionally) per-step window, flags and float32 time weights."""
+    info = PlanInfo()
+    _check(lib().gr_plan(ctypes.byref(settings), ctypes.byref(info), 0, None, None, None))
+    if not with_steps:
+        return info, None
+    n = info.steps
+    win = np.zeros(max(1, n), np.int64)
+    flags = np.zeros(max(1, n), np.int32)
+    w = np.zeros((max(1, n), 3), np.float32)
+    _check(lib().gr_plan(ctypes.byref(settings), ctypes.byref(info), n,
+                         win.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                         flags.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _fp(w)))
+    return info, dict(window=win[:n], flags=flags[:n], weights=w[:n])
 
 
 def evaluate_expression(code, ref, volume_names=(), constant_names=(), dim=3, curvature_mode=0):

@@ -24,6 +24,7 @@
 
 #include "../../include/granite_b200.h"
 #include "expr.h"
+#include "compact.cuh"
 #include "granite_kernels.cuh"
 #include "schedule.h"
 
@@ -125,7 +126,8 @@ __global__ void seed_record_kernel(const float *__restrict__ seeds, int64_t n, i
 template <int DIM>
 __global__ void save_state_kernel(const __grid_constant__ KParams P, int32_t rec, int32_t crec, int32_t irec,
                                   int write_curv) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t n = P.n_dev ? (int64_t)*P.n_dev : P.n;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t pid = P.id[i];
         float *hp = P.hpos + (pid * P.L + rec) * DIM;
         hp[0] = P.px[i];
@@ -141,7 +143,8 @@ __global__ void save_state_kernel(const __grid_constant__ KParams P, int32_t rec
 // State (slot order) -> final per-particle outputs (particle order).
 __global__ void finalize_kernel(const __grid_constant__ KParams P, int32_t *status_out, float *length_out,
                                 float *tc_out) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t n = P.n_dev ? (int64_t)*P.n_dev : P.n;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t pid = P.id[i];
         status_out[pid] = P.status[i];
         if (P.abort_mode != 0) length_out[pid] = P.length[i];
@@ -222,8 +225,20 @@ struct gr_engine {
     // particles
     int64_t n = 0;
     DevBuf<float> seeds;               // AoS n x dim
-    DevBuf<float> px, py, pz, qx, qy, qz, kx, ky, kz, lx, ly, lz, length, tc, curv, volc, cmpc;
-    DevBuf<int32_t> status, id;
+    struct State {
+        DevBuf<float> px, py, pz, qx, qy, qz, kx, ky, kz, lx, ly, lz, length, tc, curv, volc, cmpc;
+        DevBuf<int32_t> status, id, retire;
+    };
+    State st[2];                       // double-buffered live state (compaction swaps)
+    State ret;                         // retired particles (frozen state)
+    int cur = 0;
+    bool compacting = false;
+    DevBuf<int32_t> d_counts;          // [0] live, [1] live after a pass, [2] retired
+    int32_t *h_live = nullptr;         // pinned copy of the live count
+    cudaEvent_t live_ready = nullptr;
+    DevBuf<int32_t> c_key, c_hist, c_bintab;
+    int bx = 4, by = 4, bz = 2, nbx = 0, nby = 0, nbz = 0, nbins = 0;
+    DevBuf<int32_t> crec_of_rec;
     DevBuf<float> hpos, hcurv, hvol, hcmp;
     DevBuf<int32_t> out_status;
     DevBuf<float> out_length, out_tc;
@@ -246,6 +261,8 @@ struct gr_engine {
         for (auto e : slot_ready) cudaEventDestroy(e);
         for (auto e : ev_pool) cudaEventDestroy(e);
         if (h_counters) cudaFreeHost(h_counters);
+        if (h_live) cudaFreeHost(h_live);
+        if (live_ready) cudaEventDestroy(live_ready);
         if (cs) cudaStreamDestroy(cs);
         if (xs) cudaStreamDestroy(xs);
     }
@@ -567,6 +584,50 @@ int gr_compile_expression(gr_engine *e, int32_t index, const char *code, const c
     return GR_OK;
 }
 
+int gr_plan(const gr_settings *settings, gr_plan_info *out, int64_t capacity, int64_t *window, int32_t *flags,
+            float *weights) {
+    if (!settings || !out) return USER_ERR("null argument >");
+    const gr_settings &s = *settings;
+    if (s.delta_t <= 0.f || !std::isfinite(s.delta_t)) return USER_ERR("DeltaT must be positive. >");
+    if (s.data_time_distance <= 0.f || !std::isfinite(s.data_time_distance))
+        return USER_ERR("DataTimeDistance must be positive. >");
+    if (!std::isfinite(s.maximum_simulation_time) || s.maximum_simulation_time / s.delta_t > 5.0e8f)
+        return USER_ERR("Too many integration steps requested. >");
+    ScheduleInput si;
+    const int up = s.space == 0 ? s.uplift_mode : 0;
+    si.wind_dynamic = s.windfield_mode == 1;
+    si.dyn_any = si.wind_dynamic || up == 2 || s.volume_mode == 2 || s.constants_mode == 2;
+    si.delta_t = s.delta_t;
+    si.data_time_distance = s.data_time_distance;
+    si.maximum_simulation_time = s.maximum_simulation_time;
+    si.save_interval = s.save_interval;
+    si.time_mode = s.time_mode;
+    const Schedule sc = build_schedule(si);
+    const int64_t n = (int64_t)sc.steps.size();
+    int64_t saves = 0, csaves = 0;
+    for (int64_t k = 0; k < n; ++k) {
+        const HostStep &h = sc.steps[k];
+        saves += h.save;
+        csaves += h.save && h.time_pos;
+        if (k < capacity) {
+            if (window) window[k] = h.window;
+            if (flags) flags[k] = (h.save ? 1 : 0) | (h.time_pos ? 2 : 0);
+            if (weights) {
+                weights[3 * k] = h.t0;
+                weights[3 * k + 1] = h.t1;
+                weights[3 * k + 2] = h.t2;
+            }
+        }
+    }
+    const bool final_rec = s.save_interval == 0;
+    out->steps = n;
+    out->windows = (int64_t)sc.window_begin.size() - 1;
+    out->records = 1 + saves + (final_rec ? 1 : 0);
+    out->info_records = saves + (final_rec ? 1 : 0);
+    out->curvature_records = s.curvature_mode == 3 ? csaves + ((final_rec && n > 0) ? 1 : 0) : 0;
+    return GR_OK;
+}
+
 int gr_expression_evaluate(const char *code, const char *const *volume_names, int32_t n_volumes,
                            const char *const *constant_names, int32_t n_constants, int32_t dim,
                            int32_t curvature_mode, const float *ref, float *out) {
@@ -605,38 +666,107 @@ int gr_set_seeds_device(gr_engine *e, const float *pos, int64_t n, int32_t dim) 
 
 namespace {
 
+int alloc_set(gr_engine *e, gr_engine::State &S, bool retired) {
+    const size_t N = (size_t)e->n;
+    const int cm = e->s.curvature_mode;
+    CK(S.px.alloc(N)); CK(S.py.alloc(N));
+    if (e->dim == 3) CK(S.pz.alloc(N));
+    CK(S.status.alloc(N)); CK(S.id.alloc(N));
+    if (retired) CK(S.retire.alloc(N));
+    if (!retired && (cm == 1 || cm == 3)) { CK(S.qx.alloc(N)); CK(S.qy.alloc(N)); CK(S.qz.alloc(N)); }
+    if (!retired && e->s.compensated) { CK(S.kx.alloc(N)); CK(S.ky.alloc(N)); CK(S.kz.alloc(N)); }
+    if (!retired && cm == 2) { CK(S.lx.alloc(N)); CK(S.ly.alloc(N)); CK(S.lz.alloc(N)); }
+    CK(S.length.alloc(N)); CK(S.tc.alloc(N)); CK(S.curv.alloc(N));
+    const int nv = std::max(1, e->nvol), ne = std::max(1, e->nexpr);
+    CK(S.volc.alloc(N * nv)); CK(S.cmpc.alloc(N * ne));
+    return GR_OK;
+}
+
 int alloc_state(gr_engine *e) {
     const int64_t n = e->n;
     const size_t N = (size_t)n;
-    CK(e->px.alloc(N)); CK(e->py.alloc(N)); CK(e->pz.alloc(N));
-    CK(e->status.alloc(N)); CK(e->id.alloc(N));
-    const int cm = e->s.curvature_mode;
-    if (cm == 1 || cm == 3) { CK(e->qx.alloc(N)); CK(e->qy.alloc(N)); CK(e->qz.alloc(N)); }
+    e->cur = 0;
+    int rc = alloc_set(e, e->st[0], false);
+    if (rc) return rc;
+    gr_engine::State &S = e->st[0];
     if (e->s.compensated) {
-        CK(e->kx.alloc(N)); CK(e->ky.alloc(N)); CK(e->kz.alloc(N));
-        CK(cudaMemsetAsync(e->kx.p, 0, N * 4, e->cs)); CK(cudaMemsetAsync(e->ky.p, 0, N * 4, e->cs));
-        CK(cudaMemsetAsync(e->kz.p, 0, N * 4, e->cs));
+        CK(cudaMemsetAsync(S.kx.p, 0, N * 4, e->cs)); CK(cudaMemsetAsync(S.ky.p, 0, N * 4, e->cs));
+        CK(cudaMemsetAsync(S.kz.p, 0, N * 4, e->cs));
     }
-    if (cm == 2) {
-        CK(e->lx.alloc(N)); CK(e->ly.alloc(N)); CK(e->lz.alloc(N));
-        CK(cudaMemsetAsync(e->lx.p, 0, N * 4, e->cs)); CK(cudaMemsetAsync(e->ly.p, 0, N * 4, e->cs));
-        CK(cudaMemsetAsync(e->lz.p, 0, N * 4, e->cs));
+    if (e->s.curvature_mode == 2) {
+        CK(cudaMemsetAsync(S.lx.p, 0, N * 4, e->cs)); CK(cudaMemsetAsync(S.ly.p, 0, N * 4, e->cs));
+        CK(cudaMemsetAsync(S.lz.p, 0, N * 4, e->cs));
     }
-    CK(e->length.alloc(N)); CK(e->tc.alloc(N)); CK(e->curv.alloc(N));
-    CK(cudaMemsetAsync(e->length.p, 0, N * 4, e->cs));
-    CK(cudaMemsetAsync(e->tc.p, 0, N * 4, e->cs));
-    CK(cudaMemsetAsync(e->curv.p, 0, N * 4, e->cs));
+    CK(cudaMemsetAsync(S.length.p, 0, N * 4, e->cs));
+    CK(cudaMemsetAsync(S.tc.p, 0, N * 4, e->cs));
+    CK(cudaMemsetAsync(S.curv.p, 0, N * 4, e->cs));
     const int nv = std::max(1, e->nvol), ne = std::max(1, e->nexpr);
-    CK(e->volc.alloc(N * nv)); CK(e->cmpc.alloc(N * ne));
-    CK(cudaMemsetAsync(e->volc.p, 0, N * nv * 4, e->cs));
-    CK(cudaMemsetAsync(e->cmpc.p, 0, N * ne * 4, e->cs));
+    CK(cudaMemsetAsync(S.volc.p, 0, N * nv * 4, e->cs));
+    CK(cudaMemsetAsync(S.cmpc.p, 0, N * ne * 4, e->cs));
     CK(e->out_status.alloc(N)); CK(e->out_length.alloc(N)); CK(e->out_tc.alloc(N));
+    e->compacting = e->s.sort_interval > 0;
+    CK(e->d_counts.alloc(4));
+    {
+        const int32_t init[4] = {(int32_t)n, (int32_t)n, 0, 0};
+        CK(cudaMemcpyAsync(e->d_counts.p, init, sizeof init, cudaMemcpyHostToDevice, e->cs));
+    }
+    if (e->compacting) {
+        rc = alloc_set(e, e->st[1], false);
+        if (rc) return rc;
+        rc = alloc_set(e, e->ret, true);
+        if (rc) return rc;
+        CK(e->c_key.alloc(N));
+        if (!e->h_live) CK(cudaMallocHost(&e->h_live, sizeof(int32_t)));
+        *e->h_live = (int32_t)n;
+        if (!e->live_ready) CK(cudaEventCreateWithFlags(&e->live_ready, cudaEventDisableTiming));
+        // Morton-ranked brick table (bricks of bx x by x bz nodes)
+        e->bx = 4; e->by = 4; e->bz = e->dim == 3 ? 2 : 1;
+        for (;;) {
+            e->nbx = (int)((e->nx + e->bx - 1) / e->bx);
+            e->nby = (int)((e->ny + e->by - 1) / e->by);
+            e->nbz = (int)((e->nz + e->bz - 1) / e->bz);
+            if ((int64_t)e->nbx * e->nby * e->nbz <= (1 << 20) && e->nbx <= 1024 && e->nby <= 1024 && e->nbz <= 1024) break;
+            e->bx *= 2; e->by *= 2; if (e->dim == 3) e->bz *= 2;
+        }
+        e->nbins = e->nbx * e->nby * e->nbz;
+        auto spread = [](uint32_t v) {
+            uint64_t x = v & 0x3ff;
+            x = (x | (x << 16)) & 0x030000FF;
+            x = (x | (x << 8)) & 0x0300F00F;
+            x = (x | (x << 4)) & 0x030C30C3;
+            x = (x | (x << 2)) & 0x09249249;
+            return x;
+        };
+        std::vector<std::pair<uint64_t, int32_t>> codes((size_t)e->nbins);
+        for (int z = 0; z < e->nbz; ++z)
+            for (int y = 0; y < e->nby; ++y)
+                for (int x = 0; x < e->nbx; ++x) {
+                    const int32_t lin = (z * e->nby + y) * e->nbx + x;
+                    codes[lin] = {spread(x) | (spread(y) << 1) | (spread(z) << 2), lin};
+                }
+        std::sort(codes.begin(), codes.end());
+        std::vector<int32_t> tab((size_t)e->nbins);
+        for (int32_t r = 0; r < e->nbins; ++r) tab[codes[r].second] = r;
+        CK(e->c_bintab.alloc(tab.size()));
+        CK(cudaMemcpy(e->c_bintab.p, tab.data(), tab.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+        CK(e->c_hist.alloc((size_t)e->nbins + 1));
+    }
     const int threads = 256;
-    seed_kernel<<<grid_for(n, threads), threads, 0, e->cs>>>(e->seeds.p, n, e->dim, e->px.p, e->py.p, e->pz.p,
-                                                             e->status.p, e->id.p);
+    seed_kernel<<<grid_for(n, threads), threads, 0, e->cs>>>(e->seeds.p, n, e->dim, S.px.p, S.py.p, S.pz.p,
+                                                             S.status.p, S.id.p);
     CK(cudaGetLastError());
     e->stats.aux_launches++;
     return GR_OK;
+}
+
+StateView view_of(gr_engine::State &S, int64_t stride) {
+    StateView v;
+    v.px = S.px.p; v.py = S.py.p; v.pz = S.pz.p; v.qx = S.qx.p; v.qy = S.qy.p; v.qz = S.qz.p;
+    v.kx = S.kx.p; v.ky = S.ky.p; v.kz = S.kz.p; v.lx = S.lx.p; v.ly = S.ly.p; v.lz = S.lz.p;
+    v.length = S.length.p; v.tc = S.tc.p; v.curv = S.curv.p; v.volc = S.volc.p; v.cmpc = S.cmpc.p;
+    v.status = S.status.p; v.id = S.id.p; v.retire = S.retire.p;
+    v.stride = stride;
+    return v;
 }
 
 KParams make_params(gr_engine *e) {
@@ -652,13 +782,15 @@ KParams make_params(gr_engine *e) {
     P.wind = e->wind.p; P.wind_stride = e->wind_stride;
     P.vol = e->vol.p; P.vol_plane = e->nodes;
     P.cons = e->cons.p; P.lift = e->lift.p; P.topo = e->topo.p;
-    P.px = e->px.p; P.py = e->py.p; P.pz = e->pz.p;
-    P.qx = e->qx.p; P.qy = e->qy.p; P.qz = e->qz.p;
-    P.kx = e->kx.p; P.ky = e->ky.p; P.kz = e->kz.p;
-    P.lx = e->lx.p; P.ly = e->ly.p; P.lz = e->lz.p;
-    P.status = e->status.p; P.length = e->length.p; P.tc = e->tc.p; P.curv = e->curv.p;
-    P.volc = e->volc.p; P.cmpc = e->cmpc.p; P.id = e->id.p;
+    gr_engine::State &S = e->st[e->cur];
+    P.px = S.px.p; P.py = S.py.p; P.pz = S.pz.p;
+    P.qx = S.qx.p; P.qy = S.qy.p; P.qz = S.qz.p;
+    P.kx = S.kx.p; P.ky = S.ky.p; P.kz = S.kz.p;
+    P.lx = S.lx.p; P.ly = S.ly.p; P.lz = S.lz.p;
+    P.status = S.status.p; P.length = S.length.p; P.tc = S.tc.p; P.curv = S.curv.p;
+    P.volc = S.volc.p; P.cmpc = S.cmpc.p; P.id = S.id.p;
     P.n = e->n; P.n_state = e->n; P.n_total = e->n;
+    P.n_dev = e->compacting ? e->d_counts.p : nullptr;
     P.hpos = e->hpos.p; P.hcurv = e->hcurv.p; P.hvol = e->hvol.p; P.hcmp = e->hcmp.p;
     P.L = e->L; P.Lc = e->Lc; P.Li = e->Li;
     P.sched = e->d_sched.p;
@@ -686,6 +818,88 @@ KParams make_params(gr_engine *e) {
     P.prog = e->d_prog.p;
     P.counters = e->counters.p;
     return P;
+}
+
+// One compaction / re-sort pass over the live prefix (compact.cuh).
+int compact_pass(gr_engine *e, int32_t rec_now) {
+    CompactParams C;
+    std::memset(&C, 0, sizeof C);
+    const int64_t N = e->n;
+    C.src = view_of(e->st[e->cur], N);
+    C.dst = view_of(e->st[1 - e->cur], N);
+    C.ret = view_of(e->ret, N);
+    C.key = e->c_key.p;
+    C.hist = e->c_hist.p;
+    C.bintab = e->c_bintab.p;
+    C.n_act = e->d_counts.p;
+    C.n_new = e->d_counts.p + 1;
+    C.n_ret = e->d_counts.p + 2;
+    for (int d = 0; d < 3; ++d) {
+        C.off[d] = e->off[d];
+        C.inv_scale[d] = e->inv_scale[d];
+    }
+    C.nx = (int32_t)e->nx; C.ny = (int32_t)e->ny; C.nz = (int32_t)e->nz; C.dim = e->dim;
+    C.bx = e->bx; C.by = e->by; C.bz = e->bz; C.nbx = e->nbx; C.nby = e->nby; C.nbz = e->nbz; C.nbins = e->nbins;
+    const int cm = e->s.curvature_mode;
+    C.nvol = (e->nvol > 0 && e->s.volume_mode != 0) ? e->nvol : 0;
+    C.nexpr = e->nexpr;
+    C.curv_prev = cm == 1 || cm == 3;
+    C.compensated = e->s.compensated ? 1 : 0;
+    C.fast_curv = cm == 2;
+    C.abort_on = e->s.abort_mode != 0;
+    C.curv_on = cm != 0;
+    C.curv_ind = cm == 3;
+    C.rec_now = rec_now;
+    const int threads = 256;
+    const int blocks = grid_for(N, threads);
+    CK(cudaMemsetAsync(e->c_hist.p, 0, ((size_t)e->nbins + 1) * sizeof(int32_t), e->cs));
+    bin_kernel<<<blocks, threads, 0, e->cs>>>(C);
+    scan_kernel<<<1, 1024, 0, e->cs>>>(C);
+    scatter_kernel<<<blocks, threads, 0, e->cs>>>(C);
+    commit_kernel<<<1, 1, 0, e->cs>>>(C);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(e->h_live, e->d_counts.p, sizeof(int32_t), cudaMemcpyDeviceToHost, e->cs));
+    CK(cudaEventRecord(e->live_ready, e->cs));
+    e->cur = 1 - e->cur;
+    e->stats.aux_launches += 4;
+    return GR_OK;
+}
+
+// Records a retired particle would have written after it left the live set: its frozen
+// state, for records retire .. rec_end-1.
+__global__ void fill_forward_kernel(const __grid_constant__ KParams P, StateView R, const int32_t *n_ret,
+                                    const int32_t *crec_of_rec, int32_t rec_end) {
+    const int64_t nr = *n_ret;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nr; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pid = R.id[j];
+        const float x = R.px[j], y = R.py[j], z = P.dim == 3 ? R.pz[j] : 0.f;
+        for (int32_t r = R.retire[j]; r < rec_end; ++r) {
+            float *hp = P.hpos + (pid * P.L + r) * P.dim;
+            hp[0] = x;
+            hp[1] = y;
+            if (P.dim == 3) hp[2] = z;
+            const int32_t irec = r - 1;
+            if (irec >= 0) {
+                if (P.volume_mode != 0)
+                    for (int k = 0; k < P.nvol; ++k) P.hvol[((int64_t)k * P.n_total + pid) * P.Li + irec] = R.volc[k * R.stride + j];
+                for (int k = 0; k < P.nexpr; ++k) P.hcmp[((int64_t)k * P.n_total + pid) * P.Li + irec] = R.cmpc[k * R.stride + j];
+            }
+            const int32_t cr = crec_of_rec[r];
+            if (P.curvature_mode == 3 && cr >= 0) P.hcurv[pid * P.Lc + cr] = R.curv[j];
+        }
+    }
+}
+
+// Final per-particle outputs of the retired store.
+__global__ void finalize_retired_kernel(StateView R, const int32_t *n_ret, int abort_on, int curv_on, int32_t *status_out,
+                                        float *length_out, float *tc_out) {
+    const int64_t nr = *n_ret;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nr; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pid = R.id[j];
+        status_out[pid] = R.status[j];
+        if (abort_on) length_out[pid] = R.length[j];
+        if (curv_on) tc_out[pid] = R.tc[j];
+    }
 }
 
 using KernelFn = void (*)(const KParams);
@@ -858,11 +1072,29 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
         if (e->wind_holds[k] >= 0 || e->vol_holds[k] >= 0 || e->cons_holds[k] >= 0 || e->lift_holds[k] >= 0)
             CK(cudaStreamWaitEvent(e->cs, e->slot_ready[k], 0));
 
-    const int64_t spl = s.steps_per_launch > 0 ? s.steps_per_launch : (int64_t)1 << 40;
+    // records written before step k: 1 + saves in [0, k)
+    std::vector<int32_t> rec_before((size_t)nsteps + 1, 1);
+    for (int64_t k = 0; k < nsteps; ++k) rec_before[k + 1] = rec_before[k] + (sched.steps[k].save ? 1 : 0);
+    int64_t spl = s.steps_per_launch > 0 ? s.steps_per_launch : (int64_t)1 << 40;
+    if (e->compacting && s.steps_per_launch <= 0 && nwin > 0)
+        spl = std::max<int64_t>(1, sched.window_begin[1] - sched.window_begin[0]);   // one window per launch
     const int64_t gmax = std::max(1, e->K - 1);
     int64_t executed = 0, windows_run = 0;
+    int64_t launches_since_sort = 0;
     bool stop = false;
     int64_t w = 0;
+    // after a launch that ended before step k_end: maybe retire / re-sort (compact.cuh)
+    auto after_launch = [&](int64_t k_end) -> int {
+        if (!e->compacting || k_end >= nsteps) return 0;
+        if (++launches_since_sort < s.sort_interval) return 0;
+        launches_since_sort = 0;
+        int q = compact_pass(e, rec_before[k_end]);
+        if (q) return q;
+        r.P = make_params(e);
+        // live count of the last completed pass: an upper bound of the current one
+        r.P.n = std::max<int64_t>(1, *(volatile int32_t *)e->h_live);
+        return 0;
+    };
     auto launch_range = [&](int64_t b, int64_t t) -> int {
         if (s.minimum_alive > 0) {
             for (int64_t k = b; k < t; ++k) {
@@ -878,11 +1110,16 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
                 int q = launch_steps(r, k, k + 1);
                 if (q) return q;
                 ++executed;
+                q = after_launch(k + 1);
+                if (q) return q;
             }
             return 0;
         }
         for (int64_t k = b; k < t; k += spl) {
-            int q = launch_steps(r, k, std::min(t, k + spl));
+            const int64_t k1 = std::min(t, k + spl);
+            int q = launch_steps(r, k, k1);
+            if (q) return q;
+            q = after_launch(k1);
             if (q) return q;
         }
         executed += t - b;
@@ -935,8 +1172,18 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
             if (sched.steps[k].time_pos) ++crec_done;
         }
     KParams P = r.P;
+    std::vector<int32_t> crec_of_rec((size_t)e->L + 1, -1);
+    {
+        int64_t rr = 1, cc = 0;
+        for (int64_t k = 0; k < executed; ++k)
+            if (sched.steps[k].save) {
+                if (sched.steps[k].time_pos) crec_of_rec[rr] = (int32_t)cc++;
+                ++rr;
+            }
+    }
     if (s.save_interval == 0) {
         const bool tpos = executed > 0;   // data.Time > 0 after at least one step
+        if (tpos) crec_of_rec[rec_done] = (int32_t)crec_done;
         if (e->dim == 3)
             save_state_kernel<3><<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, (int32_t)rec_done, (int32_t)crec_done, (int32_t)irec_done, tpos);
         else
@@ -949,6 +1196,21 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
     }
     finalize_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, e->out_status.p, e->out_length.p, e->out_tc.p);
     CK(cudaGetLastError());
+    if (e->compacting) {
+        // retired particles: their later records repeat the frozen state
+        CK(e->crec_of_rec.alloc(crec_of_rec.size()));
+        CK(cudaMemcpyAsync(e->crec_of_rec.p, crec_of_rec.data(), crec_of_rec.size() * sizeof(int32_t),
+                           cudaMemcpyHostToDevice, e->cs));
+        const StateView R = view_of(e->ret, e->n);
+        fill_forward_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, R, e->d_counts.p + 2, e->crec_of_rec.p,
+                                                                     (int32_t)rec_done);
+        finalize_retired_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(R, e->d_counts.p + 2, s.abort_mode != 0,
+                                                                         s.curvature_mode != 0, e->out_status.p,
+                                                                         e->out_length.p, e->out_tc.p);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(e->cs));   // crec_of_rec (host vector) is read by the copy above
+        e->stats.aux_launches += 2;
+    }
     CK(cudaEventRecord(run_b, e->cs));
     CK(cudaMemcpyAsync(e->h_counters, e->counters.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->cs));
     CK(cudaStreamSynchronize(e->cs));

@@ -62,6 +62,7 @@ struct KParams {
     float *cmpc;                  // [4][n_state]
     const int32_t *id;            // original particle index
     int64_t n;                    // particles in this launch (prefix of the state arrays)
+    const int32_t *n_dev;         // if set: live prefix length on the device (<= n)
     int64_t n_state;              // stride of volc / cmpc
     int64_t n_total;              // original particle count (history / constants stride)
     // history, particle-major
@@ -357,7 +358,8 @@ __device__ __forceinline__ float eval_program(const Program *prog, const float (
 template <int DIM, bool RK4, typename W>
 __global__ void __launch_bounds__(256) advance_kernel(const __grid_constant__ KParams P) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < P.n;
+    const int64_t n_live = P.n_dev ? (int64_t)*P.n_dev : P.n;
+    const bool valid = i < n_live;
     int32_t st = valid ? P.status[i] : 1;
     bool alive = st == 0;
     const int64_t pid = valid ? (int64_t)P.id[i] : 0;

@@ -187,11 +187,15 @@ def test_transcendental_expressions_within_ulps():
     eng = H.run_engine(settings, wind, seeds)
     ref = H.run_oracle(settings, wind, seeds, precision="f32")
     H.assert_same(eng, ref, ("trajectories", "status", "curvatures"))
+    # CUDA's and glibc's float functions differ by a few ulp.  Each expression sums at most
+    # four terms of magnitude <= max(pi, |x|, |value|); tolerance: 4 terms x 4 ulp of that.
+    eps = np.finfo(np.float32).eps
+    pos = np.abs(eng["trajectories"][:, 1:, :]).max(axis=-1)
     for e in range(4):
         a, b = eng["compute_info"][e], ref["compute_info"][e]
-        # CUDA's and glibc's float functions differ by a few ulp: tolerance 4 ulp-relative
-        tol = 4 * np.finfo(np.float32).eps * np.maximum(1.0, np.abs(b))
-        assert np.all((np.abs(a - b) <= tol) | (np.isnan(a) & np.isnan(b))), e
+        tol = 16 * eps * np.maximum(np.maximum(np.pi, np.abs(b)), pos)
+        bad = ~((np.abs(a - b) <= tol) | (np.isnan(a) & np.isnan(b)))
+        assert not bad.any(), (e, np.abs(a - b)[bad][:5], tol[bad][:5])
 
 
 def test_fast_total_curvature_and_sphere_2d():
@@ -237,31 +241,84 @@ def test_loader_exhaustion_truncates_like_reference():
     assert ref["windows"] == 2 and eng["trajectories"].shape[1] == 1 + ref["steps"]
 
 
-@pytest.mark.parametrize("extra", [dict(StepsPerLaunch=1), dict(StepsPerLaunch=7), dict(BlockSize=32),
-                                   dict(BlockSize=256, RingSlots=8), dict(RingSlots=4, StepsPerLaunch=3)])
+LAUNCH_SHAPES = [dict(StepsPerLaunch=1), dict(StepsPerLaunch=7), dict(BlockSize=32),
+                 dict(BlockSize=256, RingSlots=8), dict(RingSlots=4, StepsPerLaunch=3),
+                 dict(SortInterval=1), dict(SortInterval=1, StepsPerLaunch=1), dict(SortInterval=2, StepsPerLaunch=3),
+                 dict(SortInterval=1, RingSlots=8, StepsPerLaunch=5)]
+
+
+@pytest.mark.parametrize("extra", LAUNCH_SHAPES)
 def test_launch_shape_does_not_change_results(extra):
+    """Launch granularity, block size, ring depth and compaction / re-sorting of the live
+    particles change nothing: every output stays bit-identical to the float32 oracle."""
     base, wind, seeds = problem3d(seed=2)
-    settings = dict(base, CurvatureMode=1)
-    ref = H.run_oracle(settings, wind, seeds, precision="f32")
-    eng = H.run_engine(settings, wind, seeds, **extra)
-    H.assert_same(eng, ref, ("trajectories", "status", "total_curvature"))
+    exprs = ["x + cv*2", "temp - z"]
+    vols = [{"temp": np.random.default_rng(4).standard_normal((12, 20, 24)).astype(np.float32)} for _ in wind]
+    for extra_settings in (dict(CurvatureMode=3, SaveInterval=2), dict(CurvatureMode=1, SaveInterval=0)):
+        settings = dict(base, AdditionalVolumeMode=1, AdditionalCompute=exprs, **extra_settings)
+        ref = H.run_oracle(settings, wind, seeds, volumes=vols, precision="f32")
+        eng = H.run_engine(settings, wind, seeds, volumes=vols, **extra)
+        H.assert_same(eng, ref, ("trajectories", "status", "total_curvature", "curvatures"))
+        assert np.array_equal(eng["volume_info"]["temp"], ref["volume_info"]["temp"])
+        for k in range(2):
+            assert np.array_equal(eng["compute_info"][k], ref["compute_info"][k])
+
+
+def test_compaction_with_minimum_alive_and_2d():
+    base, wind, seeds = problem2d(seed=6, n=2000)
+    wind = wind + rng_field((32, 48), 6, 78)
+    for settings in (dict(base, MinimumAliveParticles=1200, MaximumSimulationTime=40.0),
+                     dict(base, BorderMode=3, AbortMode=2, MaximumLength=8.0, CurvatureMode=2)):
+        ref = H.run_oracle(settings, wind, seeds, precision="f32")
+        eng = H.run_engine(settings, wind, seeds, SortInterval=1, StepsPerLaunch=2)
+        keys = ("trajectories", "status") + (("lengths",) if settings.get("AbortMode") else ())
+        H.assert_same(eng, ref, keys)
+
+
+def round_storage(a, storage):
+    """The float32 -> storage -> float32 round trip of the device ring (round to nearest even)."""
+    a = np.ascontiguousarray(a, np.float32)
+    if storage == "Float16":
+        return a.astype(np.float16).astype(np.float32)
+    if storage == "BFloat16":
+        u = a.view(np.uint32).astype(np.uint64)
+        u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+        return u.astype(np.uint32).view(np.float32)
+    return a
+
+
+# storage error bounds in grid cells (RMS over particles alive in both runs), from a float64
+# oracle run on the rounded field: BF16 keeps 8 mantissa bits, FP16 11.
+STORAGE_RMS_BOUND = {"Float32": 1e-3, "Float16": 2e-3, "BFloat16": 1.5e-2}
 
 
 @pytest.mark.parametrize("storage", ["BFloat16", "Float16", "Float32"])
 def test_precision_forms_against_float64(storage):
+    """Precision form: 16-bit wind storage, float32 stages, Kahan-compensated positions and
+    float64 time weights.  (1) Against the float64 oracle fed the identically rounded field the
+    only difference is float32 arithmetic: median error <= 1e-5 cells.  (2) Against the
+    float64 oracle on the original field the storage error stays within STORAGE_RMS_BOUND."""
     import pygranite_b200 as pg
     from pygranite_b200 import workloads as W
-    settings, src, seeds = W.config2(n_particles=3000, n_snapshots=8, grid=(16, 32, 32), steps=60)
+    settings, src, seeds = W.config2(n_particles=3000, n_snapshots=12, grid=(16, 32, 32), steps=100)
     settings["CurvatureMode"] = 0
+    cell = [1000.0, 1000.0, 250.0]
     eng = H.run_engine(settings, src.wind, seeds, volumes=src.volumes, WindStorage=getattr(pg.WindStorage, storage),
                        CompensatedPositions=True, Float64Time=True)
+    rounded = [[round_storage(p, storage) for p in snap] for snap in src.wind]
+    ref_r = H.run_oracle(settings, rounded, seeds, volumes=src.volumes, precision="f64", time_mode=1)
     ref = H.run_oracle(settings, src.wind, seeds, volumes=src.volumes, precision="f64", time_mode=1)
+    assert (eng["status"] == ref_r["status"]).mean() > 0.99
+    alive = (eng["status"] == 0) & (ref_r["status"] == 0)
+    arith = H.cell_error(eng["trajectories"][alive], ref_r["trajectories"][alive], cell)
+    assert float(np.median(arith[:, 1:])) <= 1e-5, np.median(arith[:, 1:])
     alive = (eng["status"] == 0) & (ref["status"] == 0)
-    err = H.cell_error(eng["trajectories"][alive], ref["trajectories"][alive], [1000.0, 1000.0, 250.0])
-    rms = float(np.sqrt((err[:, -1] ** 2).mean()))
-    print(f"{storage}: final-record error vs f64: rms {rms:.3e} max {err[:, -1].max():.3e} cells")
-    bound = {"Float32": 1e-4, "Float16": 2e-3, "BFloat16": 2e-2}[storage]
-    assert rms < bound
+    err = H.cell_error(eng["trajectories"][alive], ref["trajectories"][alive], cell)
+    for rec in (1, 2, 5, 10):
+        x = err[:, rec]
+        print(f"{storage} step {rec * 10:4d}: rms {np.sqrt((x ** 2).mean()):.2e} p50 {np.median(x):.2e} "
+              f"p99 {np.percentile(x, 99):.2e} max {x.max():.2e} cells")
+    assert float(np.sqrt((err[:, 10] ** 2).mean())) < STORAGE_RMS_BOUND[storage]
 
 
 def test_errors_match_reference_messages():
