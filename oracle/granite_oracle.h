@@ -52,6 +52,7 @@ typedef struct {
     int32_t use_sphere;       /* 2D and SphereRadius > 0 */
     int32_t time_mode;        /* 0: weights from the float32 accumulator (reference); 1: from float64 time */
     int32_t minimum_alive;
+    int32_t compensated;      /* Kahan-compensated position update (the engine's precision form) */
     int64_t save_interval;
     float sphere_radius, delta_t, data_time_distance, maximum_length, maximum_simulation_time;
     float scale[3], offset[3], domain[3];

@@ -44,7 +44,7 @@ class OrInput(ctypes.Structure):
         ("constants_mode", ctypes.c_int32), ("volume_mode", ctypes.c_int32),
         ("use_topography", ctypes.c_int32), ("reverse", ctypes.c_int32),
         ("use_sphere", ctypes.c_int32), ("time_mode", ctypes.c_int32),
-        ("minimum_alive", ctypes.c_int32), ("save_interval", ctypes.c_int64),
+        ("minimum_alive", ctypes.c_int32), ("compensated", ctypes.c_int32), ("save_interval", ctypes.c_int64),
         ("sphere_radius", ctypes.c_float), ("delta_t", ctypes.c_float),
         ("data_time_distance", ctypes.c_float), ("maximum_length", ctypes.c_float),
         ("maximum_simulation_time", ctypes.c_float),
@@ -162,7 +162,7 @@ def _ptr(a):
     return a.ctypes.data_as(_FP)
 
 
-def _build_input(s: dict, data: Inputs, time_mode=0, threads=0, step_limit=-1):
+def _build_input(s: dict, data: Inputs, time_mode=0, threads=0, step_limit=-1, compensated=False):
     keep = []
     dim = 3 if s["Space"] == 0 else 2
     seeds = np.ascontiguousarray(data.seeds, dtype=np.float32)
@@ -228,6 +228,7 @@ def _build_input(s: dict, data: Inputs, time_mode=0, threads=0, step_limit=-1):
     inp.use_sphere = int(dim == 2 and s["SphereRadius"] > 0)
     inp.time_mode = time_mode
     inp.minimum_alive = int(s["MinimumAliveParticles"])
+    inp.compensated = int(bool(compensated))
     inp.save_interval = int(s["SaveInterval"])
     inp.sphere_radius = s["SphereRadius"]
     inp.delta_t = s["DeltaT"]
@@ -272,9 +273,9 @@ def schedule(s: dict, data: Inputs, time_mode=0):
                  t0f=st.t0f, t1f=st.t1f, t2f=st.t2f) for st in steps[:k]], windows.value
 
 
-def run(s: dict, data: Inputs, precision="f64", time_mode=0, threads=0, step_limit=-1) -> dict:
+def run(s: dict, data: Inputs, precision="f64", time_mode=0, threads=0, step_limit=-1, compensated=False) -> dict:
     """Runs the oracle; returns outputs in the reference's accessor shapes."""
-    inp, keep, meta = _build_input(s, data, time_mode, threads, step_limit)
+    inp, keep, meta = _build_input(s, data, time_mode, threads, step_limit, compensated)
     n, dim = meta["n"], meta["dim"]
     windows = ctypes.c_int64(0)
     k = lib().oracle_schedule(ctypes.byref(inp), None, 0, ctypes.byref(windows))

@@ -6,6 +6,10 @@
 // retired store and are never launched again; the records they would have written later
 // are filled from their frozen state at the end of the run.  Per-particle arithmetic does
 // not depend on the order, so results stay bit-identical.
+//
+// One pass: bin (key + warp-aggregated histogram) -> two-level exclusive scan -> rank
+// (destination of every source slot, written as a permutation) -> gather (coalesced writes
+// of every state array) -> commit (counts).
 #pragma once
 
 #include <cstdint>
@@ -13,6 +17,8 @@
 #include "granite_kernels.cuh"
 
 namespace granite_b200 {
+
+constexpr int SCAN_CHUNK = 1024;   // bins per block of the first scan level
 
 struct StateView {
     float *px, *py, *pz, *qx, *qy, *qz, *kx, *ky, *kz, *lx, *ly, *lz;
@@ -24,7 +30,9 @@ struct StateView {
 struct CompactParams {
     StateView src, dst, ret;
     int32_t *key;              // bin of each active slot
-    int32_t *hist;             // nbins + 1 counters -> cursors
+    int32_t *hist;             // nbins + 1 counters -> offsets within the chunk -> cursors
+    int32_t *chunk;            // per-chunk sums -> chunk base offsets
+    int32_t *perm;             // destination slot -> source slot
     const int32_t *bintab;     // brick linear index -> Morton rank
     int32_t *n_act;            // active count (device)
     int32_t *n_new;            // live count after the pass (device)
@@ -36,50 +44,108 @@ struct CompactParams {
     int32_t rec_now;           // first record index not yet written
 };
 
+__device__ __forceinline__ int32_t bin_of(const CompactParams &C, int64_t i) {
+    if (C.src.status[i] != 0) return C.nbins;   // retired bin, last
+    const float ax = (C.src.px[i] - C.off[0]) * C.inv_scale[0];
+    const float ay = (C.src.py[i] - C.off[1]) * C.inv_scale[1];
+    const int ix = (int)fminf(fmaxf(floorf(ax), 0.f), (float)(C.nx - 1));
+    const int iy = (int)fminf(fmaxf(floorf(ay), 0.f), (float)(C.ny - 1));
+    int iz = 0;
+    if (C.dim == 3) {
+        const float az = (C.src.pz[i] - C.off[2]) * C.inv_scale[2];
+        iz = (int)fminf(fmaxf(floorf(az), 0.f), (float)(C.nz - 1));
+    }
+    return C.bintab[((iz / C.bz) * C.nby + iy / C.by) * C.nbx + ix / C.bx];
+}
+
+// key + histogram; lanes of a warp with the same key add once (sorted input: mostly one key per warp)
 __global__ void bin_kernel(const __grid_constant__ CompactParams C) {
     const int64_t n = *C.n_act;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int32_t k = C.nbins;   // retired bin, last
-        if (C.src.status[i] == 0) {
-            const float ax = (C.src.px[i] - C.off[0]) * C.inv_scale[0];
-            const float ay = (C.src.py[i] - C.off[1]) * C.inv_scale[1];
-            int ix = (int)fminf(fmaxf(floorf(ax), 0.f), (float)(C.nx - 1));
-            int iy = (int)fminf(fmaxf(floorf(ay), 0.f), (float)(C.ny - 1));
-            int iz = 0;
-            if (C.dim == 3) {
-                const float az = (C.src.pz[i] - C.off[2]) * C.inv_scale[2];
-                iz = (int)fminf(fmaxf(floorf(az), 0.f), (float)(C.nz - 1));
-            }
-            const int b = ((iz / C.bz) * C.nby + iy / C.by) * C.nbx + ix / C.bx;
-            k = C.bintab[b];
-        }
-        C.key[i] = k;
-        atomicAdd(C.hist + k, 1);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int64_t i = base + threadIdx.x;
+        const bool ok = i < n;
+        const int32_t k = ok ? bin_of(C, i) : -1;
+        if (ok) C.key[i] = k;
+        const unsigned peers = __match_any_sync(0xffffffffu, k);
+        const int leader = __ffs(peers) - 1;
+        if (ok && (int)(threadIdx.x & 31) == leader) atomicAdd(C.hist + k, __popc(peers));
     }
 }
 
-// Exclusive scan of the nbins + 1 counters in one block; n_new = start of the retired bin.
-__global__ void __launch_bounds__(1024) scan_kernel(const __grid_constant__ CompactParams C) {
-    __shared__ int32_t part[1024];
+// level 1: exclusive scan inside chunks of SCAN_CHUNK bins; chunk totals to C.chunk
+__global__ void __launch_bounds__(SCAN_CHUNK) scan_chunks_kernel(const __grid_constant__ CompactParams C) {
+    __shared__ int32_t warp_sum[SCAN_CHUNK / 32];
     const int nb = C.nbins + 1;
-    const int per = (nb + blockDim.x - 1) / blockDim.x;
-    const int b0 = threadIdx.x * per, b1 = min(nb, b0 + per);
+    const int b = blockIdx.x * SCAN_CHUNK + threadIdx.x;
+    const int32_t v = b < nb ? C.hist[b] : 0;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int32_t s = warp_sum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        warp_sum[lane] = s;   // inclusive over warps
+    }
+    __syncthreads();
+    const int32_t incl = x + (wid > 0 ? warp_sum[wid - 1] : 0);
+    if (b < nb) C.hist[b] = incl - v;
+    if (threadIdx.x == SCAN_CHUNK - 1) C.chunk[blockIdx.x] = incl;
+}
+
+// level 2: exclusive scan of the chunk totals (one block); n_new = start of the retired bin
+__global__ void __launch_bounds__(1024) scan_top_kernel(const __grid_constant__ CompactParams C, int nchunks) {
+    __shared__ int32_t part[1024];
+    const int per = (nchunks + 1023) / 1024;
+    const int c0 = threadIdx.x * per, c1 = min(nchunks, c0 + per);
     int32_t s = 0;
-    for (int b = b0; b < b1; ++b) s += C.hist[b];
+    for (int c = c0; c < c1; ++c) s += C.chunk[c];
     part[threadIdx.x] = s;
     __syncthreads();
-    for (int off = 1; off < (int)blockDim.x; off <<= 1) {
-        const int32_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0;
+    for (int o = 1; o < 1024; o <<= 1) {
+        const int32_t y = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0;
         __syncthreads();
-        part[threadIdx.x] += v;
+        part[threadIdx.x] += y;
         __syncthreads();
     }
-    int32_t run = part[threadIdx.x] - s;   // exclusive prefix of this chunk
-    for (int b = b0; b < b1; ++b) {
-        const int32_t c = C.hist[b];
-        C.hist[b] = run;
-        if (b == C.nbins) *C.n_new = run;
-        run += c;
+    int32_t run = part[threadIdx.x] - s;
+    for (int c = c0; c < c1; ++c) {
+        const int32_t t = C.chunk[c];
+        C.chunk[c] = run;
+        run += t;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *C.n_new = C.hist[C.nbins] + C.chunk[C.nbins / SCAN_CHUNK];
+}
+
+// destination of every source slot, as a permutation dest -> source
+__global__ void rank_kernel(const __grid_constant__ CompactParams C) {
+    const int64_t n = *C.n_act;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int64_t i = base + threadIdx.x;
+        const bool ok = i < n;
+        const int32_t k = ok ? C.key[i] : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, k);
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(peers) - 1;
+        int32_t first = 0;
+        if (ok && lane == leader) first = atomicAdd(C.hist + k, __popc(peers));
+        first = __shfl_sync(0xffffffffu, first, leader);
+        if (ok) {
+            const int32_t d = C.chunk[k / SCAN_CHUNK] + first + __popc(peers & ((1u << lane) - 1));
+            C.perm[d] = (int32_t)i;
+        }
     }
 }
 
@@ -113,10 +179,11 @@ __device__ __forceinline__ void move_retired(const CompactParams &C, int64_t i, 
     R.retire[r] = C.rec_now;
 }
 
-__global__ void scatter_kernel(const __grid_constant__ CompactParams C) {
+// coalesced writes in destination order; the scattered reads hit L2
+__global__ void gather_kernel(const __grid_constant__ CompactParams C) {
     const int64_t n = *C.n_act, live = *C.n_new, base = *C.n_ret;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t d = atomicAdd(C.hist + C.key[i], 1);
+    for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < n; d += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = C.perm[d];
         if (d < live) move_live(C, i, d);
         else move_retired(C, i, base + (d - live));
     }

@@ -236,7 +236,7 @@ struct gr_engine {
     DevBuf<int32_t> d_counts;          // [0] live, [1] live after a pass, [2] retired
     int32_t *h_live = nullptr;         // pinned copy of the live count
     cudaEvent_t live_ready = nullptr;
-    DevBuf<int32_t> c_key, c_hist, c_bintab;
+    DevBuf<int32_t> c_key, c_hist, c_bintab, c_chunk, c_perm;
     int bx = 4, by = 4, bz = 2, nbx = 0, nby = 0, nbz = 0, nbins = 0;
     DevBuf<int32_t> crec_of_rec;
     DevBuf<float> hpos, hcurv, hvol, hcmp;
@@ -750,6 +750,8 @@ int alloc_state(gr_engine *e) {
         CK(e->c_bintab.alloc(tab.size()));
         CK(cudaMemcpy(e->c_bintab.p, tab.data(), tab.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
         CK(e->c_hist.alloc((size_t)e->nbins + 1));
+        CK(e->c_chunk.alloc((size_t)(e->nbins + 1 + SCAN_CHUNK - 1) / SCAN_CHUNK));
+        CK(e->c_perm.alloc(N));
     }
     const int threads = 256;
     seed_kernel<<<grid_for(n, threads), threads, 0, e->cs>>>(e->seeds.p, n, e->dim, S.px.p, S.py.p, S.pz.p,
@@ -830,6 +832,8 @@ int compact_pass(gr_engine *e, int32_t rec_now) {
     C.ret = view_of(e->ret, N);
     C.key = e->c_key.p;
     C.hist = e->c_hist.p;
+    C.chunk = e->c_chunk.p;
+    C.perm = e->c_perm.p;
     C.bintab = e->c_bintab.p;
     C.n_act = e->d_counts.p;
     C.n_new = e->d_counts.p + 1;
@@ -852,16 +856,19 @@ int compact_pass(gr_engine *e, int32_t rec_now) {
     C.rec_now = rec_now;
     const int threads = 256;
     const int blocks = grid_for(N, threads);
+    const int nchunks = (e->nbins + 1 + SCAN_CHUNK - 1) / SCAN_CHUNK;
     CK(cudaMemsetAsync(e->c_hist.p, 0, ((size_t)e->nbins + 1) * sizeof(int32_t), e->cs));
     bin_kernel<<<blocks, threads, 0, e->cs>>>(C);
-    scan_kernel<<<1, 1024, 0, e->cs>>>(C);
-    scatter_kernel<<<blocks, threads, 0, e->cs>>>(C);
+    scan_chunks_kernel<<<nchunks, SCAN_CHUNK, 0, e->cs>>>(C);
+    scan_top_kernel<<<1, 1024, 0, e->cs>>>(C, nchunks);
+    rank_kernel<<<blocks, threads, 0, e->cs>>>(C);
+    gather_kernel<<<blocks, threads, 0, e->cs>>>(C);
     commit_kernel<<<1, 1, 0, e->cs>>>(C);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(e->h_live, e->d_counts.p, sizeof(int32_t), cudaMemcpyDeviceToHost, e->cs));
     CK(cudaEventRecord(e->live_ready, e->cs));
     e->cur = 1 - e->cur;
-    e->stats.aux_launches += 4;
+    e->stats.aux_launches += 6;
     return GR_OK;
 }
 

@@ -13,7 +13,7 @@
 
 namespace granite_b200 {
 
-constexpr int GR_EXPR_MAX_CODE = 64;
+constexpr int GR_EXPR_MAX_CODE = 256;
 constexpr int GR_EXPR_MAX_STACK = 8;
 
 // Reference-vector slots, the order of `ref` in TrajectoryIntegrator.tpp:381-439.

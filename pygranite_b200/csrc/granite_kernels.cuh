@@ -101,11 +101,11 @@ template <typename W> struct Store;
 
 template <> struct Store<float> {
     // 3D node {u, v, w, 0}
-    static __device__ __forceinline__ void load3(const void *base, int64_t idx, float &u, float &v, float &w) {
+    static __device__ __forceinline__ void load3(const void *base, int32_t idx, float &u, float &v, float &w) {
         const float4 q = __ldg(reinterpret_cast<const float4 *>(base) + idx);
         u = q.x; v = q.y; w = q.z;
     }
-    static __device__ __forceinline__ void load2(const void *base, int64_t idx, float &u, float &v) {
+    static __device__ __forceinline__ void load2(const void *base, int32_t idx, float &u, float &v) {
         const float2 q = __ldg(reinterpret_cast<const float2 *>(base) + idx);
         u = q.x; v = q.y;
     }
@@ -113,13 +113,13 @@ template <> struct Store<float> {
 };
 
 template <> struct Store<__nv_bfloat16> {
-    static __device__ __forceinline__ void load3(const void *base, int64_t idx, float &u, float &v, float &w) {
+    static __device__ __forceinline__ void load3(const void *base, int32_t idx, float &u, float &v, float &w) {
         const uint2 q = __ldg(reinterpret_cast<const uint2 *>(base) + idx);
         const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&q.x));
         const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&q.y));
         u = a.x; v = a.y; w = b.x;
     }
-    static __device__ __forceinline__ void load2(const void *base, int64_t idx, float &u, float &v) {
+    static __device__ __forceinline__ void load2(const void *base, int32_t idx, float &u, float &v) {
         const unsigned q = __ldg(reinterpret_cast<const unsigned *>(base) + idx);
         const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&q));
         u = a.x; v = a.y;
@@ -128,13 +128,13 @@ template <> struct Store<__nv_bfloat16> {
 };
 
 template <> struct Store<__half> {
-    static __device__ __forceinline__ void load3(const void *base, int64_t idx, float &u, float &v, float &w) {
+    static __device__ __forceinline__ void load3(const void *base, int32_t idx, float &u, float &v, float &w) {
         const uint2 q = __ldg(reinterpret_cast<const uint2 *>(base) + idx);
         const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&q.x));
         const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&q.y));
         u = a.x; v = a.y; w = b.x;
     }
-    static __device__ __forceinline__ void load2(const void *base, int64_t idx, float &u, float &v) {
+    static __device__ __forceinline__ void load2(const void *base, int32_t idx, float &u, float &v) {
         const unsigned q = __ldg(reinterpret_cast<const unsigned *>(base) + idx);
         const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&q));
         u = a.x; v = a.y;
@@ -144,8 +144,8 @@ template <> struct Store<__half> {
 
 // Trilinear corner weights of one sample: indices and border validity.
 struct Cell3 {
-    int64_t base;        // node index of corner (ix, iy, iz), clamped into the grid
-    int64_t sx, sy, sz;  // strides to the +x / +y / +z corner (0 where that corner is clamped)
+    int32_t base;        // node index of corner (ix, iy, iz), clamped into the grid (< 2^31 nodes)
+    int32_t sx, sy, sz;  // strides to the +x / +y / +z corner (0 where that corner is clamped)
     float fx, fy, fz;
     unsigned valid;      // bit (dz*4 + dy*2 + dx): corner inside the grid
 };
@@ -169,10 +169,10 @@ __device__ __forceinline__ Cell3 make_cell3(const KParams &P, float ax, float ay
     c.valid |= (x0 && y1 && z1) << 6;
     c.valid |= (x1 && y1 && z1) << 7;
     const int cx = min(max(ix, 0), P.nx - 1), cy = min(max(iy, 0), P.ny - 1), cz = min(max(iz, 0), P.nz - 1);
-    c.base = ((int64_t)cz * P.ny + cy) * P.nx + cx;
+    c.base = (cz * P.ny + cy) * P.nx + cx;
     c.sx = (ix + 1 >= 0 && ix + 1 < P.nx && ix >= 0) ? 1 : 0;
-    c.sy = (iy + 1 >= 0 && iy + 1 < P.ny && iy >= 0) ? (int64_t)P.nx : 0;
-    c.sz = (iz + 1 >= 0 && iz + 1 < P.nz && iz >= 0) ? (int64_t)P.nx * P.ny : 0;
+    c.sy = (iy + 1 >= 0 && iy + 1 < P.ny && iy >= 0) ? P.nx : 0;
+    c.sz = (iz + 1 >= 0 && iz + 1 < P.nz && iz >= 0) ? P.nx * P.ny : 0;
     return c;
 }
 
@@ -183,7 +183,7 @@ __device__ __forceinline__ void tri3(const void *slot, const Cell3 &c, float &ou
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
-        const int64_t idx = c.base + (dx ? c.sx : 0) + (dy ? c.sy : 0) + (dz ? c.sz : 0);
+        const int32_t idx = c.base + (dx ? c.sx : 0) + (dy ? c.sy : 0) + (dz ? c.sz : 0);
         u[k] = 0.f; v[k] = 0.f; w[k] = 0.f;
         if (c.valid & (1u << k)) Store<W>::load3(slot, idx, u[k], v[k], w[k]);
     }
@@ -204,7 +204,7 @@ __device__ __forceinline__ float tri1(const float *plane, const Cell3 &c) {
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
-        const int64_t idx = c.base + (dx ? c.sx : 0) + (dy ? c.sy : 0) + (dz ? c.sz : 0);
+        const int32_t idx = c.base + (dx ? c.sx : 0) + (dy ? c.sy : 0) + (dz ? c.sz : 0);
         s[k] = (c.valid & (1u << k)) ? __ldg(plane + idx) : 0.f;
     }
     const float a00 = lerp_(s[0], s[1], c.fx), a10 = lerp_(s[2], s[3], c.fx);
@@ -214,7 +214,7 @@ __device__ __forceinline__ float tri1(const float *plane, const Cell3 &c) {
 
 // Bilinear footprint with clamped indices (2D pitch textures sample as clamp).
 struct Cell2 {
-    int64_t i00, i10, i01, i11;
+    int32_t i00, i10, i01, i11;
     float fx, fy;
 };
 
@@ -225,10 +225,10 @@ __device__ __forceinline__ Cell2 make_cell2(int nx, int ny, float ax, float ay) 
     cell(ay, ny, iy, c.fy);
     const int x0 = min(max(ix, 0), nx - 1), x1 = min(max(ix + 1, 0), nx - 1);
     const int y0 = min(max(iy, 0), ny - 1), y1 = min(max(iy + 1, 0), ny - 1);
-    c.i00 = (int64_t)y0 * nx + x0;
-    c.i10 = (int64_t)y0 * nx + x1;
-    c.i01 = (int64_t)y1 * nx + x0;
-    c.i11 = (int64_t)y1 * nx + x1;
+    c.i00 = y0 * nx + x0;
+    c.i10 = y0 * nx + x1;
+    c.i01 = y1 * nx + x0;
+    c.i11 = y1 * nx + x1;
     return c;
 }
 
@@ -353,10 +353,79 @@ __device__ __forceinline__ float eval_program(const Program *prog, const float (
     return s0;
 }
 
+// Volume samples and expression values of a particle, evaluated from the inputs of its last
+// alive step: position p (that step's new position), stage-averaged velocity vc, curvature cv
+// and the step's time weight / ring slots (tpp:363-447).  The kernel calls this only when the
+// values become observable (a record, the end of a launch), which gives the same values as
+// evaluating after every alive step, as the reference does.
+template <int DIM>
+__device__ __forceinline__ void eval_extras(const KParams &P, const StepEntry &E, int64_t pid, const V3 &p,
+                                            const V3 &vc, float cv, float (&vol)[GR_MAX_VOL],
+                                            float (&cmp)[GR_MAX_EXPR]) {
+    const float t0 = P.dyn_any ? E.t0 : 0.f;
+    if (P.volume_mode != 0 && P.nvol > 0) {
+        const int vb = P.volume_mode == 2 ? E.slot_back : 0, vf = P.volume_mode == 2 ? E.slot_front : 0;
+        const float ax = (p.x - P.off[0]) * P.inv_scale[0];
+        const float ay = (p.y - P.off[1]) * P.inv_scale[1];
+        if (DIM == 3) {
+            const float az = (p.z - P.off[2]) * P.inv_scale[2];
+            const Cell3 c = make_cell3(P, ax, ay, az);
+#pragma unroll
+            for (int k = 0; k < GR_MAX_VOL; ++k) {
+                if (k < P.nvol) {
+                    const float b = tri1(P.vol + ((int64_t)vb * GR_MAX_VOL + k) * P.vol_plane, c);
+                    vol[k] = P.volume_mode == 2 ? lerp_(b, tri1(P.vol + ((int64_t)vf * GR_MAX_VOL + k) * P.vol_plane, c), t0)
+                                                : b;
+                }
+            }
+        } else {
+            const Cell2 c = make_cell2(P.nx, P.ny, ax, ay);
+#pragma unroll
+            for (int k = 0; k < GR_MAX_VOL; ++k) {
+                if (k < P.nvol) {
+                    const float b = bil1(P.vol + ((int64_t)vb * GR_MAX_VOL + k) * P.vol_plane, c);
+                    vol[k] = P.volume_mode == 2 ? lerp_(b, bil1(P.vol + ((int64_t)vf * GR_MAX_VOL + k) * P.vol_plane, c), t0)
+                                                : b;
+                }
+            }
+        }
+    }
+    if (P.nexpr > 0) {
+        float ref[19];
+        ref[0] = p.x; ref[1] = p.y; ref[2] = DIM == 3 ? p.z : 0.f;
+        ref[3] = P.curvature_mode == 3 ? cv : 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) ref[4 + k] = k < P.nvol ? vol[k] : 0.f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float c = 0.f;
+            if (k < P.ncon && P.constants_mode != 0) {
+                const int cb = P.constants_mode == 2 ? E.slot_back : 0;
+                const float b = __ldg(P.cons + ((int64_t)cb * GR_MAX_CON + k) * P.n_total + pid);
+                if (P.constants_mode == 2) {
+                    const float f = __ldg(P.cons + ((int64_t)E.slot_front * GR_MAX_CON + k) * P.n_total + pid);
+                    c = lerp_(b, f, t0);
+                } else {
+                    c = b;
+                }
+            }
+            ref[12 + k] = c;
+        }
+        ref[16] = vc.x; ref[17] = vc.y; ref[18] = DIM == 3 ? vc.z : 0.f;
+#pragma unroll
+        for (int e = 0; e < GR_MAX_EXPR; ++e)
+            if (e < P.nexpr) cmp[e] = eval_program(P.prog + e, ref);
+    }
+}
+
 // ------------------------------------------------------------------ the step kernel
 
+#ifndef GR_ADV_MIN_BLOCKS
+#define GR_ADV_MIN_BLOCKS 2
+#endif
+
 template <int DIM, bool RK4, typename W>
-__global__ void __launch_bounds__(256) advance_kernel(const __grid_constant__ KParams P) {
+__global__ void __launch_bounds__(256, GR_ADV_MIN_BLOCKS) advance_kernel(const __grid_constant__ KParams P) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t n_live = P.n_dev ? (int64_t)*P.n_dev : P.n;
     const bool valid = i < n_live;
@@ -391,6 +460,10 @@ __global__ void __launch_bounds__(256) advance_kernel(const __grid_constant__ KP
     }
     const bool was_alive = alive;
     unsigned long long my_steps = 0;
+    const bool extras = (P.volume_mode != 0 && P.nvol > 0) || P.nexpr > 0;
+    V3 vc_last{0.f, 0.f, 0.f};
+    int last_s = P.s0;
+    bool dirty = false;   // volumes / expressions not yet evaluated for the last alive step
     const int sph = P.sphere && DIM == 2;
 
     for (int s = P.s0; s < P.s1; ++s) {
@@ -568,64 +641,10 @@ __global__ void __launch_bounds__(256) advance_kernel(const __grid_constant__ KP
                     if (!isnan(k)) tc += k * ds;
                 }
 
-                // additional volumes at the new position (tpp:363-377)
-                if (P.volume_mode != 0 && P.nvol > 0) {
-                    const int vb = P.volume_mode == 2 ? E.slot_back : 0, vf = P.volume_mode == 2 ? E.slot_front : 0;
-                    const float ax = (np.x - P.off[0]) * P.inv_scale[0];
-                    const float ay = (np.y - P.off[1]) * P.inv_scale[1];
-                    if (DIM == 3) {
-                        const float az = (np.z - P.off[2]) * P.inv_scale[2];
-                        const Cell3 c = make_cell3(P, ax, ay, az);
-#pragma unroll
-                        for (int k = 0; k < GR_MAX_VOL; ++k) {
-                            if (k < P.nvol) {
-                                const float b = tri1(P.vol + ((int64_t)vb * GR_MAX_VOL + k) * P.vol_plane, c);
-                                vol[k] = P.volume_mode == 2
-                                             ? lerp_(b, tri1(P.vol + ((int64_t)vf * GR_MAX_VOL + k) * P.vol_plane, c), t0)
-                                             : b;
-                            }
-                        }
-                    } else {
-                        const Cell2 c = make_cell2(P.nx, P.ny, ax, ay);
-#pragma unroll
-                        for (int k = 0; k < GR_MAX_VOL; ++k) {
-                            if (k < P.nvol) {
-                                const float b = bil1(P.vol + ((int64_t)vb * GR_MAX_VOL + k) * P.vol_plane, c);
-                                vol[k] = P.volume_mode == 2
-                                             ? lerp_(b, bil1(P.vol + ((int64_t)vf * GR_MAX_VOL + k) * P.vol_plane, c), t0)
-                                             : b;
-                            }
-                        }
-                    }
-                }
-
-                // expressions (tpp:379-447)
-                if (P.nexpr > 0) {
-                    float ref[19];
-                    ref[0] = np.x; ref[1] = np.y; ref[2] = DIM == 3 ? np.z : 0.f;
-                    ref[3] = P.curvature_mode == 3 ? cv : 0.f;
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) ref[4 + k] = k < P.nvol ? vol[k] : 0.f;
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        float c = 0.f;
-                        if (k < P.ncon && P.constants_mode != 0) {
-                            const int cb = P.constants_mode == 2 ? E.slot_back : 0;
-                            const float b = __ldg(P.cons + ((int64_t)cb * GR_MAX_CON + k) * P.n_total + pid);
-                            if (P.constants_mode == 2) {
-                                const float f = __ldg(P.cons + ((int64_t)E.slot_front * GR_MAX_CON + k) * P.n_total + pid);
-                                c = lerp_(b, f, t0);
-                            } else {
-                                c = b;
-                            }
-                        }
-                        ref[12 + k] = c;
-                    }
-                    ref[16] = vc.x; ref[17] = vc.y; ref[18] = DIM == 3 ? vc.z : 0.f;
-#pragma unroll
-                    for (int e = 0; e < GR_MAX_EXPR; ++e)
-                        if (e < P.nexpr) cmp[e] = eval_program(P.prog + e, ref);
-                }
+                // volumes and expressions are evaluated lazily (eval_extras)
+                vc_last = vc;
+                last_s = s;
+                dirty = true;
 
                 q = p;
                 p = np;
@@ -634,6 +653,10 @@ __global__ void __launch_bounds__(256) advance_kernel(const __grid_constant__ KP
         }
 
         if (valid && (E.flags & SF_SAVE)) {
+            if (extras && dirty) {
+                eval_extras<DIM>(P, P.sched[last_s], pid, p, vc_last, cv, vol, cmp);
+                dirty = false;
+            }
             float *hp = P.hpos + (pid * P.L + E.rec) * DIM;
             hp[0] = p.x; hp[1] = p.y;
             if (DIM == 3) hp[2] = p.z;
@@ -650,6 +673,7 @@ __global__ void __launch_bounds__(256) advance_kernel(const __grid_constant__ KP
     }
 
     if (valid && was_alive) {
+        if (extras && dirty) eval_extras<DIM>(P, P.sched[last_s], pid, p, vc_last, cv, vol, cmp);
         P.status[i] = st;
         P.px[i] = p.x; P.py[i] = p.y;
         if (DIM == 3) P.pz[i] = p.z;

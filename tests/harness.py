@@ -35,10 +35,10 @@ def run_engine(settings: dict, wind, seeds, volumes=None, constants=None, uplift
 
 
 def run_oracle(settings: dict, wind, seeds, volumes=None, constants=None, uplift=None, topography=None,
-               precision="f64", time_mode=0):
+               precision="f64", time_mode=0, compensated=False):
     data = orc.Inputs(wind=wind, seeds=seeds, volumes=volumes or [], constants=constants or [],
                       uplift=uplift or [], topography=topography)
-    return orc.run(orc.settings(**settings), data, precision=precision, time_mode=time_mode)
+    return orc.run(orc.settings(**settings), data, precision=precision, time_mode=time_mode, compensated=compensated)
 
 
 def cell_error(a, b, cell):

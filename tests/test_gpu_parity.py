@@ -252,9 +252,9 @@ def test_launch_shape_does_not_change_results(extra):
     """Launch granularity, block size, ring depth and compaction / re-sorting of the live
     particles change nothing: every output stays bit-identical to the float32 oracle."""
     base, wind, seeds = problem3d(seed=2)
-    exprs = ["x + cv*2", "temp - z"]
     vols = [{"temp": np.random.default_rng(4).standard_normal((12, 20, 24)).astype(np.float32)} for _ in wind]
-    for extra_settings in (dict(CurvatureMode=3, SaveInterval=2), dict(CurvatureMode=1, SaveInterval=0)):
+    for extra_settings, exprs in ((dict(CurvatureMode=3, SaveInterval=2), ["x + cv*2", "temp - z"]),
+                                  (dict(CurvatureMode=1, SaveInterval=0), ["x*2", "temp - z"])):
         settings = dict(base, AdditionalVolumeMode=1, AdditionalCompute=exprs, **extra_settings)
         ref = H.run_oracle(settings, wind, seeds, volumes=vols, precision="f32")
         eng = H.run_engine(settings, wind, seeds, volumes=vols, **extra)
@@ -295,23 +295,30 @@ STORAGE_RMS_BOUND = {"Float32": 1e-3, "Float16": 2e-3, "BFloat16": 1.5e-2}
 @pytest.mark.parametrize("storage", ["BFloat16", "Float16", "Float32"])
 def test_precision_forms_against_float64(storage):
     """Precision form: 16-bit wind storage, float32 stages, Kahan-compensated positions and
-    float64 time weights.  (1) Against the float64 oracle fed the identically rounded field the
-    only difference is float32 arithmetic: median error <= 1e-5 cells.  (2) Against the
-    float64 oracle on the original field the storage error stays within STORAGE_RMS_BOUND."""
+    float64 time weights.
+    (1) Bit for bit against the float32 oracle with the same compensation on the field
+        rounded exactly as the device ring stores it.
+    (2) Against the float64 oracle on the original field: the storage error stays within
+        STORAGE_RMS_BOUND.  Particles that end within one cell of an upper domain face are
+        left out of the status comparison: under the reference's border addressing they
+        creep toward the face and stall (Wind), at a step set by the float resolution."""
     import pygranite_b200 as pg
     from pygranite_b200 import workloads as W
     settings, src, seeds = W.config2(n_particles=3000, n_snapshots=12, grid=(16, 32, 32), steps=100)
     settings["CurvatureMode"] = 0
-    cell = [1000.0, 1000.0, 250.0]
+    cell = np.array([1000.0, 1000.0, 250.0])
     eng = H.run_engine(settings, src.wind, seeds, volumes=src.volumes, WindStorage=getattr(pg.WindStorage, storage),
                        CompensatedPositions=True, Float64Time=True)
     rounded = [[round_storage(p, storage) for p in snap] for snap in src.wind]
-    ref_r = H.run_oracle(settings, rounded, seeds, volumes=src.volumes, precision="f64", time_mode=1)
+    ref32 = H.run_oracle(settings, rounded, seeds, volumes=src.volumes, precision="f32", time_mode=1,
+                         compensated=True)
+    H.assert_same(eng, ref32)
     ref = H.run_oracle(settings, src.wind, seeds, volumes=src.volumes, precision="f64", time_mode=1)
-    assert (eng["status"] == ref_r["status"]).mean() > 0.99
-    alive = (eng["status"] == 0) & (ref_r["status"] == 0)
-    arith = H.cell_error(eng["trajectories"][alive], ref_r["trajectories"][alive], cell)
-    assert float(np.median(arith[:, 1:])) <= 1e-5, np.median(arith[:, 1:])
+    upper = np.array([32000.0, 32000.0, 4000.0])
+    near = (np.abs(eng["trajectories"][:, -1] - upper) < cell).any(axis=1) | \
+        (np.abs(ref["trajectories"][:, -1] - upper) < cell).any(axis=1)
+    agree = (eng["status"] == ref["status"])[~near].mean()
+    assert agree > 0.995, agree
     alive = (eng["status"] == 0) & (ref["status"] == 0)
     err = H.cell_error(eng["trajectories"][alive], ref["trajectories"][alive], cell)
     for rec in (1, 2, 5, 10):
