@@ -122,6 +122,19 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def combine_ranks(dist, time_ms, particle_steps, device):
+    """Whole-job figures across ranks: the slowest rank's device time and the summed work
+    (replicas: every rank integrates its own particle set, no data-path collective)."""
+    if dist is None:
+        return time_ms, particle_steps
+    import torch
+    t = torch.tensor([float(time_ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(particle_steps)], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(c.item())
+
+
 def load_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -237,13 +250,7 @@ def main():
     info = eng.info()
 
     # max over ranks of the device time, sum of the particle-steps
-    t_max, ps_all = tot_ms, ps
-    if pg_dist:
-        t = torch.tensor([tot_ms], dtype=torch.float64, device="cuda")
-        pg_dist.all_reduce(t, op=pg_dist.ReduceOp.MAX)
-        c = torch.tensor([ps], dtype=torch.float64, device="cuda")
-        pg_dist.all_reduce(c, op=pg_dist.ReduceOp.SUM)
-        t_max, ps_all = float(t.item()), int(c.item())
+    t_max, ps_all = combine_ranks(pg_dist, tot_ms, ps, "cuda")
     value = ps_all / (t_max / 1e3)
     eng.close()
 
@@ -278,13 +285,7 @@ def main():
                 d2h = res.trajectories().nbytes + res.computeInfo(0).nbytes + res.volumeInfo("T").nbytes + \
                     res.totalCurvatures().nbytes + 4 * seeds.shape[0]
             del res
-        e_t, e_psa = e_s, e_ps
-        if pg_dist:
-            t = torch.tensor([e_s], dtype=torch.float64, device="cuda")
-            pg_dist.all_reduce(t, op=pg_dist.ReduceOp.MAX)
-            c = torch.tensor([e_ps], dtype=torch.float64, device="cuda")
-            pg_dist.all_reduce(c, op=pg_dist.ReduceOp.SUM)
-            e_t, e_psa = float(t.item()), int(c.item())
+        e_t, e_psa = combine_ranks(pg_dist, e_s, e_ps, "cuda")
         e2e = {"value": e_psa / e_t, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "steps": args.e2e_steps}
 
