@@ -46,7 +46,7 @@ def parse():
     p.add_argument("--sim-steps", type=int, default=2000)
     p.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
     p.add_argument("--steps-per-launch", type=int, default=0)
-    p.add_argument("--sort-interval", type=int, default=1,
+    p.add_argument("--sort-interval", type=int, default=4,
                    help="launches between compaction / Morton re-sorts of the live particles (0 = off)")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-e2e", action="store_true")

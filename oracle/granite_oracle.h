@@ -10,13 +10,13 @@
  * not exist, source/pygranite.cpp:37-39).  This oracle is pinned by (1) analytic
  * known answers (uniform wind, linear-in-time wind, solid-body rotation) in
  * tests/test_oracle.py and (2) fixtures produced by the reference's own `integrate`
- * kernel built from its sources and run on a B200 (tests/golden/).
+ * kernel built from its sources and run on a B200 (tests/golden/, tests/test_golden.py).
  *
- * One source, two builds:
- *   liboracle_f64.so  REAL = double : the judge (ideal arithmetic, exact 1/scale).
- *   liboracle_f32.so  REAL = float  : mirrors the CUDA kernel's float operation order
- *                                     (explicit fmaf, no contraction) so positions,
- *                                     status, lengths and curvature compare bit-exactly.
+ * One source, both precisions in liboracle.so:
+ *   *_f64  REAL = double : the judge (ideal arithmetic, exact 1/scale).
+ *   *_f32  REAL = float  : follows the CUDA kernel's float operation order (explicit
+ *                          fmaf, no contraction) so positions, status, lengths and
+ *                          curvature compare bit for bit.
  */
 #ifndef GRANITE_ORACLE_H
 #define GRANITE_ORACLE_H
