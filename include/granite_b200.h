@@ -195,6 +195,34 @@ int gr_load_windfield_device(gr_engine *engine, int64_t snapshot, const float *c
                              int32_t n_components, int64_t nz, int64_t ny, int64_t nx);
 int gr_set_seeds_device(gr_engine *engine, const float *positions, int64_t n, int32_t dim);
 
+/* Allocation-free advance of particles between two snapshots.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc — code running while a CUDA
+ * graph is being captured, hosts whose device memory belongs to their own pool allocator,
+ * real-time loops that forbid allocation after start-up.  It allocates no device memory and
+ * calls no allocating routine; the caller owns every input and output buffer:
+ *   wind_back / wind_front: the two snapshots, node-major (z, y, x), float4 {u, v, w, 0}
+ *     per node in 3D or float2 {u, v} in 2D, on the device;
+ *   px, py, pz, status: particle positions and abort codes (0 = alive), device arrays of n,
+ *     updated in place; pz unused in 2D.
+ * It runs `steps` integrator steps starting at time_start inside the window
+ * [time_back, time_front], with the reference's float32 time arithmetic, and writes the
+ * particle-steps done to *particle_steps (if non-null; this synchronises `stream`).  Only the
+ * plain integrator: Euler / RK4, Reverse, border modes, sphere coordinates; no curvature,
+ * volumes, constants, uplift, topography or length abort, float32 storage (GR_ERR_USER
+ * otherwise).
+ * Its scratch (the per-step time weights and two counters, GR_NOALLOC_SCRATCH_BYTES) is one
+ * file-scope device array that every GPU loading the library holds until the process exits;
+ * steps beyond GR_NOALLOC_MAX_STEPS are rejected.  The first call on a device looks up that
+ * array's device address, so make it before any stream capture.  All calls share the array:
+ * calls whose work overlaps on the GPU (different streams, no ordering) race. */
+#define GR_NOALLOC_MAX_STEPS 4096
+#define GR_NOALLOC_SCRATCH_BYTES (GR_NOALLOC_MAX_STEPS * 48 + 16)
+int gr_advance_noalloc(const gr_settings *settings, int64_t nz, int64_t ny, int64_t nx,
+                       const void *wind_back, const void *wind_front, float time_back,
+                       float time_front, float time_start, int32_t steps, float *px, float *py,
+                       float *pz, int32_t *status, int64_t n, void *stream,
+                       int64_t *particle_steps);
+
 #ifdef __cplusplus
 }
 #endif

@@ -23,7 +23,7 @@ EXPORTS = [
     "gr_result_info_get", "gr_stats_get", "gr_fetch_positions", "gr_fetch_status",
     "gr_fetch_lengths", "gr_fetch_total_curvature", "gr_fetch_curvatures",
     "gr_fetch_volume_info", "gr_fetch_compute_info", "gr_load_windfield_device",
-    "gr_set_seeds_device", "gr_plan",
+    "gr_set_seeds_device", "gr_plan", "gr_advance_noalloc",
 ]
 
 
@@ -101,6 +101,9 @@ def lib():
             "gr_fetch_compute_info": (ctypes.c_int, [P, I32, FP, I64]),
             "gr_plan": (ctypes.c_int, [ctypes.POINTER(Settings), ctypes.POINTER(PlanInfo), I64,
                                        ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32), FP]),
+            "gr_advance_noalloc": (ctypes.c_int, [ctypes.POINTER(Settings), I64, I64, I64, P, P, ctypes.c_float,
+                                                  ctypes.c_float, ctypes.c_float, I32, P, P, P, P, I64, P,
+                                                  ctypes.POINTER(ctypes.c_int64)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -172,6 +175,17 @@ def plan(settings: Settings, with_steps=True):
                          win.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
                          flags.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _fp(w)))
     return info, dict(window=win[:n], flags=flags[:n], weights=w[:n])
+
+
+def advance_noalloc(settings: Settings, shape, wind_back_ptr, wind_front_ptr, time_back, time_front, time_start,
+                    steps, px_ptr, py_ptr, pz_ptr, status_ptr, n, stream_ptr=None):
+    """gr_advance_noalloc on caller-owned device buffers (raw pointers); returns particle-steps."""
+    nz, ny, nx = shape if len(shape) == 3 else (1,) + tuple(shape)
+    ps = ctypes.c_int64(0)
+    _check(lib().gr_advance_noalloc(ctypes.byref(settings), nz, ny, nx, wind_back_ptr, wind_front_ptr, time_back,
+                                    time_front, time_start, steps, px_ptr, py_ptr, pz_ptr, status_ptr, n,
+                                    stream_ptr, ctypes.byref(ps)))
+    return ps.value
 
 
 def evaluate_expression(code, ref, volume_names=(), constant_names=(), dim=3, curvature_mode=0):

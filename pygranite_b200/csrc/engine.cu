@@ -46,6 +46,15 @@ int fail(int code, const char *fmt, ...) {
 
 #define USER_ERR(...) fail(GR_ERR_USER, "ERROR < USER INPUT | " __VA_ARGS__)
 
+}  // namespace
+
+namespace granite_b200 {
+// lets other translation units of the library report through gr_last_error()
+void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+}  // namespace granite_b200
+
+namespace {
+
 #define CK(call)                                                                                   \
     do {                                                                                           \
         cudaError_t err_ = (call);                                                                 \
