@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--steps-per-launch", type=int, default=0)
     p.add_argument("--sort-interval", type=int, default=4,
                    help="launches between compaction / Morton re-sorts of the live particles (0 = off)")
+    p.add_argument("--layout", type=int, default=0, help="0: window-pair wind layout, 1: ring slots")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -213,7 +214,8 @@ def main():
 
     # ---------------- device-resident engine: every snapshot in the ring before timing
     cs = capi.settings_from_reference(settings, ring_slots=n_snap, storage=storage, device=local,
-                                      steps_per_launch=args.steps_per_launch, sort_interval=args.sort_interval)
+                                      steps_per_launch=args.steps_per_launch, sort_interval=args.sort_interval,
+                                      layout=args.layout)
     eng = capi.Engine(cs)
     eng.set_seeds(seeds)
     for k, snap in enumerate(src.wind):
@@ -265,6 +267,7 @@ def main():
         s.Device = local
         s.SortInterval = args.sort_interval
         s.StepsPerLaunch = args.steps_per_launch
+        s.WindLayout = args.layout
         h2d = seeds.nbytes + sum(p.nbytes for snap in src.wind for p in snap) + src.volumes[0]["T"].nbytes
         e_ps, e_s, d2h = 0, 0.0, 0
         for k in range(1 + args.e2e_steps):
@@ -318,7 +321,8 @@ def main():
                    "snapshots": n_snap, "grid": [192, 192, 64], "storage": args.storage,
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (201 snapshots, 7.6 GB ring)",
                    "records": int(info.records), "steps_run": int(info.steps),
-                   "sort_interval": args.sort_interval, "steps_per_launch": args.steps_per_launch},
+                   "sort_interval": args.sort_interval, "steps_per_launch": args.steps_per_launch,
+                   "wind_layout": ["window-pair", "ring"][args.layout]},
         "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
         "gpu_launches": int(launches + aux), "wall_s": wall,
     }

@@ -73,6 +73,9 @@ typedef struct gr_settings {
     int32_t sort_interval;         /* launches between Morton re-sorts / compactions; 0 = off */
     int32_t block_size;            /* threads per block; 0 = autotuned default */
     int32_t device;                /* CUDA device ordinal */
+    int32_t layout;                /* wind layout read by the step kernel: 0 = window pairs when the
+                                      windfield is dynamic (one load returns the back and the front
+                                      snapshot), 1 = the ring slots directly */
 } gr_settings;
 
 /* Fills *s with the reference's IntegratorSettings defaults (IntegratorSettings.hpp:89-181). */

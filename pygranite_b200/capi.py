@@ -39,7 +39,7 @@ class Settings(ctypes.Structure):
         ("offset", ctypes.c_float * 3), ("save_interval", ctypes.c_int64), ("storage", ctypes.c_int32),
         ("time_mode", ctypes.c_int32), ("compensated", ctypes.c_int32), ("ring_slots", ctypes.c_int32),
         ("steps_per_launch", ctypes.c_int32), ("sort_interval", ctypes.c_int32), ("block_size", ctypes.c_int32),
-        ("device", ctypes.c_int32),
+        ("device", ctypes.c_int32), ("layout", ctypes.c_int32),
     ]
 
 

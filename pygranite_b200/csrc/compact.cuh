@@ -23,7 +23,7 @@ constexpr int SCAN_CHUNK = 1024;   // bins per block of the first scan level
 struct StateView {
     float *px, *py, *pz, *qx, *qy, *qz, *kx, *ky, *kz, *lx, *ly, *lz;
     float *length, *tc, *curv, *volc, *cmpc;
-    int32_t *status, *id, *retire;
+    int32_t *status, *id, *retire, *life;
     int64_t stride;   // per-array stride of volc / cmpc
 };
 
@@ -42,10 +42,12 @@ struct CompactParams {
     int32_t bx, by, bz, nbx, nby, nbz, nbins;
     int32_t nvol, nexpr, curv_prev, compensated, fast_curv, abort_on, curv_on, curv_ind;
     int32_t rec_now;           // first record index not yet written
+    int32_t k_end;             // steps run so far: a particle whose lifetime is over retires
 };
 
 __device__ __forceinline__ int32_t bin_of(const CompactParams &C, int64_t i) {
-    if (C.src.status[i] != 0) return C.nbins;   // retired bin, last
+    // retired bin (last): aborted, or its lifetime is over (status stays Time)
+    if (C.src.status[i] != 0 || (C.src.life && C.src.life[i] <= C.k_end)) return C.nbins;
     const float ax = (C.src.px[i] - C.off[0]) * C.inv_scale[0];
     const float ay = (C.src.py[i] - C.off[1]) * C.inv_scale[1];
     const int ix = (int)fminf(fmaxf(floorf(ax), 0.f), (float)(C.nx - 1));
@@ -163,6 +165,7 @@ __device__ __forceinline__ void move_live(const CompactParams &C, int64_t i, int
     for (int k = 0; k < C.nexpr; ++k) D.cmpc[k * D.stride + d] = S.cmpc[k * S.stride + i];
     D.status[d] = S.status[i];
     D.id[d] = S.id[i];
+    if (S.life) D.life[d] = S.life[i];
 }
 
 __device__ __forceinline__ void move_retired(const CompactParams &C, int64_t i, int64_t r) {

@@ -20,6 +20,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/granite_b200.h"
@@ -113,6 +114,16 @@ __global__ void pack_wind_kernel<__half>(const float *__restrict__ u, const floa
     }
 }
 
+// Window pair: node n of the pair buffer = node n of the back slot followed by node n of the
+// front slot (elements of E bytes, E = 4, 8 or 16).
+template <typename T>
+__global__ void pair_pack_kernel(const T *__restrict__ back, const T *__restrict__ front, T *out, int64_t nodes) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        out[2 * i] = back[i];
+        out[2 * i + 1] = front[i];
+    }
+}
+
 // Seeds (AoS, n x dim) -> state SoA; zeroes the per-particle accumulators.
 __global__ void seed_kernel(const float *__restrict__ seeds, int64_t n, int dim, float *px, float *py,
                             float *pz, int32_t *status, int32_t *id) {
@@ -199,6 +210,30 @@ struct PinnedBuf {
     }
 };
 
+// Host copy split over up to 8 threads: the staging copies into / out of pinned memory run
+// at a few GB/s on one core, which would otherwise set the pace of a run fed from the host.
+void parallel_memcpy(void *dst, const void *src, size_t bytes) {
+    constexpr size_t kMinChunk = size_t(8) << 20;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t t = std::min<size_t>({8, hw, std::max<size_t>(1, bytes / kMinChunk)});
+    if (t <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t chunk = ((bytes + t - 1) / t + 63) & ~size_t(63);
+    std::vector<std::thread> pool;
+    for (size_t k = 1; k < t; ++k) {
+        const size_t off = k * chunk;
+        if (off >= bytes) break;
+        pool.emplace_back([=] {
+            std::memcpy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off,
+                        std::min(chunk, bytes - off));
+        });
+    }
+    std::memcpy(dst, src, std::min(chunk, bytes));
+    for (auto &th : pool) th.join();
+}
+
 }  // namespace
 
 struct gr_engine {
@@ -216,6 +251,9 @@ struct gr_engine {
     // rings
     DevBuf<char> wind;
     int64_t wind_stride = 0;
+    bool use_pair = false;             // window-pair layout for the step kernel
+    DevBuf<char> pairbuf[2];
+    int64_t pair_window[2] = {-1, -1};
     DevBuf<float> vol, cons, lift, topo;
     int nvol = 0, ncon = 0;
     bool has_topo = false, has_uplift = false;
@@ -225,6 +263,7 @@ struct gr_engine {
     DevBuf<float> raw;                 // device staging of one snapshot's planes
     PinnedBuf pin[2];
     int pin_next = 0;
+    PinnedBuf bounce[2];               // pinned staging of result copies
 
     // expressions
     Program progs[GR_MAX_EXPR]{};
@@ -236,7 +275,7 @@ struct gr_engine {
     DevBuf<float> seeds;               // AoS n x dim
     struct State {
         DevBuf<float> px, py, pz, qx, qy, qz, kx, ky, kz, lx, ly, lz, length, tc, curv, volc, cmpc;
-        DevBuf<int32_t> status, id, retire;
+        DevBuf<int32_t> status, id, retire, life;
     };
     State st[2];                       // double-buffered live state (compaction swaps)
     State ret;                         // retired particles (frozen state)
@@ -392,7 +431,7 @@ int load_wind(gr_engine *e, int64_t snapshot, const float *const *comps, int32_t
         rc = ensure_pinned(e, plane * ncomp * sizeof(float), pb);
         if (rc) return rc;
         for (int c = 0; c < ncomp; ++c)
-            std::memcpy(static_cast<float *>(pb->p) + c * plane, comps[c], plane * sizeof(float));
+            parallel_memcpy(static_cast<float *>(pb->p) + c * plane, comps[c], plane * sizeof(float));
         CK(cudaMemcpyAsync(e->raw.p, pb->p, plane * ncomp * sizeof(float), cudaMemcpyHostToDevice, e->xs));
         CK(cudaEventRecord(pb->done, e->xs));
         e->stats.h2d_bytes += (int64_t)(plane * ncomp * sizeof(float));
@@ -503,7 +542,7 @@ int gr_load_volume(gr_engine *e, int64_t snapshot, int32_t index, const float *d
     const size_t bytes = (size_t)e->nodes * sizeof(float);
     rc = ensure_pinned(e, bytes, pb);
     if (rc) return rc;
-    std::memcpy(pb->p, data, bytes);
+    parallel_memcpy(pb->p, data, bytes);
     float *dst = e->vol.p + ((int64_t)slot * GR_MAX_VOLUMES + index) * e->nodes;
     CK(cudaMemcpyAsync(dst, pb->p, bytes, cudaMemcpyHostToDevice, e->xs));
     CK(cudaEventRecord(pb->done, e->xs));
@@ -529,7 +568,7 @@ int gr_load_constant(gr_engine *e, int64_t snapshot, int32_t index, const float 
     const size_t bytes = (size_t)n * sizeof(float);
     rc = ensure_pinned(e, bytes, pb);
     if (rc) return rc;
-    std::memcpy(pb->p, data, bytes);
+    parallel_memcpy(pb->p, data, bytes);
     CK(cudaMemcpyAsync(e->cons.p + ((int64_t)slot * GR_MAX_CONSTANTS + index) * e->n, pb->p, bytes,
                        cudaMemcpyHostToDevice, e->xs));
     CK(cudaEventRecord(pb->done, e->xs));
@@ -556,7 +595,7 @@ int gr_load_uplift(gr_engine *e, int64_t snapshot, const float *data, int64_t n,
     const size_t bytes = (size_t)n * 3 * sizeof(float);
     rc = ensure_pinned(e, bytes, pb);
     if (rc) return rc;
-    std::memcpy(pb->p, data, bytes);
+    parallel_memcpy(pb->p, data, bytes);
     CK(cudaMemcpyAsync(e->lift.p + (int64_t)slot * e->n * 3, pb->p, bytes, cudaMemcpyHostToDevice, e->xs));
     CK(cudaEventRecord(pb->done, e->xs));
     CK(cudaEventRecord(e->slot_ready[slot], e->xs));
@@ -775,7 +814,7 @@ StateView view_of(gr_engine::State &S, int64_t stride) {
     v.px = S.px.p; v.py = S.py.p; v.pz = S.pz.p; v.qx = S.qx.p; v.qy = S.qy.p; v.qz = S.qz.p;
     v.kx = S.kx.p; v.ky = S.ky.p; v.kz = S.kz.p; v.lx = S.lx.p; v.ly = S.ly.p; v.lz = S.lz.p;
     v.length = S.length.p; v.tc = S.tc.p; v.curv = S.curv.p; v.volc = S.volc.p; v.cmpc = S.cmpc.p;
-    v.status = S.status.p; v.id = S.id.p; v.retire = S.retire.p;
+    v.status = S.status.p; v.id = S.id.p; v.retire = S.retire.p; v.life = S.life.p;
     v.stride = stride;
     return v;
 }
@@ -799,7 +838,7 @@ KParams make_params(gr_engine *e) {
     P.kx = S.kx.p; P.ky = S.ky.p; P.kz = S.kz.p;
     P.lx = S.lx.p; P.ly = S.ly.p; P.lz = S.lz.p;
     P.status = S.status.p; P.length = S.length.p; P.tc = S.tc.p; P.curv = S.curv.p;
-    P.volc = S.volc.p; P.cmpc = S.cmpc.p; P.id = S.id.p;
+    P.volc = S.volc.p; P.cmpc = S.cmpc.p; P.id = S.id.p; P.life = S.life.p;
     P.n = e->n; P.n_state = e->n; P.n_total = e->n;
     P.n_dev = e->compacting ? e->d_counts.p : nullptr;
     P.hpos = e->hpos.p; P.hcurv = e->hcurv.p; P.hvol = e->hvol.p; P.hcmp = e->hcmp.p;
@@ -832,7 +871,7 @@ KParams make_params(gr_engine *e) {
 }
 
 // One compaction / re-sort pass over the live prefix (compact.cuh).
-int compact_pass(gr_engine *e, int32_t rec_now) {
+int compact_pass(gr_engine *e, int32_t rec_now, int32_t k_end) {
     CompactParams C;
     std::memset(&C, 0, sizeof C);
     const int64_t N = e->n;
@@ -863,6 +902,7 @@ int compact_pass(gr_engine *e, int32_t rec_now) {
     C.curv_on = cm != 0;
     C.curv_ind = cm == 3;
     C.rec_now = rec_now;
+    C.k_end = k_end;
     const int threads = 256;
     const int blocks = grid_for(N, threads);
     const int nchunks = (e->nbins + 1 + SCAN_CHUNK - 1) / SCAN_CHUNK;
@@ -923,6 +963,21 @@ using KernelFn = void (*)(const KParams);
 KernelFn pick_kernel(const gr_engine *e) {
     const bool rk4 = e->s.integrator == 1;
     const int st = e->s.storage;
+    if (e->use_pair) {
+        using PF = Pair<float>;
+        using PB = Pair<__nv_bfloat16>;
+        using PH = Pair<__half>;
+        if (e->dim == 3) {
+            if (rk4) return st == GR_STORE_BF16 ? advance_kernel<3, true, PB>
+                          : st == GR_STORE_F16 ? advance_kernel<3, true, PH> : advance_kernel<3, true, PF>;
+            return st == GR_STORE_BF16 ? advance_kernel<3, false, PB>
+                 : st == GR_STORE_F16 ? advance_kernel<3, false, PH> : advance_kernel<3, false, PF>;
+        }
+        if (rk4) return st == GR_STORE_BF16 ? advance_kernel<2, true, PB>
+                      : st == GR_STORE_F16 ? advance_kernel<2, true, PH> : advance_kernel<2, true, PF>;
+        return st == GR_STORE_BF16 ? advance_kernel<2, false, PB>
+             : st == GR_STORE_F16 ? advance_kernel<2, false, PH> : advance_kernel<2, false, PF>;
+    }
     if (e->dim == 3) {
         if (rk4) return st == GR_STORE_BF16 ? advance_kernel<3, true, __nv_bfloat16>
                       : st == GR_STORE_F16 ? advance_kernel<3, true, __half> : advance_kernel<3, true, float>;
@@ -952,6 +1007,27 @@ cudaEvent_t pool_event(gr_engine *e, size_t k) {
     return e->ev_pool[k];
 }
 
+// Builds the window-pair buffer of window w from its two ring slots (on the compute stream).
+int ensure_pair(gr_engine *e, int64_t w) {
+    const int b = (int)(w & 1);
+    if (e->pair_window[b] == w) return GR_OK;
+    const int elem = (int)(e->wind_stride > 0 ? (e->s.storage == GR_STORE_F32 ? (e->dim == 3 ? 16 : 8) : (e->dim == 3 ? 8 : 4)) : 0);
+    CK(e->pairbuf[b].alloc((size_t)e->nodes * 2 * elem));
+    const char *back = e->wind.p + (int64_t)(w % e->K) * e->wind_stride;
+    const char *front = e->wind.p + (int64_t)((w + 1) % e->K) * e->wind_stride;
+    const int threads = 256, blocks = grid_for(e->nodes, threads);
+    if (elem == 16)
+        pair_pack_kernel<uint4><<<blocks, threads, 0, e->cs>>>((const uint4 *)back, (const uint4 *)front, (uint4 *)e->pairbuf[b].p, e->nodes);
+    else if (elem == 8)
+        pair_pack_kernel<uint2><<<blocks, threads, 0, e->cs>>>((const uint2 *)back, (const uint2 *)front, (uint2 *)e->pairbuf[b].p, e->nodes);
+    else
+        pair_pack_kernel<unsigned><<<blocks, threads, 0, e->cs>>>((const unsigned *)back, (const unsigned *)front, (unsigned *)e->pairbuf[b].p, e->nodes);
+    CK(cudaGetLastError());
+    e->pair_window[b] = w;
+    e->stats.aux_launches++;
+    return GR_OK;
+}
+
 struct RunCtx {
     gr_engine *e;
     KParams P;
@@ -960,11 +1036,16 @@ struct RunCtx {
     size_t ev_used = 0;
 };
 
-int launch_steps(RunCtx &r, int64_t s0, int64_t s1) {
+int launch_steps(RunCtx &r, int64_t s0, int64_t s1, int64_t window) {
     gr_engine *e = r.e;
     KParams P = r.P;
     P.s0 = (int32_t)s0;
     P.s1 = (int32_t)s1;
+    if (e->use_pair) {
+        const int rc = ensure_pair(e, window);
+        if (rc) return rc;
+        P.pair = e->pairbuf[window & 1].p;
+    }
     CK(cudaMemsetAsync(e->counters.p + 1, 0, sizeof(unsigned long long), e->cs));
     cudaEvent_t a = pool_event(e, r.ev_used++), b = pool_event(e, r.ev_used++);
     CK(cudaEventRecord(a, e->cs));
@@ -1081,6 +1162,10 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
     CK(cudaMemsetAsync(e->counters.p, 0, 4 * sizeof(unsigned long long), e->cs));
 
     cudaEvent_t run_a = pool_event(e, 0), run_b = pool_event(e, 1);
+    // window-pair layout: one load per corner returns both snapshots; launches never cross a
+    // window boundary then
+    e->use_pair = e->wind_dynamic && s.layout == 0;
+    e->pair_window[0] = e->pair_window[1] = -1;
     RunCtx r{e, make_params(e), pick_kernel(e), block_size_for(e), 2};
     CK(cudaEventRecord(run_a, e->cs));
     // the first windows read snapshots already uploaded
@@ -1104,7 +1189,7 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
         if (!e->compacting || k_end >= nsteps) return 0;
         if (++launches_since_sort < s.sort_interval) return 0;
         launches_since_sort = 0;
-        int q = compact_pass(e, rec_before[k_end]);
+        int q = compact_pass(e, rec_before[k_end], (int32_t)k_end);
         if (q) return q;
         r.P = make_params(e);
         // live count of the last completed pass: an upper bound of the current one
@@ -1123,7 +1208,7 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
                     alive = e->h_counters[1];
                 }
                 if ((long long)alive < (long long)s.minimum_alive) return 1;
-                int q = launch_steps(r, k, k + 1);
+                int q = launch_steps(r, k, k + 1, sched.steps[k].window);
                 if (q) return q;
                 ++executed;
                 q = after_launch(k + 1);
@@ -1131,12 +1216,15 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
             }
             return 0;
         }
-        for (int64_t k = b; k < t; k += spl) {
-            const int64_t k1 = std::min(t, k + spl);
-            int q = launch_steps(r, k, k1);
+        for (int64_t k = b; k < t;) {
+            int64_t k1 = std::min(t, k + spl);
+            const int64_t w = sched.steps[k].window;
+            if (e->use_pair) k1 = std::min(k1, sched.window_begin[w + 1]);   // one window per launch
+            int q = launch_steps(r, k, k1, w);
             if (q) return q;
             q = after_launch(k1);
             if (q) return q;
+            k = k1;
         }
         executed += t - b;
         return 0;
@@ -1280,8 +1368,41 @@ static int fetch_rows(gr_engine *e, void *out, int64_t capacity, const void *src
     if (rows == 0 || row_used == 0) return GR_OK;
     int rc = set_device(e);
     if (rc) return rc;
-    CK(cudaMemcpy2D(out, row_used * elem, src, row_stride * elem, row_used * elem, rows, cudaMemcpyDeviceToHost));
-    e->stats.d2h_bytes += rows * row_used * (int64_t)elem;
+    const size_t row_bytes = (size_t)row_used * elem, total = row_bytes * (size_t)rows;
+    e->stats.d2h_bytes += (int64_t)total;
+    constexpr size_t kBounce = size_t(64) << 20;
+    if (total < 2 * kBounce || row_bytes > kBounce) {
+        CK(cudaMemcpy2D(out, row_bytes, src, row_stride * elem, row_bytes, rows, cudaMemcpyDeviceToHost));
+        return GR_OK;
+    }
+    // large results: DMA into two pinned bounce buffers, each emptied by a parallel host copy
+    // while the other fills
+    for (auto &b : e->bounce) {
+        if (!b.p) {
+            CK(cudaMallocHost(&b.p, kBounce));
+            b.bytes = kBounce;
+        }
+        if (!b.done) CK(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
+    }
+    const int64_t rows_per = (int64_t)(kBounce / row_bytes);
+    const char *s8 = static_cast<const char *>(src);
+    char *d8 = static_cast<char *>(out);
+    int64_t prev_rows = 0, prev_row0 = 0;
+    int j = 0;
+    for (int64_t r0 = 0; r0 < rows; r0 += rows_per, j ^= 1) {
+        const int64_t nr = std::min(rows_per, rows - r0);
+        CK(cudaMemcpy2DAsync(e->bounce[j].p, row_bytes, s8 + (size_t)r0 * row_stride * elem, row_stride * elem,
+                             row_bytes, nr, cudaMemcpyDeviceToHost, e->cs));
+        CK(cudaEventRecord(e->bounce[j].done, e->cs));
+        if (prev_rows) {
+            CK(cudaEventSynchronize(e->bounce[j ^ 1].done));
+            parallel_memcpy(d8 + (size_t)prev_row0 * row_bytes, e->bounce[j ^ 1].p, (size_t)prev_rows * row_bytes);
+        }
+        prev_rows = nr;
+        prev_row0 = r0;
+    }
+    CK(cudaEventSynchronize(e->bounce[j ^ 1].done));
+    parallel_memcpy(d8 + (size_t)prev_row0 * row_bytes, e->bounce[j ^ 1].p, (size_t)prev_rows * row_bytes);
     return GR_OK;
 }
 

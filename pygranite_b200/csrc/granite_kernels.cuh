@@ -17,6 +17,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cstdint>
+#include <type_traits>
 
 #include "expr.h"
 
@@ -46,6 +47,7 @@ struct KParams {
     // ring buffers: slot s of quantity q starts at base + s * stride
     const void *wind;
     int64_t wind_stride;          // bytes per slot
+    const void *pair;             // window-pair buffer of the launch's window (pair layouts)
     const float *vol;             // [slot][8][plane]
     int64_t vol_plane;            // floats per plane
     const float *cons;            // [slot][4][n_total]
@@ -63,6 +65,8 @@ struct KParams {
     const int32_t *id;            // original particle index
     int64_t n;                    // particles in this launch (prefix of the state arrays)
     const int32_t *n_dev;         // if set: live prefix length on the device (<= n)
+    const int32_t *life;          // if set: steps each slot may run (batched sets of uneven lifetime)
+    int32_t grid_stride;          // 1: persistent grid striding over the live prefix
     int64_t n_state;              // stride of volc / cmpc
     int64_t n_total;              // original particle count (history / constants stride)
     // history, particle-major
@@ -142,6 +146,52 @@ template <> struct Store<__half> {
     static constexpr int bytes3 = 8, bytes2 = 4;
 };
 
+// Window-pair layouts: node n holds the back snapshot's node followed by the front
+// snapshot's node, so one load returns both (32 bytes for float32 3D, 16 bytes for 16-bit 3D or
+// float32 2D, 8 bytes for 16-bit 2D).  Built per window by pair_pack_kernel from the ring.
+template <typename W> struct Pair {};
+
+template <typename W> struct IsPair { static constexpr bool value = false; };
+template <typename W> struct IsPair<Pair<W>> { static constexpr bool value = true; };
+
+template <> struct Store<Pair<float>> {
+    static __device__ __forceinline__ void load3p(const void *base, int32_t idx, float (&b)[3], float (&f)[3]) {
+        float r[8];   // {u_b, v_b, w_b, 0, u_f, v_f, w_f, 0}: one 256-bit load
+        const float *p = reinterpret_cast<const float *>(base) + (int64_t)idx * 8;
+        asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]), "=f"(r[7])
+                     : "l"(p));
+        b[0] = r[0]; b[1] = r[1]; b[2] = r[2];
+        f[0] = r[4]; f[1] = r[5]; f[2] = r[6];
+    }
+    static __device__ __forceinline__ void load2p(const void *base, int32_t idx, float (&b)[2], float (&f)[2]) {
+        const float4 q = __ldg(reinterpret_cast<const float4 *>(base) + idx);
+        b[0] = q.x; b[1] = q.y; f[0] = q.z; f[1] = q.w;
+    }
+    static constexpr int bytes3 = 32, bytes2 = 16;
+};
+
+template <typename H> struct Store<Pair<H>> {
+    static __device__ __forceinline__ float2 cvt(unsigned q) {
+        if constexpr (sizeof(H) == 2 && std::is_same<H, __half>::value)
+            return __half22float2(*reinterpret_cast<const __half2 *>(&q));
+        else
+            return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&q));
+    }
+    static __device__ __forceinline__ void load3p(const void *base, int32_t idx, float (&b)[3], float (&f)[3]) {
+        const uint4 q = __ldg(reinterpret_cast<const uint4 *>(base) + idx);
+        const float2 b01 = cvt(q.x), b2 = cvt(q.y), f01 = cvt(q.z), f2 = cvt(q.w);
+        b[0] = b01.x; b[1] = b01.y; b[2] = b2.x;
+        f[0] = f01.x; f[1] = f01.y; f[2] = f2.x;
+    }
+    static __device__ __forceinline__ void load2p(const void *base, int32_t idx, float (&b)[2], float (&f)[2]) {
+        const uint2 q = __ldg(reinterpret_cast<const uint2 *>(base) + idx);
+        const float2 bb = cvt(q.x), ff = cvt(q.y);
+        b[0] = bb.x; b[1] = bb.y; f[0] = ff.x; f[1] = ff.y;
+    }
+    static constexpr int bytes3 = 16, bytes2 = 8;
+};
+
 // Trilinear corner weights of one sample: indices and border validity.
 struct Cell3 {
     int32_t base;        // node index of corner (ix, iy, iz), clamped into the grid (< 2^31 nodes)
@@ -198,6 +248,29 @@ __device__ __forceinline__ void tri3(const void *slot, const Cell3 &c, float &ou
     ow = lerp_(lerp_(a00, a10, c.fy), lerp_(a01, a11, c.fy), c.fz);
 }
 
+__device__ __forceinline__ float tri_corners(const float (&c)[8], const Cell3 &cl) {
+    const float a00 = lerp_(c[0], c[1], cl.fx), a10 = lerp_(c[2], c[3], cl.fx);
+    const float a01 = lerp_(c[4], c[5], cl.fx), a11 = lerp_(c[6], c[7], cl.fx);
+    return lerp_(lerp_(a00, a10, cl.fy), lerp_(a01, a11, cl.fy), cl.fz);
+}
+
+// Back and front snapshot at once from a window-pair layout; same arithmetic as tri3 on each.
+template <typename W>
+__device__ __forceinline__ void tri3p(const void *pairs, const Cell3 &c, float (&ob)[3], float (&of)[3]) {
+    float u[8], v[8], w[8], uf[8], vf[8], wf[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
+        const int32_t idx = c.base + (dx ? c.sx : 0) + (dy ? c.sy : 0) + (dz ? c.sz : 0);
+        float b[3] = {0.f, 0.f, 0.f}, f[3] = {0.f, 0.f, 0.f};
+        if (c.valid & (1u << k)) Store<W>::load3p(pairs, idx, b, f);
+        u[k] = b[0]; v[k] = b[1]; w[k] = b[2];
+        uf[k] = f[0]; vf[k] = f[1]; wf[k] = f[2];
+    }
+    ob[0] = tri_corners(u, c); ob[1] = tri_corners(v, c); ob[2] = tri_corners(w, c);
+    of[0] = tri_corners(uf, c); of[1] = tri_corners(vf, c); of[2] = tri_corners(wf, c);
+}
+
 // Trilinear interpolation of one scalar float32 plane.
 __device__ __forceinline__ float tri1(const float *plane, const Cell3 &c) {
     float s[8];
@@ -243,6 +316,20 @@ __device__ __forceinline__ void bil2(const void *slot, const Cell2 &c, float &ou
     ov = lerp_(lerp_(v0, v1, c.fx), lerp_(v2, v3, c.fx), c.fy);
 }
 
+template <typename W>
+__device__ __forceinline__ void bil2p(const void *pairs, const Cell2 &c, float (&ob)[2], float (&of)[2]) {
+    float b0[2], f0[2], b1[2], f1[2], b2[2], f2[2], b3[2], f3[2];
+    Store<W>::load2p(pairs, c.i00, b0, f0);
+    Store<W>::load2p(pairs, c.i10, b1, f1);
+    Store<W>::load2p(pairs, c.i01, b2, f2);
+    Store<W>::load2p(pairs, c.i11, b3, f3);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        ob[k] = lerp_(lerp_(b0[k], b1[k], c.fx), lerp_(b2[k], b3[k], c.fx), c.fy);
+        of[k] = lerp_(lerp_(f0[k], f1[k], c.fx), lerp_(f2[k], f3[k], c.fx), c.fy);
+    }
+}
+
 __device__ __forceinline__ float bil1(const float *plane, const Cell2 &c) {
     return lerp_(lerp_(__ldg(plane + c.i00), __ldg(plane + c.i10), c.fx),
                  lerp_(__ldg(plane + c.i01), __ldg(plane + c.i11), c.fx), c.fy);
@@ -265,6 +352,22 @@ __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, co
     V3 r{0.f, 0.f, 0.f};
     const float ax = (p.x - P.off[0]) * P.inv_scale[0];
     const float ay = (p.y - P.off[1]) * P.inv_scale[1];
+    if constexpr (IsPair<W>::value) {
+        // window-pair layout (dynamic wind only): wb points at the pair buffer
+        if (DIM == 3) {
+            const float az = (p.z - P.off[2]) * P.inv_scale[2];
+            const Cell3 c = make_cell3(P, ax, ay, az);
+            float b[3], f[3];
+            tri3p<W>(wb, c, b, f);
+            r.x = lerp_(b[0], f[0], t); r.y = lerp_(b[1], f[1], t); r.z = lerp_(b[2], f[2], t);
+        } else {
+            const Cell2 c = make_cell2(P.nx, P.ny, ax, ay);
+            float b[2], f[2];
+            bil2p<W>(wb, c, b, f);
+            r.x = lerp_(b[0], f[0], t); r.y = lerp_(b[1], f[1], t);
+        }
+        return r;
+    } else {
     if (DIM == 3) {
         const float az = (p.z - P.off[2]) * P.inv_scale[2];
         const Cell3 c = make_cell3(P, ax, ay, az);
@@ -290,6 +393,7 @@ __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, co
         }
     }
     return r;
+    }
 }
 
 // sphere_coordinates (TrajectoryIntegrator.tpp:98-104).
@@ -424,10 +528,10 @@ __device__ __forceinline__ void eval_extras(const KParams &P, const StepEntry &E
 #define GR_ADV_MIN_BLOCKS 2
 #endif
 
+// Advances the particle in slot i through steps [s0, s1) (or until its lifetime ends).
 template <int DIM, bool RK4, typename W>
-__global__ void __launch_bounds__(256, GR_ADV_MIN_BLOCKS) advance_kernel(const __grid_constant__ KParams P) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t n_live = P.n_dev ? (int64_t)*P.n_dev : P.n;
+__device__ __forceinline__ void advance_particle(const KParams &P, const int64_t i, const int64_t n_live,
+                                                 unsigned long long &steps_acc, unsigned &alive_acc) {
     const bool valid = i < n_live;
     int32_t st = valid ? P.status[i] : 1;
     bool alive = st == 0;
@@ -460,6 +564,7 @@ __global__ void __launch_bounds__(256, GR_ADV_MIN_BLOCKS) advance_kernel(const _
     }
     const bool was_alive = alive;
     unsigned long long my_steps = 0;
+    const int32_t life = (valid && P.life) ? P.life[i] : 0x7fffffff;   // steps this particle may run
     const bool extras = (P.volume_mode != 0 && P.nvol > 0) || P.nexpr > 0;
     V3 vc_last{0.f, 0.f, 0.f};
     int last_s = P.s0;
@@ -468,10 +573,10 @@ __global__ void __launch_bounds__(256, GR_ADV_MIN_BLOCKS) advance_kernel(const _
 
     for (int s = P.s0; s < P.s1; ++s) {
         const StepEntry E = P.sched[s];
-        if (alive) {
+        if (alive && s < life) {
             ++my_steps;
             const int sb = P.wind_dynamic ? E.slot_back : 0, sf = P.wind_dynamic ? E.slot_front : 0;
-            const void *wb = reinterpret_cast<const char *>(P.wind) + (int64_t)sb * P.wind_stride;
+            const void *wb = IsPair<W>::value ? P.pair : reinterpret_cast<const char *>(P.wind) + (int64_t)sb * P.wind_stride;
             const void *wf = reinterpret_cast<const char *>(P.wind) + (int64_t)sf * P.wind_stride;
             const float t0 = P.dyn_any ? E.t0 : 0.f;
 
@@ -691,12 +796,31 @@ __global__ void __launch_bounds__(256, GR_ADV_MIN_BLOCKS) advance_kernel(const _
             if (k < P.nexpr) P.cmpc[k * P.n_state + i] = cmp[k];
     }
 
+    steps_acc += my_steps;
+    alive_acc += (valid && alive) ? 1u : 0u;
+}
+
+// One thread per particle, or (P.grid_stride) a persistent grid striding over the live
+// prefix, whose size is read on the device: the launch shape then stays fixed while the live
+// count shrinks, as a captured CUDA graph needs.
+template <int DIM, bool RK4, typename W>
+__global__ void __launch_bounds__(256, GR_ADV_MIN_BLOCKS) advance_kernel(const __grid_constant__ KParams P) {
+    const int64_t n_live = P.n_dev ? (int64_t)*P.n_dev : P.n;
+    unsigned long long steps = 0;
+    unsigned alive = 0;
+    if (P.grid_stride) {
+        const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+        for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n_live; base += stride)
+            advance_particle<DIM, RK4, W>(P, base + threadIdx.x, n_live, steps, alive);
+    } else {
+        advance_particle<DIM, RK4, W>(P, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, n_live, steps, alive);
+    }
     // counters: particle-steps and the alive count after the launch (warp-aggregated)
-    const unsigned long long warp_steps = __reduce_add_sync(0xffffffffu, (unsigned)my_steps);
-    const unsigned alive_mask = __ballot_sync(0xffffffffu, valid && alive);
+    const unsigned long long warp_steps = __reduce_add_sync(0xffffffffu, (unsigned)steps);
+    const unsigned warp_alive = __reduce_add_sync(0xffffffffu, alive);
     if ((threadIdx.x & 31) == 0) {
         if (warp_steps) atomicAdd(P.counters, warp_steps);
-        if (alive_mask) atomicAdd(P.counters + 1, (unsigned long long)__popc(alive_mask));
+        if (warp_alive) atomicAdd(P.counters + 1, (unsigned long long)warp_alive);
     }
 }
 

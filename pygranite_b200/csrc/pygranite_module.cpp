@@ -75,6 +75,7 @@ struct IntegratorSettings {
     int32_t SortInterval{0};
     int32_t BlockSize{0};
     int32_t Device{0};
+    int32_t WindLayout{0};
 };
 
 class DataLoader {
@@ -311,6 +312,7 @@ class TrajectoryIntegrator {
         s.sort_interval = S.SortInterval;
         s.block_size = S.BlockSize;
         s.device = S.Device;
+        s.layout = S.WindLayout;
         check(gr_create(&s, &engine_));
         check(gr_set_seeds(engine_, seeds_.data(), static_cast<int64_t>(n_), dim_));
     }
@@ -571,7 +573,8 @@ PYBIND11_MODULE(_pygranite, m) {
         .def_readwrite("StepsPerLaunch", &IntegratorSettings::StepsPerLaunch)
         .def_readwrite("SortInterval", &IntegratorSettings::SortInterval)
         .def_readwrite("BlockSize", &IntegratorSettings::BlockSize)
-        .def_readwrite("Device", &IntegratorSettings::Device);
+        .def_readwrite("Device", &IntegratorSettings::Device)
+        .def_readwrite("WindLayout", &IntegratorSettings::WindLayout);
 
     py::class_<TrajectoryIntegrator>(m, "TrajectoryIntegrator")
         .def(py::init<IntegratorSettings &, DataLoader &, TrajectorySet &>(), py::keep_alive<1, 3>())

@@ -244,7 +244,8 @@ def test_loader_exhaustion_truncates_like_reference():
 LAUNCH_SHAPES = [dict(StepsPerLaunch=1), dict(StepsPerLaunch=7), dict(BlockSize=32),
                  dict(BlockSize=256, RingSlots=8), dict(RingSlots=4, StepsPerLaunch=3),
                  dict(SortInterval=1), dict(SortInterval=1, StepsPerLaunch=1), dict(SortInterval=2, StepsPerLaunch=3),
-                 dict(SortInterval=1, RingSlots=8, StepsPerLaunch=5)]
+                 dict(SortInterval=1, RingSlots=8, StepsPerLaunch=5),
+                 dict(WindLayout=1), dict(WindLayout=1, SortInterval=2, StepsPerLaunch=3)]
 
 
 @pytest.mark.parametrize("extra", LAUNCH_SHAPES)
@@ -294,8 +295,9 @@ def round_storage(a, storage):
 STORAGE_P99_BOUND = {"Float32": 1e-4, "Float16": 5e-3, "BFloat16": 3e-2}
 
 
+@pytest.mark.parametrize("layout", [0, 1])
 @pytest.mark.parametrize("storage", ["BFloat16", "Float16", "Float32"])
-def test_precision_forms_against_float64(storage):
+def test_precision_forms_against_float64(storage, layout):
     """Precision form: 16-bit wind storage, float32 stages, Kahan-compensated positions and
     float64 time weights.
     (1) Bit for bit against the float32 oracle with the same compensation on the field
@@ -310,7 +312,7 @@ def test_precision_forms_against_float64(storage):
     settings["CurvatureMode"] = 0
     cell = np.array([1000.0, 1000.0, 250.0])
     eng = H.run_engine(settings, src.wind, seeds, volumes=src.volumes, WindStorage=getattr(pg.WindStorage, storage),
-                       CompensatedPositions=True, Float64Time=True)
+                       CompensatedPositions=True, Float64Time=True, WindLayout=layout)
     rounded = [[round_storage(p, storage) for p in snap] for snap in src.wind]
     ref32 = H.run_oracle(settings, rounded, seeds, volumes=src.volumes, precision="f32", time_mode=1,
                          compensated=True)
