@@ -76,6 +76,9 @@ typedef struct gr_settings {
     int32_t layout;                /* wind layout read by the step kernel: 0 = window pairs when the
                                       windfield is dynamic (one load returns the back and the front
                                       snapshot), 1 = the ring slots directly */
+    int32_t grid_waves;            /* graph runs: resident waves of step-kernel blocks in the
+                                      persistent grid (each thread walks live particles with a
+                                      grid stride); 0 = 1 */
 } gr_settings;
 
 /* Fills *s with the reference's IntegratorSettings defaults (IntegratorSettings.hpp:89-181). */
@@ -191,12 +194,67 @@ int gr_fetch_total_curvature(gr_engine *engine, float *out, int64_t capacity);
 int gr_fetch_curvatures(gr_engine *engine, float *out, int64_t capacity_floats);
 int gr_fetch_volume_info(gr_engine *engine, int32_t index, float *out, int64_t capacity_floats);
 int gr_fetch_compute_info(gr_engine *engine, int32_t index, float *out, int64_t capacity_floats);
+/* The last position record of every particle, (n, dim). */
+int gr_fetch_final_positions(gr_engine *engine, float *out, int64_t capacity_floats);
 
 /* Device-resident variants for callers that keep data on the GPU: the same loads and
  * seeds from device pointers (no host copy). */
 int gr_load_windfield_device(gr_engine *engine, int64_t snapshot, const float *const *components,
                              int32_t n_components, int64_t nz, int64_t ny, int64_t nx);
 int gr_set_seeds_device(gr_engine *engine, const float *positions, int64_t n, int32_t dim);
+
+/* Run options between runs.  No counterpart in the reference (its settings are fixed at
+ * construction).  Everything the loaded data was built for must stay the same: space, the
+ * windfield / constants / volume / uplift modes, grid scale and offset, storage, ring slots,
+ * device (GR_ERR_USER otherwise).  Integrator, border / curvature / abort modes, time step,
+ * lengths, MaximumSimulationTime, SaveInterval and the engine options may change. */
+int gr_update_settings(gr_engine *engine, const gr_settings *settings);
+int gr_settings_get(const gr_engine *engine, gr_settings *out);
+
+/* Per-particle lifetimes in integrator steps (n = the seed count; steps = NULL clears them).
+ * No counterpart in the reference, where every particle runs until MaximumSimulationTime.  A
+ * particle stops after its lifetime: it keeps status Time (0) and its later records repeat
+ * its last state, exactly what a separate run of it with MaximumSimulationTime = lifetime *
+ * DeltaT leaves in its last record.  A run ends after the longest lifetime.  Seed sets of
+ * different lengths on one windfield are batched this way. */
+int gr_set_lifetimes(gr_engine *engine, const int32_t *steps, int64_t n);
+
+/* Batches: several engines run as one CUDA graph.  No counterpart in the reference.
+ * Each engine's whole run (seeding, every step launch, compaction and re-sorting passes,
+ * the final records) is enqueued with fixed launch shapes — the step kernel walks the live
+ * particles with a persistent grid-stride loop over a device-side count — captured on its own
+ * stream, forked from and joined to the batch stream, and instantiated once.  Every
+ * gr_batch_run replays the graph, so results are those of a fresh gr_run of each engine over
+ * the snapshots resident in its ring (its ring must hold every snapshot the run reads, loaded
+ * before the first gr_batch_run; the loader is not called).  MinimumAliveParticles is not
+ * supported (it needs host decisions between steps).  A call that changes an engine (loads,
+ * seeds, lifetimes, settings, expressions, gr_run) makes the next gr_batch_run capture again.
+ * All engines must use the same device. */
+typedef struct gr_batch gr_batch;
+typedef struct gr_batch_stats {
+    double graph_ms;             /* device time of the last replay (CUDA events) */
+    int64_t nodes;               /* graph nodes */
+    int64_t kernel_launches;     /* step-kernel launches per replay */
+    int64_t aux_launches;        /* other kernels and memsets per replay */
+    int64_t particle_steps;      /* summed over the engines, last replay */
+    int64_t captures;            /* graphs built so far */
+    int64_t replays;
+} gr_batch_stats;
+int gr_batch_create(gr_engine *const *engines, int32_t n_engines, gr_batch **out);
+void gr_batch_destroy(gr_batch *batch);
+int gr_batch_run(gr_batch *batch);
+int gr_batch_stats_get(const gr_batch *batch, gr_batch_stats *out);
+
+/* Autotuner: picks the wind layout, block size, sort interval and persistent-grid waves of an
+ * engine by timing short runs (`trial_steps` steps each, resident snapshots, graph launch
+ * shapes) and stores the fastest in its settings.  No counterpart in the reference.  Trials
+ * overwrite the engine's results. */
+typedef struct gr_tune_result {
+    int32_t layout, block_size, sort_interval, grid_waves;
+    double particle_steps_per_s;   /* of the chosen configuration */
+    int32_t trials;
+} gr_tune_result;
+int gr_tune(gr_engine *engine, int32_t trial_steps, gr_tune_result *out);
 
 /* Allocation-free advance of particles between two snapshots.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc — code running while a CUDA

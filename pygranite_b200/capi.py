@@ -23,7 +23,9 @@ EXPORTS = [
     "gr_result_info_get", "gr_stats_get", "gr_fetch_positions", "gr_fetch_status",
     "gr_fetch_lengths", "gr_fetch_total_curvature", "gr_fetch_curvatures",
     "gr_fetch_volume_info", "gr_fetch_compute_info", "gr_load_windfield_device",
-    "gr_set_seeds_device", "gr_plan", "gr_advance_noalloc",
+    "gr_set_seeds_device", "gr_plan", "gr_advance_noalloc", "gr_update_settings", "gr_settings_get",
+    "gr_set_lifetimes", "gr_batch_create", "gr_batch_destroy", "gr_batch_run", "gr_batch_stats_get", "gr_tune",
+    "gr_fetch_final_positions",
 ]
 
 
@@ -39,7 +41,7 @@ class Settings(ctypes.Structure):
         ("offset", ctypes.c_float * 3), ("save_interval", ctypes.c_int64), ("storage", ctypes.c_int32),
         ("time_mode", ctypes.c_int32), ("compensated", ctypes.c_int32), ("ring_slots", ctypes.c_int32),
         ("steps_per_launch", ctypes.c_int32), ("sort_interval", ctypes.c_int32), ("block_size", ctypes.c_int32),
-        ("device", ctypes.c_int32), ("layout", ctypes.c_int32),
+        ("device", ctypes.c_int32), ("layout", ctypes.c_int32), ("grid_waves", ctypes.c_int32),
     ]
 
 
@@ -59,6 +61,17 @@ class Stats(ctypes.Structure):
 class PlanInfo(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_int64), ("windows", ctypes.c_int64), ("records", ctypes.c_int64),
                 ("curvature_records", ctypes.c_int64), ("info_records", ctypes.c_int64)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("graph_ms", ctypes.c_double), ("nodes", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
+                ("aux_launches", ctypes.c_int64), ("particle_steps", ctypes.c_int64), ("captures", ctypes.c_int64),
+                ("replays", ctypes.c_int64)]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("layout", ctypes.c_int32), ("block_size", ctypes.c_int32), ("sort_interval", ctypes.c_int32),
+                ("grid_waves", ctypes.c_int32), ("particle_steps_per_s", ctypes.c_double), ("trials", ctypes.c_int32)]
 
 
 LOADER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64)
@@ -104,6 +117,15 @@ def lib():
             "gr_advance_noalloc": (ctypes.c_int, [ctypes.POINTER(Settings), I64, I64, I64, P, P, ctypes.c_float,
                                                   ctypes.c_float, ctypes.c_float, I32, P, P, P, P, I64, P,
                                                   ctypes.POINTER(ctypes.c_int64)]),
+            "gr_update_settings": (ctypes.c_int, [P, ctypes.POINTER(Settings)]),
+            "gr_settings_get": (ctypes.c_int, [P, ctypes.POINTER(Settings)]),
+            "gr_set_lifetimes": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_int32), I64]),
+            "gr_batch_create": (ctypes.c_int, [ctypes.POINTER(P), I32, ctypes.POINTER(P)]),
+            "gr_batch_destroy": (None, [P]),
+            "gr_batch_run": (ctypes.c_int, [P]),
+            "gr_batch_stats_get": (ctypes.c_int, [P, ctypes.POINTER(BatchStats)]),
+            "gr_tune": (ctypes.c_int, [P, I32, ctypes.POINTER(TuneResult)]),
+            "gr_fetch_final_positions": (ctypes.c_int, [P, FP, I64]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -259,6 +281,40 @@ class Engine:
         s = np.ascontiguousarray(seeds, np.float32)
         _check(lib().gr_set_seeds(self.h, _fp(s), s.shape[0], s.shape[1]))
 
+    def set_seeds_device(self, ptr, n, dim):
+        _check(lib().gr_set_seeds_device(self.h, ptr, n, dim))
+
+    def set_lifetimes(self, steps):
+        """Per-particle lifetimes in steps (None clears them)."""
+        if steps is None:
+            _check(lib().gr_set_lifetimes(self.h, None, 0))
+            return
+        a = np.ascontiguousarray(steps, np.int32)
+        _check(lib().gr_set_lifetimes(self.h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), a.size))
+
+    def settings(self) -> Settings:
+        s = Settings()
+        _check(lib().gr_settings_get(self.h, ctypes.byref(s)))
+        return s
+
+    def update_settings(self, **kw):
+        """Changes run options (gr_update_settings) by field name."""
+        s = self.settings()
+        for k, v in kw.items():
+            setattr(s, k, v)
+        _check(lib().gr_update_settings(self.h, ctypes.byref(s)))
+
+    def tune(self, trial_steps=40) -> TuneResult:
+        r = TuneResult()
+        _check(lib().gr_tune(self.h, trial_steps, ctypes.byref(r)))
+        return r
+
+    def final_positions(self):
+        info = self.info()
+        out = np.empty((info.n, info.dim), np.float32)
+        _check(lib().gr_fetch_final_positions(self.h, _fp(out), out.size))
+        return out
+
     def run(self, loader=None):
         """loader(snapshot) -> 1 / 0 / negative; None = the ring already holds every snapshot."""
         def cb(user, eng, snapshot):
@@ -311,3 +367,32 @@ class Engine:
                 cmps.append(a)
             out["compute_info"] = cmps
         return out
+
+
+class Batch:
+    """gr_batch: the runs of several engines as one CUDA graph (captured on the first run)."""
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        arr = (ctypes.c_void_p * len(self.engines))(*[e.h.value for e in self.engines])
+        self.h = ctypes.c_void_p()
+        _check(lib().gr_batch_create(arr, len(self.engines), ctypes.byref(self.h)))
+
+    def run(self):
+        _check(lib().gr_batch_run(self.h))
+
+    def stats(self) -> BatchStats:
+        s = BatchStats()
+        _check(lib().gr_batch_stats_get(self.h, ctypes.byref(s)))
+        return s
+
+    def close(self):
+        if self.h:
+            lib().gr_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -25,7 +25,9 @@
 
 #include "../../include/granite_b200.h"
 #include "expr.h"
+#include "advance.h"
 #include "compact.cuh"
+#include "engine_graph.h"
 #include "granite_kernels.cuh"
 #include "schedule.h"
 
@@ -126,13 +128,15 @@ __global__ void pair_pack_kernel(const T *__restrict__ back, const T *__restrict
 
 // Seeds (AoS, n x dim) -> state SoA; zeroes the per-particle accumulators.
 __global__ void seed_kernel(const float *__restrict__ seeds, int64_t n, int dim, float *px, float *py,
-                            float *pz, int32_t *status, int32_t *id) {
+                            float *pz, int32_t *status, int32_t *id, const int32_t *__restrict__ life_src,
+                            int32_t *life) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         px[i] = seeds[i * dim];
         py[i] = seeds[i * dim + 1];
         if (dim == 3) pz[i] = seeds[i * dim + 2];
         status[i] = 0;
         id[i] = (int32_t)i;
+        if (life_src) life[i] = life_src[i];
     }
 }
 
@@ -236,6 +240,8 @@ void parallel_memcpy(void *dst, const void *src, size_t bytes) {
 
 }  // namespace
 
+struct RunPlan;
+
 struct gr_engine {
     gr_settings s{};
     int dim = 3;
@@ -295,6 +301,18 @@ struct gr_engine {
     DevBuf<StepEntry> d_sched;
     std::vector<StepEntry> h_sched;
     int64_t L = 0, Lc = 0, Li = 0;
+    std::shared_ptr<RunPlan> plan;     // host plan of the current / last run
+    int64_t step_cap = 0;              // > 0: runs stop after this many steps (trial runs)
+
+    // per-particle lifetimes (steps); a particle stops once it has run its lifetime
+    DevBuf<int32_t> life_src;
+    int64_t life_n = 0;
+    int32_t life_max = 0;
+    bool has_life = false;
+
+    // graph runs
+    uint64_t gen = 0;                  // bumped by every call that may move device buffers
+    int64_t graph_executed = 0, graph_records = 0;
 
     // results
     bool have_result = false;
@@ -401,6 +419,7 @@ int check_shape(gr_engine *e, int64_t nz, int64_t ny, int64_t nx) {
 
 int load_wind(gr_engine *e, int64_t snapshot, const float *const *comps, int32_t ncomp, int64_t nz, int64_t ny,
               int64_t nx, bool device_src) {
+    if (e) ++e->gen;   // device buffers may move: a captured batch is rebuilt
     if (!e) return USER_ERR("null engine >");
     if (snapshot < 0) return USER_ERR("negative snapshot index >");
     if (ncomp != e->dim)
@@ -526,6 +545,7 @@ int gr_load_windfield_device(gr_engine *e, int64_t snapshot, const float *const 
 
 int gr_load_volume(gr_engine *e, int64_t snapshot, int32_t index, const float *data, int64_t nz, int64_t ny,
                    int64_t nx) {
+    if (e) ++e->gen;   // device buffers may move: a captured batch is rebuilt
     if (!e || !data) return USER_ERR("null argument >");
     if (index < 0 || index >= GR_MAX_VOLUMES) return USER_ERR("You provided more additional volumes than supported. >");
     if (!e->grid_set) return USER_ERR("The windfield must be loaded before additional volumes. >");
@@ -554,6 +574,7 @@ int gr_load_volume(gr_engine *e, int64_t snapshot, int32_t index, const float *d
 }
 
 int gr_load_constant(gr_engine *e, int64_t snapshot, int32_t index, const float *data, int64_t n) {
+    if (e) ++e->gen;   // device buffers may move: a captured batch is rebuilt
     if (!e || !data) return USER_ERR("null argument >");
     if (index < 0 || index >= GR_MAX_CONSTANTS) return USER_ERR("You provided more constants than supported. >");
     if (e->n <= 0) return USER_ERR("Seeds must be set before constants. >");
@@ -580,6 +601,7 @@ int gr_load_constant(gr_engine *e, int64_t snapshot, int32_t index, const float 
 }
 
 int gr_load_uplift(gr_engine *e, int64_t snapshot, const float *data, int64_t n, int32_t dim) {
+    if (e) ++e->gen;   // device buffers may move: a captured batch is rebuilt
     if (!e || !data) return USER_ERR("null argument >");
     if (e->n <= 0) return USER_ERR("Seeds must be set before the uplift. >");
     if (n != e->n) return USER_ERR("Uplift dimension does not match number of particles. >");
@@ -606,6 +628,7 @@ int gr_load_uplift(gr_engine *e, int64_t snapshot, const float *data, int64_t n,
 }
 
 int gr_set_topography(gr_engine *e, const float *data, int64_t ny, int64_t nx) {
+    if (e) ++e->gen;   // device buffers may move: a captured batch is rebuilt
     if (!e || !data) return USER_ERR("null argument >");
     if (!e->grid_set) return USER_ERR("The windfield must be loaded before the topography. >");
     if (nx != e->nx || ny != e->ny) return USER_ERR("Topography dimensions does not match to provided data! >");
@@ -619,6 +642,7 @@ int gr_set_topography(gr_engine *e, const float *data, int64_t ny, int64_t nx) {
 
 int gr_compile_expression(gr_engine *e, int32_t index, const char *code, const char *const *volume_names,
                           int32_t n_volumes, const char *const *constant_names, int32_t n_constants) {
+    if (e) ++e->gen;   // device buffers may move: a captured batch is rebuilt
     if (!e || !code) return USER_ERR("null argument >");
     if (index < 0 || index >= GR_MAX_EXPRESSIONS) return USER_ERR("At most 4 AdditionalCompute expressions are supported. >");
     std::vector<std::string> vn, cn;
@@ -691,6 +715,7 @@ int gr_expression_evaluate(const char *code, const char *const *volume_names, in
 }
 
 static int set_seeds(gr_engine *e, const float *pos, int64_t n, int32_t dim, bool device_src) {
+    if (e) ++e->gen;   // device buffers may move: a captured batch is rebuilt
     if (!e || (!pos && n > 0)) return USER_ERR("null argument >");
     if (dim != e->dim) return USER_ERR("Dimensions of IntegratorSettings and provided TrajectorySet do not match. >");
     if (n <= 0) return USER_ERR("Provided TrajectorySet does not contain any data. >");
@@ -708,9 +733,76 @@ static int set_seeds(gr_engine *e, const float *pos, int64_t n, int32_t dim, boo
 int gr_set_seeds(gr_engine *e, const float *pos, int64_t n, int32_t dim) { return set_seeds(e, pos, n, dim, false); }
 int gr_set_seeds_device(gr_engine *e, const float *pos, int64_t n, int32_t dim) { return set_seeds(e, pos, n, dim, true); }
 
+int gr_set_lifetimes(gr_engine *e, const int32_t *steps, int64_t n) {
+    if (!e) return USER_ERR("null engine >");
+    ++e->gen;
+    if (!steps || n == 0) {
+        e->has_life = false;
+        e->life_n = 0;
+        e->life_max = 0;
+        return GR_OK;
+    }
+    if (n < 0 || n > (int64_t(1) << 31) - 1) return USER_ERR("Invalid lifetime count. >");
+    int32_t mx = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (steps[i] < 0) return USER_ERR("Lifetimes must not be negative. >");
+        mx = std::max(mx, steps[i]);
+    }
+    int rc = set_device(e);
+    if (rc) return rc;
+    CK(e->life_src.alloc((size_t)n));
+    CK(cudaMemcpy(e->life_src.p, steps, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    e->stats.h2d_bytes += n * (int64_t)sizeof(int32_t);
+    e->has_life = true;
+    e->life_n = n;
+    e->life_max = mx;
+    return GR_OK;
+}
+
+int gr_update_settings(gr_engine *e, const gr_settings *s) {
+    if (!e || !s) return USER_ERR("null argument >");
+    const gr_settings &o = e->s;
+    // what the loaded data and the ring were built for stays fixed
+    const bool same = s->space == o.space && s->windfield_mode == o.windfield_mode &&
+                      s->constants_mode == o.constants_mode && s->volume_mode == o.volume_mode &&
+                      (e->dim == 2 || s->uplift_mode == o.uplift_mode) && s->storage == o.storage &&
+                      (s->ring_slots >= 3 ? s->ring_slots : 3) == e->K && s->device == o.device &&
+                      s->grid_scale_len == o.grid_scale_len && s->offset_len == o.offset_len &&
+                      std::memcmp(s->grid_scale, o.grid_scale, sizeof o.grid_scale) == 0 &&
+                      std::memcmp(s->offset, o.offset, sizeof o.offset) == 0;
+    if (!same)
+        return USER_ERR("Only run options can change after creation (space, modes, grid, storage, ring and device are fixed). >");
+    if (s->delta_t <= 0.f || !std::isfinite(s->delta_t)) return USER_ERR("DeltaT must be positive. >");
+    if (s->data_time_distance <= 0.f || !std::isfinite(s->data_time_distance))
+        return USER_ERR("DataTimeDistance must be positive. >");
+    if (!std::isfinite(s->maximum_simulation_time)) return USER_ERR("MaximumSimulationTime must be finite. >");
+    if (s->maximum_simulation_time / s->delta_t > 5.0e8f) return USER_ERR("Too many integration steps requested. >");
+    if (s->save_interval < 0) return USER_ERR("SaveInterval must not be negative. >");
+    ++e->gen;
+    const int32_t uplift = e->s.uplift_mode;
+    e->s = *s;
+    e->s.uplift_mode = uplift;
+    return GR_OK;
+}
+
+int gr_settings_get(const gr_engine *e, gr_settings *out) {
+    if (!e || !out) return USER_ERR("null argument >");
+    *out = e->s;
+    return GR_OK;
+}
+
 }  // extern "C"
 
 // ====================================================================== run
+
+// Host plan of one run: the step schedule, record bookkeeping and launch granularity.
+struct RunPlan {
+    Schedule sched;
+    int64_t nsteps = 0, nwin = 0;
+    std::vector<int32_t> rec_before;   // records written before step k: 1 + saves in [0, k)
+    int64_t spl = 0;                   // steps per launch
+    bool graph = false;                // fixed launch shapes and no host reads (graph capture)
+};
 
 namespace {
 
@@ -721,6 +813,7 @@ int alloc_set(gr_engine *e, gr_engine::State &S, bool retired) {
     if (e->dim == 3) CK(S.pz.alloc(N));
     CK(S.status.alloc(N)); CK(S.id.alloc(N));
     if (retired) CK(S.retire.alloc(N));
+    if (!retired && e->has_life) CK(S.life.alloc(N));
     if (!retired && (cm == 1 || cm == 3)) { CK(S.qx.alloc(N)); CK(S.qy.alloc(N)); CK(S.qz.alloc(N)); }
     if (!retired && e->s.compensated) { CK(S.kx.alloc(N)); CK(S.ky.alloc(N)); CK(S.kz.alloc(N)); }
     if (!retired && cm == 2) { CK(S.lx.alloc(N)); CK(S.ly.alloc(N)); CK(S.lz.alloc(N)); }
@@ -730,43 +823,23 @@ int alloc_set(gr_engine *e, gr_engine::State &S, bool retired) {
     return GR_OK;
 }
 
+// Device buffers and host tables of a run; enqueues no device work.
 int alloc_state(gr_engine *e) {
-    const int64_t n = e->n;
-    const size_t N = (size_t)n;
-    e->cur = 0;
+    const size_t N = (size_t)e->n;
     int rc = alloc_set(e, e->st[0], false);
     if (rc) return rc;
-    gr_engine::State &S = e->st[0];
-    if (e->s.compensated) {
-        CK(cudaMemsetAsync(S.kx.p, 0, N * 4, e->cs)); CK(cudaMemsetAsync(S.ky.p, 0, N * 4, e->cs));
-        CK(cudaMemsetAsync(S.kz.p, 0, N * 4, e->cs));
-    }
-    if (e->s.curvature_mode == 2) {
-        CK(cudaMemsetAsync(S.lx.p, 0, N * 4, e->cs)); CK(cudaMemsetAsync(S.ly.p, 0, N * 4, e->cs));
-        CK(cudaMemsetAsync(S.lz.p, 0, N * 4, e->cs));
-    }
-    CK(cudaMemsetAsync(S.length.p, 0, N * 4, e->cs));
-    CK(cudaMemsetAsync(S.tc.p, 0, N * 4, e->cs));
-    CK(cudaMemsetAsync(S.curv.p, 0, N * 4, e->cs));
-    const int nv = std::max(1, e->nvol), ne = std::max(1, e->nexpr);
-    CK(cudaMemsetAsync(S.volc.p, 0, N * nv * 4, e->cs));
-    CK(cudaMemsetAsync(S.cmpc.p, 0, N * ne * 4, e->cs));
     CK(e->out_status.alloc(N)); CK(e->out_length.alloc(N)); CK(e->out_tc.alloc(N));
     e->compacting = e->s.sort_interval > 0;
     CK(e->d_counts.alloc(4));
-    {
-        const int32_t init[4] = {(int32_t)n, (int32_t)n, 0, 0};
-        CK(cudaMemcpyAsync(e->d_counts.p, init, sizeof init, cudaMemcpyHostToDevice, e->cs));
-    }
-    if (e->compacting) {
-        rc = alloc_set(e, e->st[1], false);
-        if (rc) return rc;
-        rc = alloc_set(e, e->ret, true);
-        if (rc) return rc;
-        CK(e->c_key.alloc(N));
-        if (!e->h_live) CK(cudaMallocHost(&e->h_live, sizeof(int32_t)));
-        *e->h_live = (int32_t)n;
-        if (!e->live_ready) CK(cudaEventCreateWithFlags(&e->live_ready, cudaEventDisableTiming));
+    if (!e->compacting) return GR_OK;
+    rc = alloc_set(e, e->st[1], false);
+    if (rc) return rc;
+    rc = alloc_set(e, e->ret, true);
+    if (rc) return rc;
+    CK(e->c_key.alloc(N));
+    if (!e->h_live) CK(cudaMallocHost(&e->h_live, sizeof(int32_t)));
+    if (!e->live_ready) CK(cudaEventCreateWithFlags(&e->live_ready, cudaEventDisableTiming));
+    if (e->nbins == 0) {
         // Morton-ranked brick table (bricks of bx x by x bz nodes)
         e->bx = 4; e->by = 4; e->bz = e->dim == 3 ? 2 : 1;
         for (;;) {
@@ -797,15 +870,219 @@ int alloc_state(gr_engine *e) {
         for (int32_t r = 0; r < e->nbins; ++r) tab[codes[r].second] = r;
         CK(e->c_bintab.alloc(tab.size()));
         CK(cudaMemcpy(e->c_bintab.p, tab.data(), tab.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
-        CK(e->c_hist.alloc((size_t)e->nbins + 1));
-        CK(e->c_chunk.alloc((size_t)(e->nbins + 1 + SCAN_CHUNK - 1) / SCAN_CHUNK));
-        CK(e->c_perm.alloc(N));
     }
+    CK(e->c_hist.alloc((size_t)e->nbins + 1));
+    CK(e->c_chunk.alloc((size_t)(e->nbins + 1 + SCAN_CHUNK - 1) / SCAN_CHUNK));
+    CK(e->c_perm.alloc(N));
+    return GR_OK;
+}
+
+__global__ void init_counts_kernel(int32_t *counts, int32_t n) {
+    counts[0] = n;   // live
+    counts[1] = n;   // live after the last pass
+    counts[2] = 0;   // retired
+    counts[3] = 0;
+}
+
+// Device start of a run on the compute stream: zeroed accumulators and counters, live and
+// retired counts, seeds -> state, record 0.  Capturable.
+int reset_state(gr_engine *e) {
+    const int64_t n = e->n;
+    const size_t N = (size_t)n;
+    e->cur = 0;
+    gr_engine::State &S = e->st[0];
+    if (e->s.compensated) {
+        CK(cudaMemsetAsync(S.kx.p, 0, N * 4, e->cs)); CK(cudaMemsetAsync(S.ky.p, 0, N * 4, e->cs));
+        CK(cudaMemsetAsync(S.kz.p, 0, N * 4, e->cs));
+    }
+    if (e->s.curvature_mode == 2) {
+        CK(cudaMemsetAsync(S.lx.p, 0, N * 4, e->cs)); CK(cudaMemsetAsync(S.ly.p, 0, N * 4, e->cs));
+        CK(cudaMemsetAsync(S.lz.p, 0, N * 4, e->cs));
+    }
+    CK(cudaMemsetAsync(S.length.p, 0, N * 4, e->cs));
+    CK(cudaMemsetAsync(S.tc.p, 0, N * 4, e->cs));
+    CK(cudaMemsetAsync(S.curv.p, 0, N * 4, e->cs));
+    const int nv = std::max(1, e->nvol), ne = std::max(1, e->nexpr);
+    CK(cudaMemsetAsync(S.volc.p, 0, N * nv * 4, e->cs));
+    CK(cudaMemsetAsync(S.cmpc.p, 0, N * ne * 4, e->cs));
+    init_counts_kernel<<<1, 1, 0, e->cs>>>(e->d_counts.p, (int32_t)n);
     const int threads = 256;
     seed_kernel<<<grid_for(n, threads), threads, 0, e->cs>>>(e->seeds.p, n, e->dim, S.px.p, S.py.p, S.pz.p,
-                                                             S.status.p, S.id.p);
+                                                             S.status.p, S.id.p,
+                                                             e->has_life ? e->life_src.p : nullptr, S.life.p);
+    seed_record_kernel<<<grid_for(n, threads), threads, 0, e->cs>>>(e->seeds.p, n, e->dim, e->hpos.p, e->L);
     CK(cudaGetLastError());
-    e->stats.aux_launches++;
+    CK(cudaMemsetAsync(e->counters.p, 0, 4 * sizeof(unsigned long long), e->cs));
+    if (e->compacting) *e->h_live = (int32_t)n;
+    e->stats.aux_launches += 3;
+    return GR_OK;
+}
+
+// Snapshots 0 .. m-1 resident in the ring for every quantity the run reloads per snapshot.
+int64_t resident_prefix(const gr_engine *e) {
+    const bool vol_dyn = e->s.volume_mode == 2 && e->nvol > 0;
+    const bool con_dyn = e->s.constants_mode == 2 && e->ncon > 0;
+    const bool lift_dyn = e->s.uplift_mode == 2 && e->has_uplift;
+    int64_t m = 0;
+    for (; m < e->K; ++m) {
+        const bool wind_ok = e->wind_dynamic ? e->wind_holds[m] == m : (m > 0 || e->wind_holds[0] == 0);
+        if (!wind_ok || (vol_dyn && e->vol_holds[m] != m) || (con_dyn && e->cons_holds[m] != m) ||
+            (lift_dyn && e->lift_holds[m] != m))
+            break;
+    }
+    return m;
+}
+
+// Keeps the first `steps` steps of a schedule.
+void truncate_schedule(Schedule &sc, int64_t steps) {
+    if ((int64_t)sc.steps.size() <= steps) return;
+    sc.steps.resize((size_t)steps);
+    std::vector<int64_t> wb;
+    for (int64_t b : sc.window_begin)
+        if (b < steps) wb.push_back(b);
+    wb.push_back(steps);
+    sc.window_begin = wb;
+}
+
+// Channel-record index of each position record, for records written in steps [0, executed).
+std::vector<int32_t> crec_table(const gr_engine *e, const RunPlan &R, int64_t executed) {
+    std::vector<int32_t> t((size_t)e->L + 1, -1);
+    int64_t rr = 1, cc = 0;
+    for (int64_t k = 0; k < executed; ++k)
+        if (R.sched.steps[k].save) {
+            if (R.sched.steps[k].time_pos) t[rr] = (int32_t)cc++;
+            ++rr;
+        }
+    if (e->s.save_interval == 0 && executed > 0) t[rr] = (int32_t)cc;   // the final record
+    return t;
+}
+
+int ensure_pair(gr_engine *e, int64_t w);
+
+int pair_elem(const gr_engine *e) {
+    return e->s.storage == GR_STORE_F32 ? (e->dim == 3 ? 16 : 8) : (e->dim == 3 ? 8 : 4);
+}
+
+// Validation, schedule, device schedule and programs, state and history buffers.
+int run_prepare(gr_engine *e, RunPlan &R, bool graph) {
+    if (!e) return USER_ERR("null engine >");
+    g_last_error.clear();
+    int rc = set_device(e);
+    if (rc) return rc;
+    rc = ensure_particles(e);
+    if (rc) return rc;
+    if (!e->grid_set) return USER_ERR("No windfield was loaded. >");
+    if (e->wind_holds[0] != 0)
+        return USER_ERR("Snapshot 0 is no longer resident in the ring; load the data again to run again. >");
+    if (e->dyn_any && e->wind_dynamic && e->wind_holds[1 % e->K] != 1) return USER_ERR("Cannot increment loader. >");
+    const gr_settings &s = e->s;
+    // settings combinations the reference has no kernel variant for
+    // (TrajectoryIntegrator.gen.py:52-53 and the 2D curvature axis, gen.py:184-187)
+    if (e->dim == 2 && (s.curvature_mode == 1 || s.curvature_mode == 3))
+        return USER_ERR("No kernel could be picked for your settings configuration. >");
+    if (s.constants_mode != 0 && e->nexpr == 0)
+        return USER_ERR("No kernel could be picked for your settings configuration. >");
+    if (e->has_life && e->life_n != e->n)
+        return USER_ERR("Lifetimes were set for %lld particles but the set holds %lld. >", (long long)e->life_n,
+                        (long long)e->n);
+    if (graph && s.minimum_alive > 0)
+        return USER_ERR("MinimumAliveParticles needs host decisions between steps; it cannot run in a graph. >");
+    e->have_result = false;
+    ++e->gen;
+    {
+        const int64_t h2d = e->stats.h2d_bytes, d2h = e->stats.d2h_bytes;
+        e->stats = gr_stats{};
+        e->stats.h2d_bytes = h2d;
+        e->stats.d2h_bytes = d2h;
+    }
+
+    ScheduleInput si;
+    si.dyn_any = e->dyn_any;
+    si.wind_dynamic = e->wind_dynamic;
+    si.delta_t = s.delta_t;
+    si.data_time_distance = s.data_time_distance;
+    si.maximum_simulation_time = s.maximum_simulation_time;
+    si.save_interval = s.save_interval;
+    si.time_mode = s.time_mode;
+    R = RunPlan{};
+    R.graph = graph;
+    R.sched = build_schedule(si);
+    // nothing runs after the longest lifetime
+    if (e->has_life) truncate_schedule(R.sched, std::max<int64_t>(0, e->life_max));
+    if (e->step_cap > 0) truncate_schedule(R.sched, e->step_cap);
+    if (graph) {
+        // a graph run covers the windows whose snapshots are all resident now
+        const int64_t m = resident_prefix(e);
+        const int64_t nw = (int64_t)R.sched.window_begin.size() - 1;
+        if (e->dyn_any) {
+            if (m < 2) return USER_ERR("A graph run needs snapshots 0 and 1 resident in the ring. >");
+            if (m - 1 < nw) truncate_schedule(R.sched, R.sched.window_begin[m - 1]);
+        }
+    }
+    R.nsteps = (int64_t)R.sched.steps.size();
+    R.nwin = (int64_t)R.sched.window_begin.size() - 1;
+
+    // records: seed + saves (+ the final record when SaveInterval == 0)
+    int64_t nsaves = 0;
+    for (const auto &st : R.sched.steps) nsaves += st.save;
+    e->L = 1 + nsaves + (s.save_interval == 0 ? 1 : 0);
+    e->Li = e->L - 1;
+    e->Lc = s.curvature_mode == 3 ? e->L - 1 : 0;
+
+    // device schedule
+    e->h_sched.resize(std::max<int64_t>(1, R.nsteps));
+    {
+        int64_t rec = 1, crec = 0, irec = 0;
+        for (int64_t k = 0; k < R.nsteps; ++k) {
+            const HostStep &h = R.sched.steps[k];
+            StepEntry E{};
+            E.t0 = h.t0; E.t1 = h.t1; E.t2 = h.t2;
+            E.flags = (h.save ? SF_SAVE : 0) | (h.time_pos ? SF_TIME_POS : 0) |
+                      (h.save && h.time_pos ? SF_CURV_REC : 0);
+            E.rec = (int32_t)rec; E.crec = (int32_t)crec; E.irec = (int32_t)irec;
+            E.slot_back = (int32_t)(h.window % e->K);
+            E.slot_front = (int32_t)((h.window + 1) % e->K);
+            if (h.save) {
+                ++rec;
+                ++irec;
+                if (h.time_pos) ++crec;
+            }
+            e->h_sched[k] = E;
+        }
+    }
+    CK(e->d_sched.alloc(e->h_sched.size()));
+    CK(cudaMemcpyAsync(e->d_sched.p, e->h_sched.data(), e->h_sched.size() * sizeof(StepEntry), cudaMemcpyHostToDevice, e->cs));
+    CK(e->d_prog.alloc(GR_MAX_EXPR));
+    CK(cudaMemcpyAsync(e->d_prog.p, e->progs, sizeof(e->progs), cudaMemcpyHostToDevice, e->cs));
+
+    rc = alloc_state(e);
+    if (rc) return rc;
+    const size_t N = (size_t)e->n;
+    CK(e->hpos.alloc(N * e->L * e->dim));
+    if (e->Lc > 0) CK(e->hcurv.alloc(N * e->Lc));
+    if (e->nvol > 0 && s.volume_mode != 0 && e->Li > 0) CK(e->hvol.alloc(N * e->Li * e->nvol));
+    if (e->nexpr > 0 && e->Li > 0) CK(e->hcmp.alloc(N * e->Li * e->nexpr));
+
+    R.rec_before.assign((size_t)R.nsteps + 1, 1);
+    for (int64_t k = 0; k < R.nsteps; ++k) R.rec_before[k + 1] = R.rec_before[k] + (R.sched.steps[k].save ? 1 : 0);
+    R.spl = s.steps_per_launch > 0 ? s.steps_per_launch : (int64_t)1 << 40;
+    if (e->compacting && s.steps_per_launch <= 0 && R.nwin > 0)
+        R.spl = std::max<int64_t>(1, R.sched.window_begin[1] - R.sched.window_begin[0]);   // one window per launch
+
+    // window-pair layout: one load per corner returns both snapshots; launches never cross a
+    // window boundary then
+    e->use_pair = e->wind_dynamic && s.layout == 0;
+    e->pair_window[0] = e->pair_window[1] = -1;
+    if (graph) {
+        if (e->use_pair)
+            for (int b = 0; b < 2; ++b) CK(e->pairbuf[b].alloc((size_t)e->nodes * 2 * pair_elem(e)));
+        // the fill-forward table of the full run, uploaded before the capture
+        const std::vector<int32_t> t = crec_table(e, R, R.nsteps);
+        CK(e->crec_of_rec.alloc(t.size()));
+        CK(cudaMemcpyAsync(e->crec_of_rec.p, t.data(), t.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e->cs));
+        CK(cudaStreamSynchronize(e->cs));
+        CK(cudaStreamSynchronize(e->xs));   // snapshot uploads done: the graph waits on nothing outside
+    }
     return GR_OK;
 }
 
@@ -838,7 +1115,7 @@ KParams make_params(gr_engine *e) {
     P.kx = S.kx.p; P.ky = S.ky.p; P.kz = S.kz.p;
     P.lx = S.lx.p; P.ly = S.ly.p; P.lz = S.lz.p;
     P.status = S.status.p; P.length = S.length.p; P.tc = S.tc.p; P.curv = S.curv.p;
-    P.volc = S.volc.p; P.cmpc = S.cmpc.p; P.id = S.id.p; P.life = S.life.p;
+    P.volc = S.volc.p; P.cmpc = S.cmpc.p; P.id = S.id.p; P.life = e->has_life ? S.life.p : nullptr;
     P.n = e->n; P.n_state = e->n; P.n_total = e->n;
     P.n_dev = e->compacting ? e->d_counts.p : nullptr;
     P.hpos = e->hpos.p; P.hcurv = e->hcurv.p; P.hvol = e->hvol.p; P.hcmp = e->hcmp.p;
@@ -870,14 +1147,17 @@ KParams make_params(gr_engine *e) {
     return P;
 }
 
-// One compaction / re-sort pass over the live prefix (compact.cuh).
-int compact_pass(gr_engine *e, int32_t rec_now, int32_t k_end) {
+// One compaction / re-sort pass over the live prefix (compact.cuh).  `graph`: no host copy of
+// the live count.
+int compact_pass(gr_engine *e, int32_t rec_now, int32_t k_end, bool graph) {
     CompactParams C;
     std::memset(&C, 0, sizeof C);
     const int64_t N = e->n;
     C.src = view_of(e->st[e->cur], N);
     C.dst = view_of(e->st[1 - e->cur], N);
     C.ret = view_of(e->ret, N);
+    if (!e->has_life) C.src.life = C.dst.life = nullptr;
+    C.ret.life = nullptr;
     C.key = e->c_key.p;
     C.hist = e->c_hist.p;
     C.chunk = e->c_chunk.p;
@@ -904,7 +1184,8 @@ int compact_pass(gr_engine *e, int32_t rec_now, int32_t k_end) {
     C.rec_now = rec_now;
     C.k_end = k_end;
     const int threads = 256;
-    const int blocks = grid_for(N, threads);
+    // grid-stride kernels over the device live count: a few resident waves cover any count
+    const int blocks = std::min(grid_for(N, threads), 148 * 16);
     const int nchunks = (e->nbins + 1 + SCAN_CHUNK - 1) / SCAN_CHUNK;
     CK(cudaMemsetAsync(e->c_hist.p, 0, ((size_t)e->nbins + 1) * sizeof(int32_t), e->cs));
     bin_kernel<<<blocks, threads, 0, e->cs>>>(C);
@@ -914,8 +1195,10 @@ int compact_pass(gr_engine *e, int32_t rec_now, int32_t k_end) {
     gather_kernel<<<blocks, threads, 0, e->cs>>>(C);
     commit_kernel<<<1, 1, 0, e->cs>>>(C);
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(e->h_live, e->d_counts.p, sizeof(int32_t), cudaMemcpyDeviceToHost, e->cs));
-    CK(cudaEventRecord(e->live_ready, e->cs));
+    if (!graph) {
+        CK(cudaMemcpyAsync(e->h_live, e->d_counts.p, sizeof(int32_t), cudaMemcpyDeviceToHost, e->cs));
+        CK(cudaEventRecord(e->live_ready, e->cs));
+    }
     e->cur = 1 - e->cur;
     e->stats.aux_launches += 6;
     return GR_OK;
@@ -963,31 +1246,8 @@ using KernelFn = void (*)(const KParams);
 KernelFn pick_kernel(const gr_engine *e) {
     const bool rk4 = e->s.integrator == 1;
     const int st = e->s.storage;
-    if (e->use_pair) {
-        using PF = Pair<float>;
-        using PB = Pair<__nv_bfloat16>;
-        using PH = Pair<__half>;
-        if (e->dim == 3) {
-            if (rk4) return st == GR_STORE_BF16 ? advance_kernel<3, true, PB>
-                          : st == GR_STORE_F16 ? advance_kernel<3, true, PH> : advance_kernel<3, true, PF>;
-            return st == GR_STORE_BF16 ? advance_kernel<3, false, PB>
-                 : st == GR_STORE_F16 ? advance_kernel<3, false, PH> : advance_kernel<3, false, PF>;
-        }
-        if (rk4) return st == GR_STORE_BF16 ? advance_kernel<2, true, PB>
-                      : st == GR_STORE_F16 ? advance_kernel<2, true, PH> : advance_kernel<2, true, PF>;
-        return st == GR_STORE_BF16 ? advance_kernel<2, false, PB>
-             : st == GR_STORE_F16 ? advance_kernel<2, false, PH> : advance_kernel<2, false, PF>;
-    }
-    if (e->dim == 3) {
-        if (rk4) return st == GR_STORE_BF16 ? advance_kernel<3, true, __nv_bfloat16>
-                      : st == GR_STORE_F16 ? advance_kernel<3, true, __half> : advance_kernel<3, true, float>;
-        return st == GR_STORE_BF16 ? advance_kernel<3, false, __nv_bfloat16>
-             : st == GR_STORE_F16 ? advance_kernel<3, false, __half> : advance_kernel<3, false, float>;
-    }
-    if (rk4) return st == GR_STORE_BF16 ? advance_kernel<2, true, __nv_bfloat16>
-                  : st == GR_STORE_F16 ? advance_kernel<2, true, __half> : advance_kernel<2, true, float>;
-    return st == GR_STORE_BF16 ? advance_kernel<2, false, __nv_bfloat16>
-         : st == GR_STORE_F16 ? advance_kernel<2, false, __half> : advance_kernel<2, false, float>;
+    return st == GR_STORE_BF16 ? advance_bf16(e->dim, rk4, e->use_pair)
+         : st == GR_STORE_F16 ? advance_f16(e->dim, rk4, e->use_pair) : advance_f32(e->dim, rk4, e->use_pair);
 }
 
 int block_size_for(const gr_engine *e) {
@@ -1011,7 +1271,7 @@ cudaEvent_t pool_event(gr_engine *e, size_t k) {
 int ensure_pair(gr_engine *e, int64_t w) {
     const int b = (int)(w & 1);
     if (e->pair_window[b] == w) return GR_OK;
-    const int elem = (int)(e->wind_stride > 0 ? (e->s.storage == GR_STORE_F32 ? (e->dim == 3 ? 16 : 8) : (e->dim == 3 ? 8 : 4)) : 0);
+    const int elem = pair_elem(e);
     CK(e->pairbuf[b].alloc((size_t)e->nodes * 2 * elem));
     const char *back = e->wind.p + (int64_t)(w % e->K) * e->wind_stride;
     const char *front = e->wind.p + (int64_t)((w + 1) % e->K) * e->wind_stride;
@@ -1030,11 +1290,35 @@ int ensure_pair(gr_engine *e, int64_t w) {
 
 struct RunCtx {
     gr_engine *e;
+    RunPlan *R;
     KParams P;
     KernelFn fn;
     int threads;
-    size_t ev_used = 0;
+    int64_t grid = 0;          // graph runs: persistent grid of the step kernel
+    size_t ev_used = 2;        // events 0 and 1 bracket the run
+    int64_t executed = 0;      // steps enqueued
+    int64_t since_sort = 0;    // launches since the last compaction
 };
+
+int make_ctx(gr_engine *e, RunPlan &R, RunCtx &r) {
+    r = RunCtx{};
+    r.e = e;
+    r.R = &R;
+    r.P = make_params(e);
+    r.fn = pick_kernel(e);
+    r.threads = block_size_for(e);
+    if (R.graph) {
+        // one resident wave (times grid_waves) walks the live prefix with a grid-stride loop
+        int per_sm = 0, sms = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, r.fn, r.threads, 0));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->s.device));
+        const int64_t waves = e->s.grid_waves > 0 ? e->s.grid_waves : 1;
+        const int64_t need = (e->n + r.threads - 1) / r.threads;
+        r.grid = std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)std::max(1, per_sm) * sms * waves));
+        r.P.grid_stride = 1;
+    }
+    return GR_OK;
+}
 
 int launch_steps(RunCtx &r, int64_t s0, int64_t s1, int64_t window) {
     gr_engine *e = r.e;
@@ -1046,6 +1330,12 @@ int launch_steps(RunCtx &r, int64_t s0, int64_t s1, int64_t window) {
         if (rc) return rc;
         P.pair = e->pairbuf[window & 1].p;
     }
+    if (r.R->graph) {
+        r.fn<<<(unsigned)r.grid, r.threads, 0, e->cs>>>(P);
+        CK(cudaGetLastError());
+        e->stats.launches++;
+        return GR_OK;
+    }
     CK(cudaMemsetAsync(e->counters.p + 1, 0, sizeof(unsigned long long), e->cs));
     cudaEvent_t a = pool_event(e, r.ev_used++), b = pool_event(e, r.ev_used++);
     CK(cudaEventRecord(a, e->cs));
@@ -1055,6 +1345,155 @@ int launch_steps(RunCtx &r, int64_t s0, int64_t s1, int64_t window) {
     CK(cudaGetLastError());
     CK(cudaEventRecord(b, e->cs));
     e->stats.launches++;
+    return GR_OK;
+}
+
+// After a launch that ended before step k_end: maybe retire / re-sort (compact.cuh).
+int after_launch(RunCtx &r, int64_t k_end) {
+    gr_engine *e = r.e;
+    const RunPlan &R = *r.R;
+    if (!e->compacting || k_end >= R.nsteps) return 0;
+    if (++r.since_sort < e->s.sort_interval) return 0;
+    r.since_sort = 0;
+    int q = compact_pass(e, R.rec_before[k_end], (int32_t)k_end, R.graph);
+    if (q) return q;
+    const int32_t gs = r.P.grid_stride;
+    r.P = make_params(e);
+    r.P.grid_stride = gs;
+    // live count of the last completed pass: an upper bound of the current one
+    if (!R.graph) r.P.n = std::max<int64_t>(1, *(volatile int32_t *)e->h_live);
+    return 0;
+}
+
+// Steps [b, t): returns 1 when MinimumAliveParticles stopped the run.
+int launch_range(RunCtx &r, int64_t b, int64_t t) {
+    gr_engine *e = r.e;
+    const RunPlan &R = *r.R;
+    if (e->s.minimum_alive > 0) {
+        for (int64_t k = b; k < t; ++k) {
+            // alive() before every step (tpp:973-975)
+            unsigned long long alive = e->n;
+            if (k > 0 || r.executed > 0) {
+                CK(cudaMemcpyAsync(e->h_counters, e->counters.p, 2 * sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToHost, e->cs));
+                CK(cudaStreamSynchronize(e->cs));
+                alive = e->h_counters[1];
+            }
+            if ((long long)alive < (long long)e->s.minimum_alive) return 1;
+            int q = launch_steps(r, k, k + 1, R.sched.steps[k].window);
+            if (q) return q;
+            ++r.executed;
+            q = after_launch(r, k + 1);
+            if (q) return q;
+        }
+        return 0;
+    }
+    for (int64_t k = b; k < t;) {
+        int64_t k1 = std::min(t, k + R.spl);
+        const int64_t w = R.sched.steps[k].window;
+        if (e->use_pair) k1 = std::min(k1, R.sched.window_begin[w + 1]);   // one window per launch
+        int q = launch_steps(r, k, k1, w);
+        if (q) return q;
+        q = after_launch(r, k1);
+        if (q) return q;
+        k = k1;
+    }
+    r.executed += t - b;
+    return 0;
+}
+
+// Record counts after `executed` steps, including the SaveInterval == 0 final record.
+struct RecordCounts {
+    int64_t rec = 1, crec = 0, irec = 0;
+};
+
+RecordCounts count_records(const RunPlan &R, int64_t executed) {
+    RecordCounts c;
+    for (int64_t k = 0; k < executed; ++k)
+        if (R.sched.steps[k].save) {
+            ++c.rec;
+            ++c.irec;
+            if (R.sched.steps[k].time_pos) ++c.crec;
+        }
+    return c;
+}
+
+// After the step loop: the SaveInterval == 0 final record, final per-particle outputs, and the
+// records of retired particles.  Graph runs upload the fill-forward table beforehand.
+int run_tail(RunCtx &r, RecordCounts &c) {
+    gr_engine *e = r.e;
+    const RunPlan &R = *r.R;
+    const gr_settings &s = e->s;
+    const int64_t executed = r.executed;
+    c = count_records(R, executed);
+    KParams P = r.P;
+    if (s.save_interval == 0) {
+        const bool tpos = executed > 0;   // data.Time > 0 after at least one step
+        if (e->dim == 3)
+            save_state_kernel<3><<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, (int32_t)c.rec, (int32_t)c.crec, (int32_t)c.irec, tpos);
+        else
+            save_state_kernel<2><<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, (int32_t)c.rec, (int32_t)c.crec, (int32_t)c.irec, tpos);
+        CK(cudaGetLastError());
+        ++c.rec;
+        ++c.irec;
+        if (tpos) ++c.crec;
+        e->stats.aux_launches++;
+    }
+    finalize_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, e->out_status.p, e->out_length.p, e->out_tc.p);
+    CK(cudaGetLastError());
+    e->stats.aux_launches++;
+    if (e->compacting) {
+        // retired particles: their later records repeat the frozen state
+        std::vector<int32_t> t;
+        if (!R.graph) {
+            t = crec_table(e, R, executed);
+            CK(e->crec_of_rec.alloc(t.size()));
+            CK(cudaMemcpyAsync(e->crec_of_rec.p, t.data(), t.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e->cs));
+        }
+        const StateView Rv = view_of(e->ret, e->n);
+        fill_forward_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, Rv, e->d_counts.p + 2, e->crec_of_rec.p,
+                                                                     (int32_t)c.rec);
+        finalize_retired_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(Rv, e->d_counts.p + 2, s.abort_mode != 0,
+                                                                         s.curvature_mode != 0, e->out_status.p,
+                                                                         e->out_length.p, e->out_tc.p);
+        CK(cudaGetLastError());
+        if (!R.graph) CK(cudaStreamSynchronize(e->cs));   // the host table t is read by the copy above
+        e->stats.aux_launches += 2;
+    }
+    return GR_OK;
+}
+
+// After the device work finished: counters, timings and result sizes.
+int run_collect(gr_engine *e, const RunPlan &R, int64_t executed, int64_t windows_run, const RecordCounts &c,
+                size_t ev_used) {
+    const gr_settings &s = e->s;
+    CK(cudaMemcpyAsync(e->h_counters, e->counters.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->cs));
+    CK(cudaStreamSynchronize(e->cs));
+    if (ev_used >= 2) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e->ev_pool[0], e->ev_pool[1]));
+        e->stats.run_ms = ms;
+        double kms = 0.0;
+        for (size_t k = 2; k + 1 < ev_used; k += 2) {
+            float t = 0.f;
+            CK(cudaEventElapsedTime(&t, e->ev_pool[k], e->ev_pool[k + 1]));
+            kms += t;
+        }
+        e->stats.kernel_ms = kms;
+    }
+    e->stats.particle_steps = (int64_t)e->h_counters[0];
+    (void)R;
+    e->info.n = e->n;
+    e->info.dim = e->dim;
+    e->info.records = c.rec;
+    e->info.curvature_records = s.curvature_mode == 3 ? c.crec : 0;
+    e->info.info_records = c.irec;
+    e->info.steps = executed;
+    e->info.windows = windows_run;
+    e->info.particle_steps = (int64_t)e->h_counters[0];
+    e->info.n_volumes = s.volume_mode != 0 ? e->nvol : 0;
+    e->info.n_expressions = e->nexpr;
+    e->have_result = true;
     return GR_OK;
 }
 
@@ -1081,155 +1520,29 @@ int call_loader(gr_engine *e, gr_loader_fn loader, void *user, int64_t snapshot,
 
 extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
     if (!e) return USER_ERR("null engine >");
-    g_last_error.clear();
-    int rc = set_device(e);
+    if (!e->plan) e->plan = std::make_unique<RunPlan>();
+    RunPlan &R = *e->plan;
+    int rc = run_prepare(e, R, false);
     if (rc) return rc;
-    rc = ensure_particles(e);
+    rc = reset_state(e);
     if (rc) return rc;
-    if (!e->grid_set) return USER_ERR("No windfield was loaded. >");
-    if (e->wind_holds[0] != 0)
-        return USER_ERR("Snapshot 0 is no longer resident in the ring; load the data again to run again. >");
-    if (e->dyn_any && e->wind_dynamic && e->wind_holds[1 % e->K] != 1) return USER_ERR("Cannot increment loader. >");
     const gr_settings &s = e->s;
-    // settings combinations the reference has no kernel variant for
-    // (TrajectoryIntegrator.gen.py:52-53 and the 2D curvature axis, gen.py:184-187)
-    if (e->dim == 2 && (s.curvature_mode == 1 || s.curvature_mode == 3))
-        return USER_ERR("No kernel could be picked for your settings configuration. >");
-    if (s.constants_mode != 0 && e->nexpr == 0)
-        return USER_ERR("No kernel could be picked for your settings configuration. >");
-    e->have_result = false;
-    {
-        const int64_t h2d = e->stats.h2d_bytes, d2h = e->stats.d2h_bytes;
-        e->stats = gr_stats{};
-        e->stats.h2d_bytes = h2d;
-        e->stats.d2h_bytes = d2h;
-    }
-
-    ScheduleInput si;
-    si.dyn_any = e->dyn_any;
-    si.wind_dynamic = e->wind_dynamic;
-    si.delta_t = s.delta_t;
-    si.data_time_distance = s.data_time_distance;
-    si.maximum_simulation_time = s.maximum_simulation_time;
-    si.save_interval = s.save_interval;
-    si.time_mode = s.time_mode;
-    const Schedule sched = build_schedule(si);
-    const int64_t nsteps = (int64_t)sched.steps.size();
-    const int64_t nwin = (int64_t)sched.window_begin.size() - 1;
-
-    // records: seed + saves (+ the final record when SaveInterval == 0)
-    int64_t nsaves = 0;
-    for (const auto &st : sched.steps) nsaves += st.save;
-    e->L = 1 + nsaves + (s.save_interval == 0 ? 1 : 0);
-    e->Li = e->L - 1;
-    e->Lc = s.curvature_mode == 3 ? e->L - 1 : 0;
-
-    // device schedule
-    e->h_sched.resize(std::max<int64_t>(1, nsteps));
-    {
-        int64_t rec = 1, crec = 0, irec = 0;
-        for (int64_t k = 0; k < nsteps; ++k) {
-            const HostStep &h = sched.steps[k];
-            StepEntry E{};
-            E.t0 = h.t0; E.t1 = h.t1; E.t2 = h.t2;
-            E.flags = (h.save ? SF_SAVE : 0) | (h.time_pos ? SF_TIME_POS : 0) |
-                      (h.save && h.time_pos ? SF_CURV_REC : 0);
-            E.rec = (int32_t)rec; E.crec = (int32_t)crec; E.irec = (int32_t)irec;
-            E.slot_back = (int32_t)(h.window % e->K);
-            E.slot_front = (int32_t)((h.window + 1) % e->K);
-            if (h.save) {
-                ++rec;
-                ++irec;
-                if (h.time_pos) ++crec;
-            }
-            e->h_sched[k] = E;
-        }
-    }
-    CK(e->d_sched.alloc(e->h_sched.size()));
-    CK(cudaMemcpyAsync(e->d_sched.p, e->h_sched.data(), e->h_sched.size() * sizeof(StepEntry), cudaMemcpyHostToDevice, e->cs));
-    CK(e->d_prog.alloc(GR_MAX_EXPR));
-    CK(cudaMemcpyAsync(e->d_prog.p, e->progs, sizeof(e->progs), cudaMemcpyHostToDevice, e->cs));
-
-    rc = alloc_state(e);
-    if (rc) return rc;
-    const size_t N = (size_t)e->n;
-    CK(e->hpos.alloc(N * e->L * e->dim));
-    if (e->Lc > 0) CK(e->hcurv.alloc(N * e->Lc));
-    if (e->nvol > 0 && s.volume_mode != 0 && e->Li > 0) CK(e->hvol.alloc(N * e->Li * e->nvol));
-    if (e->nexpr > 0 && e->Li > 0) CK(e->hcmp.alloc(N * e->Li * e->nexpr));
-    seed_record_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(e->seeds.p, e->n, e->dim, e->hpos.p, e->L);
-    CK(cudaGetLastError());
-    CK(cudaMemsetAsync(e->counters.p, 0, 4 * sizeof(unsigned long long), e->cs));
 
     cudaEvent_t run_a = pool_event(e, 0), run_b = pool_event(e, 1);
-    // window-pair layout: one load per corner returns both snapshots; launches never cross a
-    // window boundary then
-    e->use_pair = e->wind_dynamic && s.layout == 0;
-    e->pair_window[0] = e->pair_window[1] = -1;
-    RunCtx r{e, make_params(e), pick_kernel(e), block_size_for(e), 2};
+    RunCtx r;
+    rc = make_ctx(e, R, r);
+    if (rc) return rc;
     CK(cudaEventRecord(run_a, e->cs));
     // the first windows read snapshots already uploaded
     for (int k = 0; k < e->K; ++k)
         if (e->wind_holds[k] >= 0 || e->vol_holds[k] >= 0 || e->cons_holds[k] >= 0 || e->lift_holds[k] >= 0)
             CK(cudaStreamWaitEvent(e->cs, e->slot_ready[k], 0));
 
-    // records written before step k: 1 + saves in [0, k)
-    std::vector<int32_t> rec_before((size_t)nsteps + 1, 1);
-    for (int64_t k = 0; k < nsteps; ++k) rec_before[k + 1] = rec_before[k] + (sched.steps[k].save ? 1 : 0);
-    int64_t spl = s.steps_per_launch > 0 ? s.steps_per_launch : (int64_t)1 << 40;
-    if (e->compacting && s.steps_per_launch <= 0 && nwin > 0)
-        spl = std::max<int64_t>(1, sched.window_begin[1] - sched.window_begin[0]);   // one window per launch
+    const int64_t nwin = R.nwin;
     const int64_t gmax = std::max(1, e->K - 1);
-    int64_t executed = 0, windows_run = 0;
-    int64_t launches_since_sort = 0;
+    int64_t windows_run = 0;
     bool stop = false;
     int64_t w = 0;
-    // after a launch that ended before step k_end: maybe retire / re-sort (compact.cuh)
-    auto after_launch = [&](int64_t k_end) -> int {
-        if (!e->compacting || k_end >= nsteps) return 0;
-        if (++launches_since_sort < s.sort_interval) return 0;
-        launches_since_sort = 0;
-        int q = compact_pass(e, rec_before[k_end], (int32_t)k_end);
-        if (q) return q;
-        r.P = make_params(e);
-        // live count of the last completed pass: an upper bound of the current one
-        r.P.n = std::max<int64_t>(1, *(volatile int32_t *)e->h_live);
-        return 0;
-    };
-    auto launch_range = [&](int64_t b, int64_t t) -> int {
-        if (s.minimum_alive > 0) {
-            for (int64_t k = b; k < t; ++k) {
-                // alive() before every step (tpp:973-975)
-                unsigned long long alive = e->n;
-                if (k > 0 || executed > 0) {
-                    CK(cudaMemcpyAsync(e->h_counters, e->counters.p, 2 * sizeof(unsigned long long),
-                                       cudaMemcpyDeviceToHost, e->cs));
-                    CK(cudaStreamSynchronize(e->cs));
-                    alive = e->h_counters[1];
-                }
-                if ((long long)alive < (long long)s.minimum_alive) return 1;
-                int q = launch_steps(r, k, k + 1, sched.steps[k].window);
-                if (q) return q;
-                ++executed;
-                q = after_launch(k + 1);
-                if (q) return q;
-            }
-            return 0;
-        }
-        for (int64_t k = b; k < t;) {
-            int64_t k1 = std::min(t, k + spl);
-            const int64_t w = sched.steps[k].window;
-            if (e->use_pair) k1 = std::min(k1, sched.window_begin[w + 1]);   // one window per launch
-            int q = launch_steps(r, k, k1, w);
-            if (q) return q;
-            q = after_launch(k1);
-            if (q) return q;
-            k = k1;
-        }
-        executed += t - b;
-        return 0;
-    };
-
     while (w < nwin && !stop) {
         int64_t g_end = w + 1;
         bool exhausted = false;
@@ -1244,7 +1557,7 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
         }
         for (int64_t k = w; k < g_end + (e->dyn_any ? 1 : 0) && k <= w + e->K; ++k)
             CK(cudaStreamWaitEvent(e->cs, e->slot_ready[k % e->K], 0));
-        const int q = launch_range(sched.window_begin[w], sched.window_begin[g_end]);
+        const int q = launch_range(r, R.sched.window_begin[w], R.sched.window_begin[g_end]);
         if (q < 0) return q;
         windows_run = g_end;
         // slots read by this group become free once it has run
@@ -1267,83 +1580,66 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
         w = g_end;
     }
 
-    // number of records written so far
-    int64_t rec_done = 1, crec_done = 0, irec_done = 0;
-    for (int64_t k = 0; k < executed; ++k)
-        if (sched.steps[k].save) {
-            ++rec_done;
-            ++irec_done;
-            if (sched.steps[k].time_pos) ++crec_done;
-        }
-    KParams P = r.P;
-    std::vector<int32_t> crec_of_rec((size_t)e->L + 1, -1);
-    {
-        int64_t rr = 1, cc = 0;
-        for (int64_t k = 0; k < executed; ++k)
-            if (sched.steps[k].save) {
-                if (sched.steps[k].time_pos) crec_of_rec[rr] = (int32_t)cc++;
-                ++rr;
-            }
-    }
-    if (s.save_interval == 0) {
-        const bool tpos = executed > 0;   // data.Time > 0 after at least one step
-        if (tpos) crec_of_rec[rec_done] = (int32_t)crec_done;
-        if (e->dim == 3)
-            save_state_kernel<3><<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, (int32_t)rec_done, (int32_t)crec_done, (int32_t)irec_done, tpos);
-        else
-            save_state_kernel<2><<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, (int32_t)rec_done, (int32_t)crec_done, (int32_t)irec_done, tpos);
-        CK(cudaGetLastError());
-        ++rec_done;
-        ++irec_done;
-        if (tpos) ++crec_done;
-        e->stats.aux_launches++;
-    }
-    finalize_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, e->out_status.p, e->out_length.p, e->out_tc.p);
-    CK(cudaGetLastError());
-    if (e->compacting) {
-        // retired particles: their later records repeat the frozen state
-        CK(e->crec_of_rec.alloc(crec_of_rec.size()));
-        CK(cudaMemcpyAsync(e->crec_of_rec.p, crec_of_rec.data(), crec_of_rec.size() * sizeof(int32_t),
-                           cudaMemcpyHostToDevice, e->cs));
-        const StateView R = view_of(e->ret, e->n);
-        fill_forward_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, R, e->d_counts.p + 2, e->crec_of_rec.p,
-                                                                     (int32_t)rec_done);
-        finalize_retired_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(R, e->d_counts.p + 2, s.abort_mode != 0,
-                                                                         s.curvature_mode != 0, e->out_status.p,
-                                                                         e->out_length.p, e->out_tc.p);
-        CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(e->cs));   // crec_of_rec (host vector) is read by the copy above
-        e->stats.aux_launches += 2;
-    }
+    RecordCounts c;
+    rc = run_tail(r, c);
+    if (rc) return rc;
     CK(cudaEventRecord(run_b, e->cs));
-    CK(cudaMemcpyAsync(e->h_counters, e->counters.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, e->cs));
-    CK(cudaStreamSynchronize(e->cs));
+    return run_collect(e, R, r.executed, windows_run, c, r.ev_used);
+}
 
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, run_a, run_b));
-    e->stats.run_ms = ms;
-    double kms = 0.0;
-    for (size_t k = 2; k + 1 < r.ev_used; k += 2) {
-        float t = 0.f;
-        CK(cudaEventElapsedTime(&t, e->ev_pool[k], e->ev_pool[k + 1]));
-        kms += t;
-    }
-    e->stats.kernel_ms = kms;
-    e->stats.particle_steps = (int64_t)e->h_counters[0];
+// ------------------------------------------------------------------ graph runs (batch.cu)
 
-    e->info.n = e->n;
-    e->info.dim = e->dim;
-    e->info.records = rec_done;
-    e->info.curvature_records = s.curvature_mode == 3 ? crec_done : 0;
-    e->info.info_records = irec_done;
-    e->info.steps = executed;
-    e->info.windows = windows_run;
-    e->info.particle_steps = (int64_t)e->h_counters[0];
-    e->info.n_volumes = s.volume_mode != 0 ? e->nvol : 0;
-    e->info.n_expressions = e->nexpr;
-    e->have_result = true;
+namespace granite_b200 {
+
+int graph_prepare(gr_engine *e) {
+    if (!e) return USER_ERR("null engine >");
+    if (!e->plan) e->plan = std::make_unique<RunPlan>();
+    return run_prepare(e, *e->plan, true);
+}
+
+int graph_enqueue(gr_engine *e) {
+    RunPlan &R = *e->plan;
+    e->pair_window[0] = e->pair_window[1] = -1;   // every window pair is packed inside the run
+    int rc = reset_state(e);
+    if (rc) return rc;
+    RunCtx r;
+    rc = make_ctx(e, R, r);
+    if (rc) return rc;
+    rc = launch_range(r, 0, R.nsteps);
+    if (rc < 0) return rc;
+    RecordCounts c;
+    rc = run_tail(r, c);
+    if (rc) return rc;
+    e->graph_executed = r.executed;
+    e->graph_records = c.rec;
     return GR_OK;
 }
+
+int graph_collect(gr_engine *e) {
+    const RunPlan &R = *e->plan;
+    RecordCounts c = count_records(R, e->graph_executed);
+    if (e->s.save_interval == 0) {
+        ++c.rec;
+        ++c.irec;
+        if (e->graph_executed > 0) ++c.crec;
+    }
+    const int64_t launches = e->stats.launches, aux = e->stats.aux_launches;
+    const int rc = run_collect(e, R, e->graph_executed, R.nwin, c, 0);
+    e->stats.launches = launches;
+    e->stats.aux_launches = aux;
+    return rc;
+}
+
+cudaStream_t engine_stream(gr_engine *e) { return e->cs; }
+int engine_device(const gr_engine *e) { return e->s.device; }
+uint64_t engine_generation(const gr_engine *e) { return e->gen; }
+int64_t engine_launches(const gr_engine *e, int64_t *aux) {
+    if (aux) *aux = e->stats.aux_launches;
+    return e->stats.launches;
+}
+int64_t engine_particle_steps(const gr_engine *e) { return e->stats.particle_steps; }
+
+}  // namespace granite_b200
 
 extern "C" {
 
@@ -1411,6 +1707,13 @@ int gr_fetch_positions(gr_engine *e, float *out, int64_t cap) {
     return fetch_rows(e, out, cap, e->hpos.p, e->n, e->info.records * e->dim, e->L * e->dim, sizeof(float));
 }
 
+int gr_fetch_final_positions(gr_engine *e, float *out, int64_t cap) {
+    if (!e) return USER_ERR("null engine >");
+    if (!e->have_result) return USER_ERR("No result: run() has not completed. >");
+    const float *last = e->hpos.p + (e->info.records - 1) * e->dim;
+    return fetch_rows(e, out, cap, last, e->n, e->dim, e->L * e->dim, sizeof(float));
+}
+
 int gr_fetch_status(gr_engine *e, int32_t *out, int64_t cap) {
     if (!e) return USER_ERR("null engine >");
     return fetch_rows(e, out, cap, e->out_status.p, 1, e->n, e->n, sizeof(int32_t));
@@ -1451,3 +1754,101 @@ int gr_fetch_compute_info(gr_engine *e, int32_t index, float *out, int64_t cap) 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ autotuner
+
+namespace {
+
+// Times one configuration over the first `steps` steps (graph launch shapes, not captured);
+// the faster of two runs, so lazy module loading does not count.
+int tune_trial(gr_engine *e, const gr_settings &cfg, int32_t steps, double &rate) {
+    e->s = cfg;
+    e->step_cap = steps;
+    rate = 0.0;
+    cudaEvent_t a = pool_event(e, 0), b = pool_event(e, 1);
+    for (int rep = 0; rep < 2; ++rep) {
+        int rc = granite_b200::graph_prepare(e);
+        if (rc) return rc;
+        CK(cudaEventRecord(a, e->cs));
+        rc = granite_b200::graph_enqueue(e);
+        if (rc) return rc;
+        CK(cudaEventRecord(b, e->cs));
+        CK(cudaStreamSynchronize(e->cs));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        rc = granite_b200::graph_collect(e);
+        if (rc) return rc;
+        if (ms > 0.f) rate = std::max(rate, (double)e->stats.particle_steps / (ms * 1e-3));
+    }
+    return GR_OK;
+}
+
+}  // namespace
+
+extern "C" int gr_tune(gr_engine *e, int32_t trial_steps, gr_tune_result *out) {
+    if (!e) return USER_ERR("null engine >");
+    if (e->s.minimum_alive > 0)
+        return USER_ERR("MinimumAliveParticles needs host decisions between steps; it cannot run in a graph. >");
+    const int32_t steps = trial_steps > 0 ? trial_steps : 40;
+    const gr_settings base = e->s;
+    gr_settings cur = base;
+    if (cur.block_size <= 0) cur.block_size = 256;
+    if (cur.sort_interval <= 0) cur.sort_interval = 4;
+    if (cur.grid_waves <= 0) cur.grid_waves = 1;
+    int trials = 0;
+    double best = 0.0;
+    int rc = tune_trial(e, cur, steps, best);
+    ++trials;
+    // coordinate descent: layout, block size, sort interval, grid waves
+    auto consider = [&](gr_settings c) -> int {
+        double r = 0.0;
+        const int q = tune_trial(e, c, steps, r);
+        ++trials;
+        if (q) return q;
+        if (r > best * 1.01) {
+            best = r;
+            cur = c;
+        }
+        return 0;
+    };
+    if (!rc && e->wind_dynamic) {
+        gr_settings c = cur;
+        c.layout = cur.layout == 0 ? 1 : 0;
+        rc = consider(c);
+    }
+    for (int bs : {64, 128, 256})
+        if (!rc && bs != cur.block_size) {
+            gr_settings c = cur;
+            c.block_size = bs;
+            rc = consider(c);
+        }
+    for (int si : {1, 2, 4, 8})
+        if (!rc && si != cur.sort_interval) {
+            gr_settings c = cur;
+            c.sort_interval = si;
+            rc = consider(c);
+        }
+    for (int gw : {1, 2, 4})
+        if (!rc && gw != cur.grid_waves) {
+            gr_settings c = cur;
+            c.grid_waves = gw;
+            rc = consider(c);
+        }
+    e->step_cap = 0;
+    ++e->gen;
+    e->have_result = false;
+    if (rc) {
+        e->s = base;
+        return rc;
+    }
+    e->s = cur;
+    if (out) {
+        out->layout = cur.layout;
+        out->block_size = cur.block_size;
+        out->sort_interval = cur.sort_interval;
+        out->grid_waves = cur.grid_waves;
+        out->particle_steps_per_s = best;
+        out->trials = trials;
+    }
+    return GR_OK;
+}

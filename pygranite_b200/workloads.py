@@ -190,6 +190,69 @@ def config2(n_particles=1_000_000, n_snapshots=201, grid=(64, 192, 192), steps=2
     return settings, src, seeds
 
 
+def batch_sets(n_sets=512, n_min=100, n_max=200_000, life_min=100, life_max=5000, frac3d=0.7, seed=0):
+    """Seed-set descriptors of the batching workload: particle counts log-uniform in
+    [n_min, n_max], lifetimes (RK4 steps) uniform in [life_min, life_max], a fraction `frac3d`
+    on the 3D field and the rest on the 2D field."""
+    rng = np.random.default_rng(seed)
+    counts = np.rint(np.exp(rng.uniform(math.log(n_min), math.log(n_max), n_sets))).astype(np.int64)
+    lifes = rng.integers(life_min, life_max + 1, n_sets)
+    is3d = rng.random(n_sets) < frac3d
+    return [dict(n=int(counts[j]), life=int(lifes[j]), dim=3 if is3d[j] else 2, seed=seed * 100_003 + j)
+            for j in range(n_sets)]
+
+
+class BatchWorkload:
+    """The batching configuration: seed sets of uneven size and lifetime on a 3D field (the
+    plain 3D configuration's Fourier field, 1 km x 1 km x 250 m) and a 2D Fourier field of the
+    same spectrum (1 km spacing), 600 s snapshots, h = 60 s RK4, final records only."""
+
+    def __init__(self, n_sets=512, grid3=(64, 192, 192), grid2=(512, 1024), n_min=100, n_max=200_000,
+                 life_min=100, life_max=5000, frac3d=0.7, seed=0):
+        self.grid3, self.grid2 = tuple(grid3), tuple(grid2)
+        self.sets = batch_sets(n_sets, n_min, n_max, life_min, life_max, frac3d, seed)
+        self.life_max = max(s["life"] for s in self.sets)
+        self.n_snapshots = (self.life_max * 60 + 599) // 600 + 1
+        self.field3 = FourierField(self.grid3, (250.0, 1000.0, 1000.0), n_modes=32, seed=seed)
+        self.field2 = FourierField(self.grid2, (1000.0, 1000.0), n_modes=32, seed=seed + 7,
+                                   rms=(7.0710678, 7.0710678))
+
+    def settings(self, dim):
+        gs = [1000.0, 1000.0, 250.0] if dim == 3 else [1000.0, 1000.0]
+        return dict(Space=0 if dim == 3 else 1, Integrator=1, WindfieldMode=1, DeltaT=60.0, DataTimeDistance=600.0,
+                    GridScale=gs, Offset=[0.0] * len(gs), SaveInterval=0, BorderMode=0, CurvatureMode=0,
+                    MaximumSimulationTime=60.0 * self.life_max)
+
+    def snapshot(self, dim, k):
+        return (self.field3 if dim == 3 else self.field2).snapshot(600.0 * k)
+
+    def seeds(self, j):
+        s = self.sets[j]
+        if s["dim"] == 3:
+            nz, ny, nx = self.grid3
+            return uniform_seeds(s["n"], s["seed"], [0.0, 0.0, 0.0], [nx * 1000.0, ny * 1000.0, nz * 250.0 / 2])
+        ny, nx = self.grid2
+        return uniform_seeds(s["n"], s["seed"], [0.0, 0.0], [nx * 1000.0, ny * 1000.0])
+
+    def group(self, dim):
+        """Concatenated seeds, lifetimes and the (set index, offset, count) of every set on
+        the field of dimension `dim`."""
+        idx = [j for j, s in enumerate(self.sets) if s["dim"] == dim]
+        seeds, lifes, spans, off = [], [], [], 0
+        for j in idx:
+            sd = self.seeds(j)
+            seeds.append(sd)
+            lifes.append(np.full(len(sd), self.sets[j]["life"], np.int32))
+            spans.append((j, off, len(sd)))
+            off += len(sd)
+        if not idx:
+            return np.zeros((0, dim), np.float32), np.zeros(0, np.int32), []
+        return np.concatenate(seeds), np.concatenate(lifes), spans
+
+    def particle_steps_upper(self):
+        return sum(s["n"] * s["life"] for s in self.sets)
+
+
 def apply_settings(obj, settings: dict, enums=None):
     """Sets reference-named fields on a pygranite IntegratorSettings instance."""
     for k, v in settings.items():
