@@ -54,6 +54,13 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-particles", type=int, default=20000)
     p.add_argument("--cpu-steps", type=int, default=100)
+    p.add_argument("--workload", default="plain", choices=["plain", "batch"],
+                   help="plain: the 3D RK4 configuration; batch: 512 seed sets of uneven size and lifetime")
+    p.add_argument("--batch-storage", default="bf16", choices=["f32", "bf16", "f16"])
+    p.add_argument("--batch-sets", type=int, default=512)
+    p.add_argument("--tune-steps", type=int, default=40, help="steps per autotuner trial (0 = no tuning)")
+    p.add_argument("--acc-life", type=int, default=500,
+                   help="accuracy sample: sets with at most this lifetime are checked against the float64 oracle")
     return p.parse_args()
 
 
@@ -189,10 +196,232 @@ def run_reference(args):
     return 0
 
 
+# algorithmic bytes per particle-step of plain RK4 with the final record only, per
+# (dimension, storage): 4 stages x 2 snapshots x components x corners x element bytes
+# + position read / write + status
+RK4_FINAL_BYTES = {(3, "f32"): 796, (3, "bf16"): 412, (3, "f16"): 412,
+                   (2, "f32"): 276, (2, "bf16"): 148, (2, "f16"): 148}
+BATCH_WORKLOAD = "batch-512-sets-3d-2d-rk4"
+
+
+def batch_accuracy(w, eng_b, spans, storage, max_life, per_set=64, max_sets=6):
+    """Final-position error in grid cells of the batched run against the float64 oracle, on
+    sets with lifetime <= max_life: against the float32 field (storage rounding included) and
+    against the stored field (integration arithmetic only).  Errors are taken over particles
+    alive at the end in both runs; particles whose abort decision differs (a float64 path
+    crossing the domain edge one step earlier or later) are counted separately."""
+    from oracle import oracle as orc
+    from pygranite_b200 import workloads as W
+    out = {}
+    for dim in sorted(eng_b):
+        pos_all = eng_b[dim].final_positions()
+        st_all = eng_b[dim].status()
+        cell = np.array([1000.0, 1000.0, 250.0][:dim])
+        picked = [(j, off, cnt) for j, off, cnt in spans[dim] if w.sets[j]["life"] <= max_life][:max_sets]
+        if not picked:
+            continue
+        err = {"f": [], "s": []}
+        mism = {"f": 0, "s": 0}
+        steps = []
+        for j, off, cnt in picked:
+            life = w.sets[j]["life"]
+            m = min(per_set, cnt)
+            seeds = w.seeds(j)[:m]
+            snaps = [w.snapshot(dim, k) for k in range(life // 10 + 2)]
+            st = orc.settings(**dict(w.settings(dim), MaximumSimulationTime=60.0 * life))
+            ref = orc.run(st, orc.Inputs(wind=snaps, seeds=seeds), precision="f64")
+            rsnaps = [[W.round_storage(p, storage) for p in sn] for sn in snaps]
+            ref_s = orc.run(st, orc.Inputs(wind=rsnaps, seeds=seeds), precision="f64")
+            got = pos_all[off:off + m].astype(np.float64)
+            got_st = st_all[off:off + m]
+            for key, r in (("f", ref), ("s", ref_s)):
+                both = (r["status"] == 0) & (got_st == 0)
+                mism[key] += int(np.sum(r["status"] != got_st))
+                d = np.abs(got - r["trajectories"][:, -1]) / cell
+                err[key].extend(d.max(axis=1)[both].tolist())
+            steps.append(life)
+
+        def stats(e):
+            e = np.array(e)
+            if not e.size:
+                return None, None, None
+            return float(np.sqrt(np.mean(e ** 2))), float(np.percentile(e, 99)), float(e.max())
+        rf, pf, mf = stats(err["f"])
+        rs, ps_, ms_ = stats(err["s"])
+        out[f"{dim}d"] = {"sets": len(picked), "particles": int(sum(min(per_set, c) for _, _, c in picked)),
+                          "lifetimes": steps, "alive_in_both": len(err["f"]),
+                          "cell_rms_vs_f64": rf, "cell_p99_vs_f64": pf, "cell_max_vs_f64": mf,
+                          "status_mismatch_vs_f64": mism["f"],
+                          "cell_rms_vs_f64_same_field": rs, "cell_p99_vs_f64_same_field": ps_,
+                          "cell_max_vs_f64_same_field": ms_, "status_mismatch_vs_f64_same_field": mism["s"]}
+    return out
+
+
+def run_batch(args, world, rank, local, pg_dist):
+    """512 seed sets, BF16 batched in one graph vs one plain FP32 run per set."""
+    import torch
+    from pygranite_b200 import capi
+    from pygranite_b200 import workloads as W
+
+    w = W.BatchWorkload(n_sets=args.batch_sets, seed=rank)
+    n_snap = w.n_snapshots
+    bst = args.batch_storage
+    code = {"f32": 0, "bf16": 1, "f16": 2}
+    groups, eng_b, eng_p, spans = {}, {}, {}, {}
+    for dim in (3, 2):
+        seeds, lifes, sp = w.group(dim)
+        if not sp:
+            continue
+        groups[dim] = (seeds, lifes)
+        spans[dim] = sp
+        eng_b[dim] = capi.Engine(capi.settings_from_reference(w.settings(dim), ring_slots=n_snap, storage=code[bst],
+                                                              device=local))
+        eng_b[dim].set_seeds(seeds)
+        eng_b[dim].set_lifetimes(lifes)
+        eng_p[dim] = capi.Engine(capi.settings_from_reference(w.settings(dim), ring_slots=n_snap, storage=0,
+                                                              device=local, sort_interval=args.sort_interval))
+    t0 = time.perf_counter()
+    for k in range(n_snap):
+        for dim in eng_b:
+            snap = w.snapshot(dim, k)
+            eng_b[dim].load_windfield(k, snap)
+            eng_p[dim].load_windfield(k, snap)
+    load_s = time.perf_counter() - t0
+    resident = lambda s: 1 if s < n_snap else 0  # noqa: E731
+
+    # ---- autotuner, then one graph over both field groups
+    tuned = {}
+    for dim, e in eng_b.items():
+        if args.tune_steps > 0:
+            r = e.tune(trial_steps=args.tune_steps)
+            tuned[f"{dim}d"] = {"layout": ["window-pair", "ring"][r.layout], "block_size": r.block_size,
+                                "sort_interval": r.sort_interval, "grid_waves": r.grid_waves,
+                                "trials": r.trials, "trial_rate": r.particle_steps_per_s}
+    batch = capi.Batch([eng_b[d] for d in sorted(eng_b)])
+    for _ in range(max(1, args.warmup)):
+        batch.run()
+    torch.cuda.synchronize()
+    if pg_dist:
+        pg_dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    g_ms, g_ps, ps_dim = 0.0, 0, {d: 0 for d in eng_b}
+    for _ in range(args.steps):
+        batch.run()
+        st = batch.stats()
+        g_ms += st.graph_ms
+        g_ps += st.particle_steps
+        for d, e in eng_b.items():
+            ps_dim[d] += e.stats().particle_steps
+    sampler.stop()
+    clocks = sampler.summary()
+    bst_stats = batch.stats()
+    t_max, ps_all = combine_ranks(pg_dist, g_ms, g_ps, "cuda")
+    value = ps_all / (t_max / 1e3)
+
+    # ---- end to end: new host seeds every step (same counts: the graph replays), final
+    # positions and abort codes back to the host
+    e2e_s, e2e_ps, h2d, d2h = 0.0, 0, 0, 0
+    for k in range(1 + max(1, args.e2e_steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for d in sorted(eng_b):
+            eng_b[d].set_seeds(groups[d][0])
+        batch.run()
+        outs = [(eng_b[d].final_positions(), eng_b[d].status()) for d in sorted(eng_b)]
+        dt = time.perf_counter() - t0
+        if k >= 1:
+            e2e_s += dt
+            e2e_ps += batch.stats().particle_steps
+            h2d = sum(groups[d][0].nbytes for d in eng_b)
+            d2h = sum(p.nbytes + s_.nbytes for p, s_ in outs)
+    assert batch.stats().captures == bst_stats.captures, "new seeds of the same counts must not capture again"
+    e_t, e_ps = combine_ranks(pg_dist, e2e_s * 1e3, e2e_ps, "cuda")
+    e2e = {"value": e_ps / (e_t / 1e3), "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "steps": max(1, args.e2e_steps),
+           "path": "capi.Engine.set_seeds (host) + capi.Batch.run + final positions / status to host"}
+
+    # ---- plain FP32: one run per set, sequentially, every snapshot resident
+    plain_ms, plain_ps = 0.0, 0
+    loc = {j: (d, off, cnt) for d in spans for j, off, cnt in spans[d]}
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    for j, s in enumerate(w.sets):
+        d, off, cnt = loc[j]
+        e = eng_p[d]
+        e.set_seeds(groups[d][0][off:off + cnt])
+        e.update_settings(maximum_simulation_time=60.0 * s["life"])
+        e.run(resident)
+        st = e.stats()
+        plain_ms += st.run_ms
+        plain_ps += st.particle_steps
+    torch.cuda.synchronize()
+    plain_wall = time.perf_counter() - wall0
+    p_t, p_ps = combine_ranks(pg_dist, plain_wall * 1e3, plain_ps, "cuda")
+    plain_value_wall = p_ps / (p_t / 1e3)
+    pd_t, _ = combine_ranks(pg_dist, plain_ms, plain_ps, "cuda")
+    plain_value_dev = p_ps / (pd_t / 1e3)
+
+    acc = batch_accuracy(w, eng_b, spans, bst, args.acc_life) if rank == 0 else None
+    batch.close()
+    for e in list(eng_b.values()) + list(eng_p.values()):
+        e.close()
+    if pg_dist:
+        pg_dist.barrier()
+    if rank != 0:
+        return None
+
+    peak, peak_src = load_peaks()
+    alg = sum(ps_dim[d] * RK4_FINAL_BYTES[(d, bst)] for d in ps_dim)
+    achieved = alg / (g_ms / 1e3) / 1e9 if g_ms > 0 else None
+    return {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": t_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": bst,
+        "data": "synthetic (seeded Fourier-mode fields, 3D 192x192x64 and 2D 1024x512)",
+        "config": {"workload": BATCH_WORKLOAD, "sets": len(w.sets),
+                   "particles_per_gpu": int(sum(s["n"] for s in w.sets)),
+                   "sets_3d": int(sum(s["dim"] == 3 for s in w.sets)), "snapshots": n_snap,
+                   "lifetimes": [100, 5000], "storage": bst, "parallelism": f"replicas{world}",
+                   "l2": f"inputs larger than L2 ({n_snap} snapshots per field resident)", "tuned": tuned,
+                   "graph_nodes": bst_stats.nodes},
+        "plain": {"storage": "f32", "value_device": plain_value_dev, "value_wall": plain_value_wall,
+                  "seconds_wall": p_t / 1e3, "particle_steps": int(p_ps),
+                  "path": "one capi.Engine.run per set (set_seeds, MaximumSimulationTime = lifetime * 60 s)"},
+        "speedup_vs_plain_f32": value / plain_value_wall,
+        "speedup_vs_plain_f32_device": value / plain_value_dev,
+        "accuracy": acc, "e2e": e2e,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None, "peak_source": peak_src,
+                     "bytes_per_particle_step": {f"{d}d": RK4_FINAL_BYTES[(d, bst)] for d in ps_dim},
+                     "kernel": "advance_kernel (graph replay, whole run)"},
+        "clocks": clocks, "gpu_launches": int((bst_stats.kernel_launches + bst_stats.aux_launches) * args.steps),
+        "load_s": load_s,
+    }
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        world, rank, local = dist_env()
+        import torch
+        torch.cuda.set_device(local)
+        pg_dist = None
+        if world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+            pg_dist = dist
+        line = run_batch(args, world, rank, local, pg_dist)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        if pg_dist:
+            pg_dist.destroy_process_group()
+        return 0
 
     world, rank, local = dist_env()
     import torch

@@ -256,6 +256,66 @@ typedef struct gr_tune_result {
 } gr_tune_result;
 int gr_tune(gr_engine *engine, int32_t trial_steps, gr_tune_result *out);
 
+/* Request server: continuous batching of trajectory requests over one field.  No counterpart
+ * in the reference, which integrates one seed set per TrajectoryIntegrator.
+ *
+ * The field (n_snapshots snapshots of nz x ny x nx nodes, DataTimeDistance apart, stored as
+ * settings->storage) is packed once into pinned host memory by gr_server_set_snapshot.  A
+ * worker thread sweeps it window by window through a 4-slot device ring refilled from there.
+ * A request is a seed set, a start time (seconds on the field's clock, rounded to the step
+ * grid DeltaT), a step count and an integrator (0 Euler, 1 RK4); it runs from its start step
+ * until the step count, an abort, or the end of the field, whichever comes first.  Requests
+ * whose start falls in the current window join the particle pool of their integrator, while
+ * their state fits `hbm_budget_bytes` (0 = a quarter of the free device memory); all requests
+ * in flight advance together, one launch per integrator and window.  A request whose start
+ * window the sweep has passed waits for the next sweep.  Results (final positions and abort
+ * codes) are those of an integration of the request alone.  Positions only: settings with
+ * curvature, volumes, constants, uplift, length abort, MinimumAliveParticles or compensation
+ * are rejected.  Submit, wait, result, cancel and stats may be called from any thread. */
+#define GR_REQ_PENDING 0
+#define GR_REQ_ACTIVE 1
+#define GR_REQ_DONE 2
+#define GR_REQ_CANCELLED 3
+#define GR_REQ_FAILED 4
+typedef struct gr_server gr_server;
+typedef struct gr_request_info {
+    int64_t n;
+    int32_t dim, integrator;
+    int64_t start_step;          /* on the field's step clock */
+    int64_t steps;               /* steps it runs (after clipping at the field's end) */
+    double submit_s, admit_s, done_s;   /* server clock, seconds since gr_server_start */
+    int32_t state;               /* GR_REQ_* */
+} gr_request_info;
+typedef struct gr_server_stats {
+    int64_t submitted, admitted, completed, cancelled;
+    int64_t deferred;            /* admissions postponed for lack of HBM budget */
+    int64_t windows, sweeps, jumps;
+    int64_t particle_steps;
+    int64_t capacity_particles;  /* particle slots per integrator pool */
+    int64_t peak_particles;      /* most particles in flight at once */
+    int64_t h2d_bytes, d2h_bytes;
+    int64_t pending, active;
+    int64_t clock_steps;         /* steps of the field's clock */
+    int64_t windows_per_sweep;
+} gr_server_stats;
+int gr_server_create(const gr_settings *settings, int64_t n_snapshots, int64_t nz, int64_t ny, int64_t nx,
+                     int64_t hbm_budget_bytes, gr_server **out);
+/* Snapshot k as float32 planes (z, y, x) / (y, x); device_src = 1 for device pointers. */
+int gr_server_set_snapshot(gr_server *server, int64_t snapshot, const float *const *components,
+                           int32_t n_components, int32_t device_src);
+int gr_server_start(gr_server *server);
+int gr_server_submit(gr_server *server, const float *seeds, int64_t n, int32_t dim, double start_time,
+                     int32_t steps, int32_t integrator, int64_t *request_id);
+/* Waits until the request is done, cancelled or failed (timeout_s < 0: no limit). */
+int gr_server_wait(gr_server *server, int64_t request_id, double timeout_s, int32_t *state);
+/* Info, and when done the final positions (n, dim) and abort codes (n). */
+int gr_server_result(gr_server *server, int64_t request_id, gr_request_info *info, float *positions,
+                     int32_t *status, int64_t capacity);
+int gr_server_release(gr_server *server, int64_t request_id);
+int gr_server_cancel(gr_server *server, int64_t request_id);
+int gr_server_stats_get(gr_server *server, gr_server_stats *out);
+void gr_server_destroy(gr_server *server);
+
 /* Allocation-free advance of particles between two snapshots.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc — code running while a CUDA
  * graph is being captured, hosts whose device memory belongs to their own pool allocator,

@@ -25,8 +25,12 @@ EXPORTS = [
     "gr_fetch_volume_info", "gr_fetch_compute_info", "gr_load_windfield_device",
     "gr_set_seeds_device", "gr_plan", "gr_advance_noalloc", "gr_update_settings", "gr_settings_get",
     "gr_set_lifetimes", "gr_batch_create", "gr_batch_destroy", "gr_batch_run", "gr_batch_stats_get", "gr_tune",
-    "gr_fetch_final_positions",
+    "gr_fetch_final_positions", "gr_server_create", "gr_server_set_snapshot", "gr_server_start",
+    "gr_server_submit", "gr_server_wait", "gr_server_result", "gr_server_release", "gr_server_cancel",
+    "gr_server_stats_get", "gr_server_destroy",
 ]
+
+GR_REQ_PENDING, GR_REQ_ACTIVE, GR_REQ_DONE, GR_REQ_CANCELLED, GR_REQ_FAILED = 0, 1, 2, 3, 4
 
 
 class Settings(ctypes.Structure):
@@ -72,6 +76,19 @@ class BatchStats(ctypes.Structure):
 class TuneResult(ctypes.Structure):
     _fields_ = [("layout", ctypes.c_int32), ("block_size", ctypes.c_int32), ("sort_interval", ctypes.c_int32),
                 ("grid_waves", ctypes.c_int32), ("particle_steps_per_s", ctypes.c_double), ("trials", ctypes.c_int32)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("dim", ctypes.c_int32), ("integrator", ctypes.c_int32),
+                ("start_step", ctypes.c_int64), ("steps", ctypes.c_int64), ("submit_s", ctypes.c_double),
+                ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double), ("state", ctypes.c_int32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in (
+        "submitted", "admitted", "completed", "cancelled", "deferred", "windows", "sweeps", "jumps",
+        "particle_steps", "capacity_particles", "peak_particles", "h2d_bytes", "d2h_bytes", "pending", "active",
+        "clock_steps", "windows_per_sweep")]
 
 
 LOADER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64)
@@ -126,6 +143,18 @@ def lib():
             "gr_batch_stats_get": (ctypes.c_int, [P, ctypes.POINTER(BatchStats)]),
             "gr_tune": (ctypes.c_int, [P, I32, ctypes.POINTER(TuneResult)]),
             "gr_fetch_final_positions": (ctypes.c_int, [P, FP, I64]),
+            "gr_server_create": (ctypes.c_int, [ctypes.POINTER(Settings), I64, I64, I64, I64, I64, ctypes.POINTER(P)]),
+            "gr_server_set_snapshot": (ctypes.c_int, [P, I64, ctypes.POINTER(P), I32, I32]),
+            "gr_server_start": (ctypes.c_int, [P]),
+            "gr_server_submit": (ctypes.c_int, [P, FP, I64, I32, ctypes.c_double, I32, I32,
+                                                ctypes.POINTER(ctypes.c_int64)]),
+            "gr_server_wait": (ctypes.c_int, [P, I64, ctypes.c_double, ctypes.POINTER(ctypes.c_int32)]),
+            "gr_server_result": (ctypes.c_int, [P, I64, ctypes.POINTER(RequestInfo), FP,
+                                                ctypes.POINTER(ctypes.c_int32), I64]),
+            "gr_server_release": (ctypes.c_int, [P, I64]),
+            "gr_server_cancel": (ctypes.c_int, [P, I64]),
+            "gr_server_stats_get": (ctypes.c_int, [P, ctypes.POINTER(ServerStats)]),
+            "gr_server_destroy": (None, [P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -309,6 +338,12 @@ class Engine:
         _check(lib().gr_tune(self.h, trial_steps, ctypes.byref(r)))
         return r
 
+    def status(self):
+        n = self.info().n
+        st = np.empty(n, np.int32)
+        _check(lib().gr_fetch_status(self.h, st.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), n))
+        return st
+
     def final_positions(self):
         info = self.info()
         out = np.empty((info.n, info.dim), np.float32)
@@ -389,6 +424,78 @@ class Batch:
     def close(self):
         if self.h:
             lib().gr_batch_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """gr_server: trajectory requests served with continuous batching over one field."""
+
+    def __init__(self, settings: Settings, n_snapshots, shape, hbm_budget=0):
+        nz, ny, nx = shape if len(shape) == 3 else (1,) + tuple(shape)
+        self.dim = 3 if settings.space == 0 else 2
+        self.h = ctypes.c_void_p()
+        _check(lib().gr_server_create(ctypes.byref(settings), n_snapshots, nz, ny, nx, hbm_budget,
+                                      ctypes.byref(self.h)))
+
+    def set_snapshot(self, k, planes):
+        """Host float32 planes (numpy)."""
+        planes = [np.ascontiguousarray(p, np.float32) for p in planes]
+        arr = (ctypes.c_void_p * len(planes))(*[p.ctypes.data for p in planes])
+        _check(lib().gr_server_set_snapshot(self.h, k, arr, len(planes), 0))
+
+    def set_snapshot_device(self, k, ptrs):
+        """Device float32 planes (raw pointers)."""
+        arr = (ctypes.c_void_p * len(ptrs))(*ptrs)
+        _check(lib().gr_server_set_snapshot(self.h, k, arr, len(ptrs), 1))
+
+    def start(self):
+        _check(lib().gr_server_start(self.h))
+
+    def submit(self, seeds, start_time, steps, integrator=1):
+        s = np.ascontiguousarray(seeds, np.float32)
+        rid = ctypes.c_int64(0)
+        _check(lib().gr_server_submit(self.h, _fp(s), s.shape[0], s.shape[1], float(start_time), int(steps),
+                                      int(integrator), ctypes.byref(rid)))
+        return rid.value
+
+    def wait(self, rid, timeout=-1.0):
+        st = ctypes.c_int32(0)
+        _check(lib().gr_server_wait(self.h, rid, float(timeout), ctypes.byref(st)))
+        return st.value
+
+    def info(self, rid) -> RequestInfo:
+        r = RequestInfo()
+        _check(lib().gr_server_result(self.h, rid, ctypes.byref(r), None, None, 0))
+        return r
+
+    def result(self, rid):
+        info = self.info(rid)
+        pos = np.empty((info.n, info.dim), np.float32)
+        st = np.empty(info.n, np.int32)
+        _check(lib().gr_server_result(self.h, rid, None, _fp(pos), st.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                      info.n))
+        return pos, st, info
+
+    def cancel(self, rid):
+        _check(lib().gr_server_cancel(self.h, rid))
+
+    def release(self, rid):
+        _check(lib().gr_server_release(self.h, rid))
+
+    def stats(self) -> ServerStats:
+        s = ServerStats()
+        _check(lib().gr_server_stats_get(self.h, ctypes.byref(s)))
+        return s
+
+    def close(self):
+        if self.h:
+            lib().gr_server_destroy(self.h)
             self.h = ctypes.c_void_p()
 
     def __del__(self):

@@ -7,6 +7,8 @@
 // are filled from their frozen state at the end of the run.  Per-particle arithmetic does
 // not depend on the order, so results stay bit-identical.
 //
+// Kernels are static: every translation unit that includes this header owns its instances.
+//
 // One pass: bin (key + warp-aggregated histogram) -> two-level exclusive scan -> rank
 // (destination of every source slot, written as a permutation) -> gather (coalesced writes
 // of every state array) -> commit (counts).
@@ -23,7 +25,7 @@ constexpr int SCAN_CHUNK = 1024;   // bins per block of the first scan level
 struct StateView {
     float *px, *py, *pz, *qx, *qy, *qz, *kx, *ky, *kz, *lx, *ly, *lz;
     float *length, *tc, *curv, *volc, *cmpc;
-    int32_t *status, *id, *retire, *life;
+    int32_t *status, *id, *retire, *life, *birth;
     int64_t stride;   // per-array stride of volc / cmpc
 };
 
@@ -43,6 +45,7 @@ struct CompactParams {
     int32_t nvol, nexpr, curv_prev, compensated, fast_curv, abort_on, curv_on, curv_ind;
     int32_t rec_now;           // first record index not yet written
     int32_t k_end;             // steps run so far: a particle whose lifetime is over retires
+    int32_t ret_by_id;         // 1: retired particles go to slot id of `ret` (final state only)
 };
 
 __device__ __forceinline__ int32_t bin_of(const CompactParams &C, int64_t i) {
@@ -61,7 +64,7 @@ __device__ __forceinline__ int32_t bin_of(const CompactParams &C, int64_t i) {
 }
 
 // key + histogram; lanes of a warp with the same key add once (sorted input: mostly one key per warp)
-__global__ void bin_kernel(const __grid_constant__ CompactParams C) {
+static __global__ void bin_kernel(const __grid_constant__ CompactParams C) {
     const int64_t n = *C.n_act;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
@@ -76,7 +79,7 @@ __global__ void bin_kernel(const __grid_constant__ CompactParams C) {
 }
 
 // level 1: exclusive scan inside chunks of SCAN_CHUNK bins; chunk totals to C.chunk
-__global__ void __launch_bounds__(SCAN_CHUNK) scan_chunks_kernel(const __grid_constant__ CompactParams C) {
+static __global__ void __launch_bounds__(SCAN_CHUNK) scan_chunks_kernel(const __grid_constant__ CompactParams C) {
     __shared__ int32_t warp_sum[SCAN_CHUNK / 32];
     const int nb = C.nbins + 1;
     const int b = blockIdx.x * SCAN_CHUNK + threadIdx.x;
@@ -106,7 +109,7 @@ __global__ void __launch_bounds__(SCAN_CHUNK) scan_chunks_kernel(const __grid_co
 }
 
 // level 2: exclusive scan of the chunk totals (one block); n_new = start of the retired bin
-__global__ void __launch_bounds__(1024) scan_top_kernel(const __grid_constant__ CompactParams C, int nchunks) {
+static __global__ void __launch_bounds__(1024) scan_top_kernel(const __grid_constant__ CompactParams C, int nchunks) {
     __shared__ int32_t part[1024];
     const int per = (nchunks + 1023) / 1024;
     const int c0 = threadIdx.x * per, c1 = min(nchunks, c0 + per);
@@ -131,7 +134,7 @@ __global__ void __launch_bounds__(1024) scan_top_kernel(const __grid_constant__ 
 }
 
 // destination of every source slot, as a permutation dest -> source
-__global__ void rank_kernel(const __grid_constant__ CompactParams C) {
+static __global__ void rank_kernel(const __grid_constant__ CompactParams C) {
     const int64_t n = *C.n_act;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
@@ -166,10 +169,18 @@ __device__ __forceinline__ void move_live(const CompactParams &C, int64_t i, int
     D.status[d] = S.status[i];
     D.id[d] = S.id[i];
     if (S.life) D.life[d] = S.life[i];
+    if (S.birth) D.birth[d] = S.birth[i];
 }
 
 __device__ __forceinline__ void move_retired(const CompactParams &C, int64_t i, int64_t r) {
     const StateView &S = C.src, &R = C.ret;
+    if (C.ret_by_id) {   // final state straight into the result slot of the particle
+        const int64_t id = S.id[i];
+        R.px[id] = S.px[i]; R.py[id] = S.py[i];
+        if (C.dim == 3) R.pz[id] = S.pz[i];
+        R.status[id] = S.status[i];
+        return;
+    }
     R.px[r] = S.px[i]; R.py[r] = S.py[i];
     if (C.dim == 3) R.pz[r] = S.pz[i];
     if (C.abort_on) R.length[r] = S.length[i];
@@ -183,7 +194,7 @@ __device__ __forceinline__ void move_retired(const CompactParams &C, int64_t i, 
 }
 
 // coalesced writes in destination order; the scattered reads hit L2
-__global__ void gather_kernel(const __grid_constant__ CompactParams C) {
+static __global__ void gather_kernel(const __grid_constant__ CompactParams C) {
     const int64_t n = *C.n_act, live = *C.n_new, base = *C.n_ret;
     for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < n; d += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = C.perm[d];
@@ -192,7 +203,7 @@ __global__ void gather_kernel(const __grid_constant__ CompactParams C) {
     }
 }
 
-__global__ void commit_kernel(const __grid_constant__ CompactParams C) {
+static __global__ void commit_kernel(const __grid_constant__ CompactParams C) {
     *C.n_ret += *C.n_act - *C.n_new;
     *C.n_act = *C.n_new;
 }

@@ -25,6 +25,8 @@
 
 #include "../../include/granite_b200.h"
 #include "expr.h"
+#include "host_util.h"
+#include "pack_kernels.cuh"
 #include "advance.h"
 #include "compact.cuh"
 #include "engine_graph.h"
@@ -67,64 +69,6 @@ namespace {
     } while (0)
 
 // ------------------------------------------------------------------ aux kernels
-
-// Planes (ncomp x nodes, float32) -> node-major packed snapshot of storage type W.
-template <typename W>
-__global__ void pack_wind_kernel(const float *__restrict__ u, const float *__restrict__ v,
-                                 const float *__restrict__ w, void *out, int64_t nodes, int dim);
-
-template <>
-__global__ void pack_wind_kernel<float>(const float *__restrict__ u, const float *__restrict__ v,
-                                        const float *__restrict__ w, void *out, int64_t nodes, int dim) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
-        if (dim == 3) reinterpret_cast<float4 *>(out)[i] = make_float4(u[i], v[i], w[i], 0.f);
-        else reinterpret_cast<float2 *>(out)[i] = make_float2(u[i], v[i]);
-    }
-}
-
-template <>
-__global__ void pack_wind_kernel<__nv_bfloat16>(const float *__restrict__ u, const float *__restrict__ v,
-                                                const float *__restrict__ w, void *out, int64_t nodes, int dim) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
-        const __nv_bfloat162 a = __floats2bfloat162_rn(u[i], v[i]);
-        if (dim == 3) {
-            const __nv_bfloat162 b = __floats2bfloat162_rn(w[i], 0.f);
-            uint2 q;
-            q.x = *reinterpret_cast<const unsigned *>(&a);
-            q.y = *reinterpret_cast<const unsigned *>(&b);
-            reinterpret_cast<uint2 *>(out)[i] = q;
-        } else {
-            reinterpret_cast<unsigned *>(out)[i] = *reinterpret_cast<const unsigned *>(&a);
-        }
-    }
-}
-
-template <>
-__global__ void pack_wind_kernel<__half>(const float *__restrict__ u, const float *__restrict__ v,
-                                         const float *__restrict__ w, void *out, int64_t nodes, int dim) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
-        const __half2 a = __floats2half2_rn(u[i], v[i]);
-        if (dim == 3) {
-            const __half2 b = __floats2half2_rn(w[i], 0.f);
-            uint2 q;
-            q.x = *reinterpret_cast<const unsigned *>(&a);
-            q.y = *reinterpret_cast<const unsigned *>(&b);
-            reinterpret_cast<uint2 *>(out)[i] = q;
-        } else {
-            reinterpret_cast<unsigned *>(out)[i] = *reinterpret_cast<const unsigned *>(&a);
-        }
-    }
-}
-
-// Window pair: node n of the pair buffer = node n of the back slot followed by node n of the
-// front slot (elements of E bytes, E = 4, 8 or 16).
-template <typename T>
-__global__ void pair_pack_kernel(const T *__restrict__ back, const T *__restrict__ front, T *out, int64_t nodes) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
-        out[2 * i] = back[i];
-        out[2 * i + 1] = front[i];
-    }
-}
 
 // Seeds (AoS, n x dim) -> state SoA; zeroes the per-particle accumulators.
 __global__ void seed_kernel(const float *__restrict__ seeds, int64_t n, int dim, float *px, float *py,
@@ -174,68 +118,6 @@ __global__ void finalize_kernel(const __grid_constant__ KParams P, int32_t *stat
         if (P.abort_mode != 0) length_out[pid] = P.length[i];
         if (P.curvature_mode != 0) tc_out[pid] = P.tc[i];
     }
-}
-
-int grid_for(int64_t n, int threads) {
-    int64_t b = (n + threads - 1) / threads;
-    if (b < 1) b = 1;
-    if (b > 148 * 64) b = 148 * 64;
-    return (int)b;
-}
-
-template <typename T>
-struct DevBuf {
-    T *p = nullptr;
-    size_t count = 0;
-    ~DevBuf() { reset(); }
-    void reset() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        count = 0;
-    }
-    cudaError_t alloc(size_t n) {
-        if (n <= count && p) return cudaSuccess;
-        reset();
-        if (n == 0) return cudaSuccess;
-        cudaError_t e = cudaMalloc(&p, n * sizeof(T));
-        if (e == cudaSuccess) count = n;
-        else p = nullptr;
-        return e;
-    }
-};
-
-struct PinnedBuf {
-    void *p = nullptr;
-    size_t bytes = 0;
-    cudaEvent_t done = nullptr;
-    ~PinnedBuf() {
-        if (p) cudaFreeHost(p);
-        if (done) cudaEventDestroy(done);
-    }
-};
-
-// Host copy split over up to 8 threads: the staging copies into / out of pinned memory run
-// at a few GB/s on one core, which would otherwise set the pace of a run fed from the host.
-void parallel_memcpy(void *dst, const void *src, size_t bytes) {
-    constexpr size_t kMinChunk = size_t(8) << 20;
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t t = std::min<size_t>({8, hw, std::max<size_t>(1, bytes / kMinChunk)});
-    if (t <= 1) {
-        std::memcpy(dst, src, bytes);
-        return;
-    }
-    const size_t chunk = ((bytes + t - 1) / t + 63) & ~size_t(63);
-    std::vector<std::thread> pool;
-    for (size_t k = 1; k < t; ++k) {
-        const size_t off = k * chunk;
-        if (off >= bytes) break;
-        pool.emplace_back([=] {
-            std::memcpy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off,
-                        std::min(chunk, bytes - off));
-        });
-    }
-    std::memcpy(dst, src, std::min(chunk, bytes));
-    for (auto &th : pool) th.join();
 }
 
 }  // namespace
@@ -715,8 +597,17 @@ int gr_expression_evaluate(const char *code, const char *const *volume_names, in
 }
 
 static int set_seeds(gr_engine *e, const float *pos, int64_t n, int32_t dim, bool device_src) {
-    if (e) ++e->gen;   // device buffers may move: a captured batch is rebuilt
     if (!e || (!pos && n > 0)) return USER_ERR("null argument >");
+    // a captured batch reads the seed buffer when it replays: only a new count or a moved
+    // buffer makes it capture again
+    const float *before = e->seeds.p;
+    const int64_t n_before = e->n;
+    struct Bump {
+        gr_engine *e;
+        const float *p;
+        int64_t n;
+        ~Bump() { if (e->seeds.p != p || e->n != n) ++e->gen; }
+    } bump{e, before, n_before};
     if (dim != e->dim) return USER_ERR("Dimensions of IntegratorSettings and provided TrajectorySet do not match. >");
     if (n <= 0) return USER_ERR("Provided TrajectorySet does not contain any data. >");
     if (n > (int64_t(1) << 31) - 1) return USER_ERR("Too many particles. >");
@@ -1091,7 +982,7 @@ StateView view_of(gr_engine::State &S, int64_t stride) {
     v.px = S.px.p; v.py = S.py.p; v.pz = S.pz.p; v.qx = S.qx.p; v.qy = S.qy.p; v.qz = S.qz.p;
     v.kx = S.kx.p; v.ky = S.ky.p; v.kz = S.kz.p; v.lx = S.lx.p; v.ly = S.ly.p; v.lz = S.lz.p;
     v.length = S.length.p; v.tc = S.tc.p; v.curv = S.curv.p; v.volc = S.volc.p; v.cmpc = S.cmpc.p;
-    v.status = S.status.p; v.id = S.id.p; v.retire = S.retire.p; v.life = S.life.p;
+    v.status = S.status.p; v.id = S.id.p; v.retire = S.retire.p; v.life = S.life.p; v.birth = nullptr;
     v.stride = stride;
     return v;
 }

@@ -66,6 +66,7 @@ struct KParams {
     int64_t n;                    // particles in this launch (prefix of the state arrays)
     const int32_t *n_dev;         // if set: live prefix length on the device (<= n)
     const int32_t *life;          // if set: steps each slot may run (batched sets of uneven lifetime)
+    const int32_t *birth;         // if set: first step each slot runs (served requests joining mid-window)
     int32_t grid_stride;          // 1: persistent grid striding over the live prefix
     int64_t n_state;              // stride of volc / cmpc
     int64_t n_total;              // original particle count (history / constants stride)
@@ -565,6 +566,7 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
     const bool was_alive = alive;
     unsigned long long my_steps = 0;
     const int32_t life = (valid && P.life) ? P.life[i] : 0x7fffffff;   // steps this particle may run
+    const int32_t birth = (valid && P.birth) ? P.birth[i] : 0;          // first step it runs
     const bool extras = (P.volume_mode != 0 && P.nvol > 0) || P.nexpr > 0;
     V3 vc_last{0.f, 0.f, 0.f};
     int last_s = P.s0;
@@ -573,7 +575,7 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
 
     for (int s = P.s0; s < P.s1; ++s) {
         const StepEntry E = P.sched[s];
-        if (alive && s < life) {
+        if (alive && s < life && s >= birth) {
             ++my_steps;
             const int sb = P.wind_dynamic ? E.slot_back : 0, sf = P.wind_dynamic ? E.slot_front : 0;
             const void *wb = IsPair<W>::value ? P.pair : reinterpret_cast<const char *>(P.wind) + (int64_t)sb * P.wind_stride;

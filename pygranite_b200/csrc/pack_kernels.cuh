@@ -1,0 +1,73 @@
+// pack_kernels.cuh — snapshot packing shared by the engine (engine.cu) and the request
+// server (server.cu): float32 planes -> the node-major storage layout of the device ring, and
+// two ring slots -> the window-pair buffer the step kernel reads.  Internal linkage: each
+// translation unit that includes this header owns its instances (static kernels).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace granite_b200 {
+
+// Planes (ncomp x nodes, float32) -> node-major packed snapshot of storage type W.
+template <typename W>
+static __global__ void pack_wind_kernel(const float *__restrict__ u, const float *__restrict__ v,
+                                 const float *__restrict__ w, void *out, int64_t nodes, int dim);
+
+template <>
+__global__ void pack_wind_kernel<float>(const float *__restrict__ u, const float *__restrict__ v,
+                                        const float *__restrict__ w, void *out, int64_t nodes, int dim) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        if (dim == 3) reinterpret_cast<float4 *>(out)[i] = make_float4(u[i], v[i], w[i], 0.f);
+        else reinterpret_cast<float2 *>(out)[i] = make_float2(u[i], v[i]);
+    }
+}
+
+template <>
+__global__ void pack_wind_kernel<__nv_bfloat16>(const float *__restrict__ u, const float *__restrict__ v,
+                                                const float *__restrict__ w, void *out, int64_t nodes, int dim) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        const __nv_bfloat162 a = __floats2bfloat162_rn(u[i], v[i]);
+        if (dim == 3) {
+            const __nv_bfloat162 b = __floats2bfloat162_rn(w[i], 0.f);
+            uint2 q;
+            q.x = *reinterpret_cast<const unsigned *>(&a);
+            q.y = *reinterpret_cast<const unsigned *>(&b);
+            reinterpret_cast<uint2 *>(out)[i] = q;
+        } else {
+            reinterpret_cast<unsigned *>(out)[i] = *reinterpret_cast<const unsigned *>(&a);
+        }
+    }
+}
+
+template <>
+__global__ void pack_wind_kernel<__half>(const float *__restrict__ u, const float *__restrict__ v,
+                                         const float *__restrict__ w, void *out, int64_t nodes, int dim) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        const __half2 a = __floats2half2_rn(u[i], v[i]);
+        if (dim == 3) {
+            const __half2 b = __floats2half2_rn(w[i], 0.f);
+            uint2 q;
+            q.x = *reinterpret_cast<const unsigned *>(&a);
+            q.y = *reinterpret_cast<const unsigned *>(&b);
+            reinterpret_cast<uint2 *>(out)[i] = q;
+        } else {
+            reinterpret_cast<unsigned *>(out)[i] = *reinterpret_cast<const unsigned *>(&a);
+        }
+    }
+}
+
+// Window pair: node n of the pair buffer = node n of the back slot followed by node n of the
+// front slot (elements of E bytes, E = 4, 8 or 16).
+template <typename T>
+static __global__ void pair_pack_kernel(const T *__restrict__ back, const T *__restrict__ front, T *out, int64_t nodes) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        out[2 * i] = back[i];
+        out[2 * i + 1] = front[i];
+    }
+}
+
+}  // namespace granite_b200

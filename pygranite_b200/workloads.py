@@ -190,6 +190,19 @@ def config2(n_particles=1_000_000, n_snapshots=201, grid=(64, 192, 192), steps=2
     return settings, src, seeds
 
 
+def round_storage(a, storage):
+    """The float32 -> storage -> float32 round trip of the device ring (round to nearest even);
+    storage is "f32", "bf16" or "f16"."""
+    a = np.ascontiguousarray(a, np.float32)
+    if storage == "f16":
+        return a.astype(np.float16).astype(np.float32)
+    if storage == "bf16":
+        u = a.view(np.uint32).astype(np.uint64)
+        u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+        return u.astype(np.uint32).view(np.float32)
+    return a
+
+
 def batch_sets(n_sets=512, n_min=100, n_max=200_000, life_min=100, life_max=5000, frac3d=0.7, seed=0):
     """Seed-set descriptors of the batching workload: particle counts log-uniform in
     [n_min, n_max], lifetimes (RK4 steps) uniform in [life_min, life_max], a fraction `frac3d`

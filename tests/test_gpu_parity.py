@@ -10,6 +10,7 @@ in the test.  Against the float64 oracle (the judge) errors are reported in grid
 import numpy as np
 import pytest
 
+from pygranite_b200 import workloads as W
 from tests import harness as H
 
 pytestmark = pytest.mark.gpu
@@ -278,14 +279,7 @@ def test_compaction_with_minimum_alive_and_2d():
 
 def round_storage(a, storage):
     """The float32 -> storage -> float32 round trip of the device ring (round to nearest even)."""
-    a = np.ascontiguousarray(a, np.float32)
-    if storage == "Float16":
-        return a.astype(np.float16).astype(np.float32)
-    if storage == "BFloat16":
-        u = a.view(np.uint32).astype(np.uint64)
-        u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
-        return u.astype(np.uint32).view(np.float32)
-    return a
+    return W.round_storage(a, {"Float16": "f16", "BFloat16": "bf16"}.get(storage, "f32"))
 
 
 # storage error bounds in grid cells after 100 steps (99th percentile over particles alive in
