@@ -54,8 +54,12 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-particles", type=int, default=20000)
     p.add_argument("--cpu-steps", type=int, default=100)
-    p.add_argument("--workload", default="plain", choices=["plain", "batch"],
-                   help="plain: the 3D RK4 configuration; batch: 512 seed sets of uneven size and lifetime")
+    p.add_argument("--workload", default="plain", choices=["plain", "batch", "serve"],
+                   help="plain: the 3D RK4 configuration; batch: 512 seed sets of uneven size and lifetime; "
+                        "serve: a Poisson stream of requests on the request server")
+    p.add_argument("--serve-rate", type=float, default=200.0, help="requests per second")
+    p.add_argument("--serve-seconds", type=float, default=60.0, help="length of the arrival stream")
+    p.add_argument("--serve-storage", default="bf16", choices=["f32", "bf16", "f16"])
     p.add_argument("--batch-storage", default="bf16", choices=["f32", "bf16", "f16"])
     p.add_argument("--batch-sets", type=int, default=512)
     p.add_argument("--tune-steps", type=int, default=40, help="steps per autotuner trial (0 = no tuning)")
@@ -401,11 +405,102 @@ def run_batch(args, world, rank, local, pg_dist):
     }
 
 
+SERVE_WORKLOAD = "serve-poisson-3d-512x512x96"
+
+
+def run_serve(args, world, rank, local, pg_dist):
+    """Requests arrive as a Poisson stream; latency = submit -> results on the host."""
+    import torch
+    from pygranite_b200 import capi
+    from pygranite_b200 import workloads as W
+
+    w = W.ServeWorkload(rate=args.serve_rate, seconds=args.serve_seconds, seed=rank)
+    nz, ny, nx = w.grid
+    code = {"f32": 0, "bf16": 1, "f16": 2}[args.serve_storage]
+    t0 = time.perf_counter()
+    srv = capi.Server(capi.settings_from_reference(w.settings(), storage=code, device=local), w.n_snapshots, w.grid)
+    dev = W.DeviceFourierField(w.field, device=f"cuda:{local}")
+    for k in range(w.n_snapshots):
+        planes = dev.snapshot(600.0 * k)
+        torch.cuda.synchronize()
+        srv.set_snapshot_device(k, [p.data_ptr() for p in planes])
+    del dev
+    torch.cuda.empty_cache()
+    setup_s = time.perf_counter() - t0
+    srv.start()
+    # warm-up: a few small requests so module loading and first-touch costs are not timed
+    for j in range(3):
+        rid = srv.submit(w.seeds(j)[:1000], 600.0 * (3 + 5 * j), 50, j % 2)
+        srv.wait(rid, 60.0)
+        srv.release(rid)
+    s0 = srv.stats()
+    ps0 = s0.particle_steps
+    if pg_dist:
+        pg_dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ids = []
+    start = time.perf_counter()
+    for j in range(len(w.arrivals)):
+        sd = w.seeds(j)
+        delay = w.arrivals[j] - (time.perf_counter() - start)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(sd, float(w.starts[j]), int(w.steps[j]), int(w.integrators[j])))
+    submit_end = time.perf_counter() - start
+    lat, queue, nparts, steps_run = [], [], 0, 0
+    for rid in ids:
+        st = srv.wait(rid, 600.0)
+        info = srv.info(rid)
+        if st == capi.GR_REQ_DONE:
+            lat.append(info.done_s - info.submit_s)
+            queue.append(info.admit_s - info.submit_s)
+            nparts += info.n
+            steps_run += info.steps
+        srv.release(rid)
+    wall = time.perf_counter() - start
+    sampler.stop()
+    clocks = sampler.summary()
+    s1 = srv.stats()
+    srv.close()
+    ps = s1.particle_steps - ps0
+    t_max, ps_all = combine_ranks(pg_dist, wall * 1e3, ps, "cuda")
+    value = ps_all / (t_max / 1e3)
+    if pg_dist:
+        pg_dist.barrier()
+    if rank != 0:
+        return None
+    lat, queue = np.array(lat), np.array(queue)
+    pct = lambda a, q: float(np.percentile(a, q)) if a.size else None  # noqa: E731
+    return {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": 1, "warmup": 3, "ms_per_step": t_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": args.serve_storage,
+        "data": "synthetic (seeded Fourier-mode field, Poisson request stream)",
+        "config": {"workload": SERVE_WORKLOAD, "grid": [nx, ny, nz], "snapshots": w.n_snapshots, "ring_slots": 4,
+                   "rate_per_s": args.serve_rate, "arrival_seconds": args.serve_seconds,
+                   "requests": len(ids), "completed": int(lat.size), "particles": int(nparts),
+                   "storage": args.serve_storage, "parallelism": f"replicas{world}",
+                   "l2": "window pair 403 MB > L2: streamed from HBM"},
+        "latency_s": {"p50": pct(lat, 50), "p90": pct(lat, 90), "p99": pct(lat, 99), "max": pct(lat, 100),
+                      "mean": float(lat.mean()) if lat.size else None},
+        "queue_s": {"p50": pct(queue, 50), "p99": pct(queue, 99)},
+        "server": {"windows": s1.windows, "sweeps": s1.sweeps, "jumps": s1.jumps, "deferred": s1.deferred,
+                   "peak_particles": s1.peak_particles, "capacity_particles": s1.capacity_particles,
+                   "steps_requested_mean": float(np.mean(w.steps)), "steps_run_mean": steps_run / max(1, lat.size),
+                   "submit_seconds": submit_end, "setup_s": setup_s},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(s1.h2d_bytes - s0.h2d_bytes),
+                "d2h_bytes_per_step": int(s1.d2h_bytes - s0.d2h_bytes),
+                "path": "capi.Server.submit (host seeds) -> results on the host; wall clock over the stream"},
+        "roofline": None, "clocks": clocks, "gpu_launches": None,
+    }
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload == "batch":
+    if args.workload in ("batch", "serve"):
         world, rank, local = dist_env()
         import torch
         torch.cuda.set_device(local)
@@ -416,7 +511,8 @@ def main():
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                     device_id=torch.device("cuda", local))
             pg_dist = dist
-        line = run_batch(args, world, rank, local, pg_dist)
+        run = run_batch if args.workload == "batch" else run_serve
+        line = run(args, world, rank, local, pg_dist)
         if line is not None:
             print(json.dumps(line), flush=True)
         if pg_dist:

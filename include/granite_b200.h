@@ -262,8 +262,8 @@ int gr_tune(gr_engine *engine, int32_t trial_steps, gr_tune_result *out);
  * The field (n_snapshots snapshots of nz x ny x nx nodes, DataTimeDistance apart, stored as
  * settings->storage) is packed once into pinned host memory by gr_server_set_snapshot.  A
  * worker thread sweeps it window by window through a 4-slot device ring refilled from there.
- * A request is a seed set, a start time (seconds on the field's clock, rounded to the step
- * grid DeltaT), a step count and an integrator (0 Euler, 1 RK4); it runs from its start step
+ * A request is a seed set, a start time (seconds on the field's clock, rounded down to the
+ * step grid DeltaT), a step count and an integrator (0 Euler, 1 RK4); it runs from its start step
  * until the step count, an abort, or the end of the field, whichever comes first.  Requests
  * whose start falls in the current window join the particle pool of their integrator, while
  * their state fits `hbm_budget_bytes` (0 = a quarter of the free device memory); all requests

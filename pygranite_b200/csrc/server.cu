@@ -5,7 +5,7 @@
 // any thread.  One worker thread sweeps the field window by window: a 4-slot device ring
 // holds the snapshots of the current window and the next ones, refilled from pinned host
 // memory on a copy stream while the current window integrates.  All requests share the
-// field's global step clock (start times are rounded to the step grid), so the particles of
+// field's global step clock (start times are rounded down to the step grid), so the particles of
 // every request active in a window advance in the same launch (continuous batching):
 //
 //   per window, on the compute stream:
@@ -873,7 +873,8 @@ int gr_server_submit(gr_server *S, const float *seeds, int64_t n, int32_t dim, d
     if (integrator != 0 && integrator != 1) return SUSER("Invalid Integrator.");
     if (steps < 0) return SUSER("steps must not be negative");
     const int64_t total = (int64_t)S->sched.steps.size();
-    int64_t k0 = (int64_t)std::llround(start_time / (double)S->s.delta_t);
+    // the step that contains the start time
+    int64_t k0 = (int64_t)std::floor(start_time / (double)S->s.delta_t + 1e-9);
     if (k0 < 0 || k0 >= total) return SUSER("start time outside the field window");
     auto r = std::make_unique<Req>();
     r->integrator = integrator;

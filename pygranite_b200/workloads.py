@@ -105,6 +105,37 @@ class FourierField:
         return [self._eval(c, t) for c in range(self.dim)]
 
 
+class DeviceFourierField:
+    """A FourierField's modes evaluated on a CUDA device with torch (complex64): the same
+    wave vectors, amplitudes, phases and RMS scaling, for fields too large to generate on the
+    host in reasonable time.  Snapshots are float32 CUDA tensors in (z, y, x) / (y, x) order."""
+
+    def __init__(self, field: FourierField, device="cuda"):
+        import torch
+        self.torch, self.field, self.device = torch, field, device
+        self.parts = []
+        for m in field.comps:
+            f = [torch.as_tensor(x, dtype=torch.complex64, device=device) for x in m["factors"]]
+            if field.dim == 3:
+                fz, fy, fx = f
+                b = (fy[:, :, None] * fx[:, None, :]).reshape(fy.shape[0], -1)
+                self.parts.append((fz, b))
+            else:
+                fy, fx = f
+                self.parts.append((fy, fx))
+
+    def snapshot(self, t):
+        torch = self.torch
+        out = []
+        for m, (lead, b) in zip(self.field.comps, self.parts):
+            coef = m["amp"] * np.exp(1j * (m["phase0"] - m["omega"] * t))
+            c = torch.as_tensor(coef, dtype=torch.complex64, device=self.device)
+            a = (c[:, None] * lead).T
+            val = (a @ b).real.reshape(self.field.shape) * float(m.get("scale", 1.0))
+            out.append(val.to(torch.float32).contiguous())
+        return out
+
+
 def temperature(shape, spacing_z, seed=1):
     """T = 290 - 6.5e-3 * z + 2 * N(0,1) noise, z = iz * spacing_z (metres)."""
     nz = shape[0]
@@ -264,6 +295,42 @@ class BatchWorkload:
 
     def particle_steps_upper(self):
         return sum(s["n"] * s["life"] for s in self.sets)
+
+
+class ServeWorkload:
+    """The serving configuration: a Poisson stream of trajectory requests on a 3D field of the
+    plain configuration's spectrum at 512 x 512 x 96 nodes (1 km, 1 km, 250 m), 120 snapshots
+    600 s apart.  Each request: seeds uniform in the lower half of the domain (count
+    log-uniform in [n_min, n_max]), a start time uniform over the field window, a step count
+    uniform in [steps_min, steps_max], RK4 with probability p_rk4, else Euler."""
+
+    def __init__(self, rate=200.0, seconds=60.0, grid=(96, 512, 512), n_snapshots=120, n_min=1000, n_max=500_000,
+                 steps_min=200, steps_max=3000, p_rk4=0.8, seed=0):
+        self.grid, self.n_snapshots, self.seed = tuple(grid), n_snapshots, seed
+        self.field = FourierField(self.grid, (250.0, 1000.0, 1000.0), n_modes=32, seed=seed)
+        rng = np.random.default_rng(seed + 17)
+        t, arrivals = 0.0, []
+        while True:
+            t += rng.exponential(1.0 / rate)
+            if t >= seconds:
+                break
+            arrivals.append(t)
+        k = len(arrivals)
+        self.arrivals = np.array(arrivals)
+        self.counts = np.rint(np.exp(rng.uniform(math.log(n_min), math.log(n_max), k))).astype(np.int64)
+        self.starts = rng.uniform(0.0, 600.0 * (n_snapshots - 1), k)
+        self.steps = rng.integers(steps_min, steps_max + 1, k)
+        self.integrators = (rng.random(k) < p_rk4).astype(np.int32)
+
+    def settings(self):
+        return dict(Space=0, Integrator=1, WindfieldMode=1, DeltaT=60.0, DataTimeDistance=600.0,
+                    GridScale=[1000.0, 1000.0, 250.0], Offset=[0.0, 0.0, 0.0], SaveInterval=0, BorderMode=0,
+                    CurvatureMode=0, MaximumSimulationTime=600.0 * (self.n_snapshots - 1))
+
+    def seeds(self, j):
+        nz, ny, nx = self.grid
+        return uniform_seeds(int(self.counts[j]), self.seed * 1_000_003 + j, [0.0, 0.0, 0.0],
+                             [nx * 1000.0, ny * 1000.0, nz * 250.0 / 2])
 
 
 def apply_settings(obj, settings: dict, enums=None):
