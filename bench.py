@@ -208,56 +208,64 @@ RK4_FINAL_BYTES = {(3, "f32"): 796, (3, "bf16"): 412, (3, "f16"): 412,
 BATCH_WORKLOAD = "batch-512-sets-3d-2d-rk4"
 
 
-def batch_accuracy(w, eng_b, spans, storage, max_life, per_set=64, max_sets=6):
-    """Final-position error in grid cells of the batched run against the float64 oracle, on
-    sets with lifetime <= max_life: against the float32 field (storage rounding included) and
-    against the stored field (integration arithmetic only).  Errors are taken over particles
-    alive at the end in both runs; particles whose abort decision differs (a float64 path
-    crossing the domain edge one step earlier or later) are counted separately."""
+def _cell_err(got, got_st, ref, ref_st, cell):
+    both = (ref_st == 0) & (got_st == 0)
+    d = (np.abs(np.asarray(got, np.float64) - ref) / cell).max(axis=1)[both]
+    return d, int(np.sum(ref_st != got_st))
+
+
+def _summ(d):
+    d = np.concatenate(d) if d else np.zeros(0)
+    if not d.size:
+        return {"particles": 0}
+    return {"particles": int(d.size), "cell_rms": float(np.sqrt(np.mean(d ** 2))),
+            "cell_p99": float(np.percentile(d, 99)), "cell_max": float(d.max())}
+
+
+def batch_accuracy(w, storage, sample, batch_final, plain_final, horizon):
+    """Final-position error in grid cells against the float64 oracle on sampled particles.
+
+    sample[dim] = [(set, count)]; batch_final / plain_final[(dim, horizon_key)][set] =
+    (positions, status) of the batched run and of the float32 plain run.  Two horizons: a
+    fixed one (`horizon` steps, every sampled set) and each set's own lifetime.  Errors are
+    taken over particles alive in both runs; differing abort codes are counted.  Over long
+    horizons this 3D field amplifies any rounding (float32 and float64 arithmetic part by
+    cells after a few hundred steps), so the float32 plain path's own error is reported
+    beside the batched one; "same_field" compares with a float64 run on the stored
+    (rounded) field."""
     from oracle import oracle as orc
     from pygranite_b200 import workloads as W
     out = {}
-    for dim in sorted(eng_b):
-        pos_all = eng_b[dim].final_positions()
-        st_all = eng_b[dim].status()
+    for dim in sorted(sample):
         cell = np.array([1000.0, 1000.0, 250.0][:dim])
-        picked = [(j, off, cnt) for j, off, cnt in spans[dim] if w.sets[j]["life"] <= max_life][:max_sets]
-        if not picked:
-            continue
-        err = {"f": [], "s": []}
-        mism = {"f": 0, "s": 0}
-        steps = []
-        for j, off, cnt in picked:
-            life = w.sets[j]["life"]
-            m = min(per_set, cnt)
-            seeds = w.seeds(j)[:m]
-            snaps = [w.snapshot(dim, k) for k in range(life // 10 + 2)]
-            st = orc.settings(**dict(w.settings(dim), MaximumSimulationTime=60.0 * life))
-            ref = orc.run(st, orc.Inputs(wind=snaps, seeds=seeds), precision="f64")
-            rsnaps = [[W.round_storage(p, storage) for p in sn] for sn in snaps]
-            ref_s = orc.run(st, orc.Inputs(wind=rsnaps, seeds=seeds), precision="f64")
-            got = pos_all[off:off + m].astype(np.float64)
-            got_st = st_all[off:off + m]
-            for key, r in (("f", ref), ("s", ref_s)):
-                both = (r["status"] == 0) & (got_st == 0)
-                mism[key] += int(np.sum(r["status"] != got_st))
-                d = np.abs(got - r["trajectories"][:, -1]) / cell
-                err[key].extend(d.max(axis=1)[both].tolist())
-            steps.append(life)
-
-        def stats(e):
-            e = np.array(e)
-            if not e.size:
-                return None, None, None
-            return float(np.sqrt(np.mean(e ** 2))), float(np.percentile(e, 99)), float(e.max())
-        rf, pf, mf = stats(err["f"])
-        rs, ps_, ms_ = stats(err["s"])
-        out[f"{dim}d"] = {"sets": len(picked), "particles": int(sum(min(per_set, c) for _, _, c in picked)),
-                          "lifetimes": steps, "alive_in_both": len(err["f"]),
-                          "cell_rms_vs_f64": rf, "cell_p99_vs_f64": pf, "cell_max_vs_f64": mf,
-                          "status_mismatch_vs_f64": mism["f"],
-                          "cell_rms_vs_f64_same_field": rs, "cell_p99_vs_f64_same_field": ps_,
-                          "cell_max_vs_f64_same_field": ms_, "status_mismatch_vs_f64_same_field": mism["s"]}
+        res = {}
+        for hkey in ("fixed", "lifetime"):
+            acc = {"batched_vs_f64": [], "batched_vs_f64_same_field": [], "plain_f32_vs_f64": []}
+            mism = {k: 0 for k in acc}
+            steps = []
+            for j, m in sample[dim]:
+                life = w.sets[j]["life"] if hkey == "lifetime" else horizon
+                if (dim, hkey) not in batch_final or j not in batch_final[(dim, hkey)]:
+                    continue
+                seeds = w.seeds(j)[:m]
+                snaps = [w.snapshot(dim, k) for k in range(life // 10 + 2)]
+                st = orc.settings(**dict(w.settings(dim), MaximumSimulationTime=60.0 * life))
+                ref = orc.run(st, orc.Inputs(wind=snaps, seeds=seeds), precision="f64")
+                rsn = [[W.round_storage(p, storage) for p in sn] for sn in snaps]
+                ref_s = orc.run(st, orc.Inputs(wind=rsn, seeds=seeds), precision="f64")
+                bp, bs = batch_final[(dim, hkey)][j]
+                pp, ps_ = plain_final[(dim, hkey)][j]
+                for key, (gp, gs, r) in {"batched_vs_f64": (bp, bs, ref),
+                                         "batched_vs_f64_same_field": (bp, bs, ref_s),
+                                         "plain_f32_vs_f64": (pp, ps_, ref)}.items():
+                    d, mm = _cell_err(gp[:m], gs[:m], r["trajectories"][:, -1], r["status"], cell)
+                    acc[key].append(d)
+                    mism[key] += mm
+                steps.append(life)
+            res[hkey] = {"steps": steps if hkey == "lifetime" else horizon, "sets": len(steps)}
+            for key in acc:
+                res[hkey][key] = dict(_summ(acc[key]), status_mismatch=mism[key])
+        out[f"{dim}d"] = res
     return out
 
 
@@ -346,6 +354,18 @@ def run_batch(args, world, rank, local, pg_dist):
            "d2h_bytes_per_step": int(d2h), "steps": max(1, args.e2e_steps),
            "path": "capi.Engine.set_seeds (host) + capi.Batch.run + final positions / status to host"}
 
+    # ---- accuracy sample: a few sets per field, the first particles of each
+    per_set, horizon = 64, 100
+    sample = {d: [(j, min(per_set, cnt)) for j, off, cnt in spans[d] if w.sets[j]["life"] <= args.acc_life][:6]
+              for d in spans}
+    batch_final, plain_final = {}, {}
+    for d in spans:
+        pos, st = eng_b[d].final_positions(), eng_b[d].status()
+        batch_final[(d, "lifetime")] = {j: (pos[off:off + cnt], st[off:off + cnt])
+                                        for j, off, cnt in spans[d] if any(j == q for q, _ in sample[d])}
+    plain_final = {(d, "lifetime"): {} for d in spans}
+    sampled = {j for d in sample for j, _ in sample[d]}
+
     # ---- plain FP32: one run per set, sequentially, every snapshot resident
     plain_ms, plain_ps = 0.0, 0
     loc = {j: (d, off, cnt) for d in spans for j, off, cnt in spans[d]}
@@ -360,6 +380,8 @@ def run_batch(args, world, rank, local, pg_dist):
         st = e.stats()
         plain_ms += st.run_ms
         plain_ps += st.particle_steps
+        if j in sampled:
+            plain_final[(d, "lifetime")][j] = (e.final_positions(), e.status())
     torch.cuda.synchronize()
     plain_wall = time.perf_counter() - wall0
     p_t, p_ps = combine_ranks(pg_dist, plain_wall * 1e3, plain_ps, "cuda")
@@ -367,7 +389,24 @@ def run_batch(args, world, rank, local, pg_dist):
     pd_t, _ = combine_ranks(pg_dist, plain_ms, plain_ps, "cuda")
     plain_value_dev = p_ps / (pd_t / 1e3)
 
-    acc = batch_accuracy(w, eng_b, spans, bst, args.acc_life) if rank == 0 else None
+    # fixed horizon: the batch again with every lifetime capped, and the sampled sets alone
+    acc = None
+    if rank == 0:
+        for d in spans:
+            eng_b[d].set_lifetimes(np.minimum(groups[d][1], horizon))
+        batch.run()
+        for d in spans:
+            pos, st = eng_b[d].final_positions(), eng_b[d].status()
+            batch_final[(d, "fixed")] = {j: (pos[off:off + cnt], st[off:off + cnt])
+                                         for j, off, cnt in spans[d] if j in sampled}
+            plain_final[(d, "fixed")] = {}
+            for j, m in sample[d]:
+                _, off, cnt = loc[j]
+                eng_p[d].set_seeds(groups[d][0][off:off + cnt])
+                eng_p[d].update_settings(maximum_simulation_time=60.0 * horizon)
+                eng_p[d].run(resident)
+                plain_final[(d, "fixed")][j] = (eng_p[d].final_positions(), eng_p[d].status())
+        acc = batch_accuracy(w, bst, sample, batch_final, plain_final, horizon)
     batch.close()
     for e in list(eng_b.values()) + list(eng_p.values()):
         e.close()
