@@ -63,6 +63,10 @@ def parse():
     p.add_argument("--batch-storage", default="bf16", choices=["f32", "bf16", "f16"])
     p.add_argument("--batch-sets", type=int, default=512)
     p.add_argument("--tune-steps", type=int, default=40, help="steps per autotuner trial (0 = no tuning)")
+    p.add_argument("--batch-life-max", type=int, default=5000, help="longest lifetime of the batching workload")
+    p.add_argument("--no-plain", action="store_true", help="batch: skip the one-run-per-set baseline")
+    p.add_argument("--no-acc", action="store_true", help="batch: skip the float64 accuracy sample")
+    p.add_argument("--serve-budget-gb", type=float, default=0.0, help="serve: HBM budget (0 = 1/4 of free)")
     p.add_argument("--acc-life", type=int, default=500,
                    help="accuracy sample: sets with at most this lifetime are checked against the float64 oracle")
     return p.parse_args()
@@ -275,7 +279,7 @@ def run_batch(args, world, rank, local, pg_dist):
     from pygranite_b200 import capi
     from pygranite_b200 import workloads as W
 
-    w = W.BatchWorkload(n_sets=args.batch_sets, seed=rank)
+    w = W.BatchWorkload(n_sets=args.batch_sets, life_max=args.batch_life_max, seed=rank)
     n_snap = w.n_snapshots
     bst = args.batch_storage
     code = {"f32": 0, "bf16": 1, "f16": 2}
@@ -287,17 +291,19 @@ def run_batch(args, world, rank, local, pg_dist):
         groups[dim] = (seeds, lifes)
         spans[dim] = sp
         eng_b[dim] = capi.Engine(capi.settings_from_reference(w.settings(dim), ring_slots=n_snap, storage=code[bst],
-                                                              device=local))
+                                                              device=local, sort_interval=args.sort_interval))
         eng_b[dim].set_seeds(seeds)
         eng_b[dim].set_lifetimes(lifes)
-        eng_p[dim] = capi.Engine(capi.settings_from_reference(w.settings(dim), ring_slots=n_snap, storage=0,
-                                                              device=local, sort_interval=args.sort_interval))
+        if not args.no_plain:
+            eng_p[dim] = capi.Engine(capi.settings_from_reference(w.settings(dim), ring_slots=n_snap, storage=0,
+                                                                  device=local, sort_interval=args.sort_interval))
     t0 = time.perf_counter()
     for k in range(n_snap):
         for dim in eng_b:
             snap = w.snapshot(dim, k)
             eng_b[dim].load_windfield(k, snap)
-            eng_p[dim].load_windfield(k, snap)
+            if dim in eng_p:
+                eng_p[dim].load_windfield(k, snap)
     load_s = time.perf_counter() - t0
     resident = lambda s: 1 if s < n_snap else 0  # noqa: E731
 
@@ -335,7 +341,7 @@ def run_batch(args, world, rank, local, pg_dist):
     # ---- end to end: new host seeds every step (same counts: the graph replays), final
     # positions and abort codes back to the host
     e2e_s, e2e_ps, h2d, d2h = 0.0, 0, 0, 0
-    for k in range(1 + max(1, args.e2e_steps)):
+    for k in range(0 if args.no_e2e else 1 + max(1, args.e2e_steps)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for d in sorted(eng_b):
@@ -350,7 +356,7 @@ def run_batch(args, world, rank, local, pg_dist):
             d2h = sum(p.nbytes + s_.nbytes for p, s_ in outs)
     assert batch.stats().captures == bst_stats.captures, "new seeds of the same counts must not capture again"
     e_t, e_ps = combine_ranks(pg_dist, e2e_s * 1e3, e2e_ps, "cuda")
-    e2e = {"value": e_ps / (e_t / 1e3), "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
+    e2e = None if args.no_e2e else {"value": e_ps / (e_t / 1e3), "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "steps": max(1, args.e2e_steps),
            "path": "capi.Engine.set_seeds (host) + capi.Batch.run + final positions / status to host"}
 
@@ -371,7 +377,7 @@ def run_batch(args, world, rank, local, pg_dist):
     loc = {j: (d, off, cnt) for d in spans for j, off, cnt in spans[d]}
     torch.cuda.synchronize()
     wall0 = time.perf_counter()
-    for j, s in enumerate(w.sets):
+    for j, s in enumerate([] if args.no_plain else w.sets):
         d, off, cnt = loc[j]
         e = eng_p[d]
         e.set_seeds(groups[d][0][off:off + cnt])
@@ -385,13 +391,13 @@ def run_batch(args, world, rank, local, pg_dist):
     torch.cuda.synchronize()
     plain_wall = time.perf_counter() - wall0
     p_t, p_ps = combine_ranks(pg_dist, plain_wall * 1e3, plain_ps, "cuda")
-    plain_value_wall = p_ps / (p_t / 1e3)
+    plain_value_wall = p_ps / (p_t / 1e3) if p_ps else None
     pd_t, _ = combine_ranks(pg_dist, plain_ms, plain_ps, "cuda")
-    plain_value_dev = p_ps / (pd_t / 1e3)
+    plain_value_dev = p_ps / (pd_t / 1e3) if p_ps else None
 
     # fixed horizon: the batch again with every lifetime capped, and the sampled sets alone
     acc = None
-    if rank == 0:
+    if rank == 0 and not args.no_acc and not args.no_plain:
         for d in spans:
             eng_b[d].set_lifetimes(np.minimum(groups[d][1], horizon))
         batch.run()
@@ -426,14 +432,15 @@ def run_batch(args, world, rank, local, pg_dist):
         "config": {"workload": BATCH_WORKLOAD, "sets": len(w.sets),
                    "particles_per_gpu": int(sum(s["n"] for s in w.sets)),
                    "sets_3d": int(sum(s["dim"] == 3 for s in w.sets)), "snapshots": n_snap,
-                   "lifetimes": [100, 5000], "storage": bst, "parallelism": f"replicas{world}",
+                   "lifetimes": [100, args.batch_life_max], "storage": bst, "parallelism": f"replicas{world}",
                    "l2": f"inputs larger than L2 ({n_snap} snapshots per field resident)", "tuned": tuned,
                    "graph_nodes": bst_stats.nodes},
-        "plain": {"storage": "f32", "value_device": plain_value_dev, "value_wall": plain_value_wall,
-                  "seconds_wall": p_t / 1e3, "particle_steps": int(p_ps),
-                  "path": "one capi.Engine.run per set (set_seeds, MaximumSimulationTime = lifetime * 60 s)"},
-        "speedup_vs_plain_f32": value / plain_value_wall,
-        "speedup_vs_plain_f32_device": value / plain_value_dev,
+        "plain": None if args.no_plain else {
+            "storage": "f32", "value_device": plain_value_dev, "value_wall": plain_value_wall,
+            "seconds_wall": p_t / 1e3, "particle_steps": int(p_ps),
+            "path": "one capi.Engine.run per set (set_seeds, MaximumSimulationTime = lifetime * 60 s)"},
+        "speedup_vs_plain_f32": value / plain_value_wall if plain_value_wall else None,
+        "speedup_vs_plain_f32_device": value / plain_value_dev if plain_value_dev else None,
         "accuracy": acc, "e2e": e2e,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": None, "peak_source": peak_src,
@@ -457,7 +464,8 @@ def run_serve(args, world, rank, local, pg_dist):
     nz, ny, nx = w.grid
     code = {"f32": 0, "bf16": 1, "f16": 2}[args.serve_storage]
     t0 = time.perf_counter()
-    srv = capi.Server(capi.settings_from_reference(w.settings(), storage=code, device=local), w.n_snapshots, w.grid)
+    srv = capi.Server(capi.settings_from_reference(w.settings(), storage=code, device=local), w.n_snapshots, w.grid,
+                      hbm_budget=int(args.serve_budget_gb * (1 << 30)))
     dev = W.DeviceFourierField(w.field, device=f"cuda:{local}")
     for k in range(w.n_snapshots):
         planes = dev.snapshot(600.0 * k)

@@ -297,6 +297,7 @@ typedef struct gr_server_stats {
     int64_t pending, active;
     int64_t clock_steps;         /* steps of the field's clock */
     int64_t windows_per_sweep;
+    int64_t staged_later;        /* completions whose copy-out waited for pinned staging */
 } gr_server_stats;
 int gr_server_create(const gr_settings *settings, int64_t n_snapshots, int64_t nz, int64_t ny, int64_t nx,
                      int64_t hbm_budget_bytes, gr_server **out);

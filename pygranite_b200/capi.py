@@ -88,7 +88,7 @@ class ServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_int64) for k in (
         "submitted", "admitted", "completed", "cancelled", "deferred", "windows", "sweeps", "jumps",
         "particle_steps", "capacity_particles", "peak_particles", "h2d_bytes", "d2h_bytes", "pending", "active",
-        "clock_steps", "windows_per_sweep")]
+        "clock_steps", "windows_per_sweep", "staged_later")]
 
 
 LOADER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64)

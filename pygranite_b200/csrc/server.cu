@@ -11,7 +11,8 @@
 //   per window, on the compute stream:
 //     admit   requests whose start step falls in the window, while their state fits the
 //             HBM budget: seeds -> the tail of the integrator's particle pool;
-//     pack    the window-pair buffer from the two ring slots;
+//     pack    the window-pair buffer from the two ring slots (planar, unpadded on the host
+//             and in the ring: 25% less upload than padded 3D nodes);
 //     advance one persistent grid-stride launch per pool over the window's steps (a
 //             particle runs steps [start, end) of the clock);
 //     retire  compaction + Morton re-sort of each pool; particles that aborted or reached
@@ -36,6 +37,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/granite_b200.h"
@@ -43,7 +45,6 @@
 #include "compact.cuh"
 #include "engine_graph.h"
 #include "host_util.h"
-#include "pack_kernels.cuh"
 #include "schedule.h"
 
 using namespace granite_b200;
@@ -119,6 +120,7 @@ struct Req {
     double t_submit = 0, t_admit = 0, t_done = 0;
     int32_t state = GR_REQ_PENDING;
     bool cancelled = false;
+    bool ended = false;                // its particles have all retired; results wait for staging
     cudaEvent_t done_ev = nullptr;
 };
 
@@ -132,7 +134,7 @@ struct gr_server {
     int64_t n_snap = 0, W = 0;
     Schedule sched;
     DevBuf<StepEntry> d_sched;
-    int64_t node_bytes = 0;            // packed bytes per node and snapshot
+    int64_t elem = 4;                  // bytes per stored value
     std::vector<void *> host_snap;     // pinned packed snapshots
     int64_t snap_bytes = 0, slot_stride = 0;
     DevBuf<char> ring, pair;
@@ -223,15 +225,50 @@ __global__ void append_kernel(const float *__restrict__ seeds, const int32_t *__
 
 __global__ void grow_kernel(int32_t *counts, int32_t m) { counts[0] += m; }
 
+// Host snapshots and ring slots are planar, unpadded (u, v[, w] planes of the storage type,
+// round to nearest even): 25% fewer bytes per 3D upload than padded nodes.
+template <typename T>
+__device__ __forceinline__ T to_storage(float x) {
+    if constexpr (std::is_same<T, __nv_bfloat16>::value) return __float2bfloat16_rn(x);
+    else if constexpr (std::is_same<T, __half>::value) return __float2half_rn(x);
+    else return x;
+}
+
+template <typename T>
+__global__ void planar_pack_kernel(const float *__restrict__ u, const float *__restrict__ v,
+                                   const float *__restrict__ w, T *__restrict__ out, int64_t nodes, int dim) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        out[i] = to_storage<T>(u[i]);
+        out[nodes + i] = to_storage<T>(v[i]);
+        if (dim == 3) out[2 * nodes + i] = to_storage<T>(w[i]);
+    }
+}
+
+// Two planar slots -> the window-pair layout the step kernel reads: per node
+// {u_b, v_b, w_b, 0, u_f, v_f, w_f, 0} (3D) or {u_b, v_b, u_f, v_f} (2D), vector stores.
+template <typename T>
+__global__ void planar_pair_kernel(const T *__restrict__ b, const T *__restrict__ f, T *__restrict__ out,
+                                   int64_t nodes, int dim) {
+    using V = typename std::conditional<sizeof(T) == 4, uint4, uint2>::type;   // 4 values of T
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        if (dim == 3) {
+            alignas(sizeof(V)) T lo[4] = {b[i], b[nodes + i], b[2 * nodes + i], to_storage<T>(0.f)};
+            alignas(sizeof(V)) T hi[4] = {f[i], f[nodes + i], f[2 * nodes + i], to_storage<T>(0.f)};
+            V *o = reinterpret_cast<V *>(out + 8 * i);
+            o[0] = *reinterpret_cast<const V *>(lo);
+            o[1] = *reinterpret_cast<const V *>(hi);
+        } else {
+            alignas(sizeof(V)) T q[4] = {b[i], b[nodes + i], f[i], f[nodes + i]};
+            *reinterpret_cast<V *>(out + 4 * i) = *reinterpret_cast<const V *>(q);
+        }
+    }
+}
+
 __global__ void init_pool_kernel(int32_t *counts) {
     counts[0] = 0;
     counts[1] = 0;
     counts[2] = 0;
     counts[3] = 0;
-}
-
-int storage_bytes(const gr_settings &s, int dim) {
-    return s.storage == GR_STORE_F32 ? (dim == 3 ? 16 : 8) : (dim == 3 ? 8 : 4);
 }
 
 int setup(gr_server *S, int64_t nz, int64_t ny, int64_t nx) {
@@ -252,11 +289,11 @@ int setup(gr_server *S, int64_t nz, int64_t ny, int64_t nx) {
         S->dom[d] = g[d] * S->scale[d];
         S->inv_scale[d] = 1.0f / S->scale[d];
     }
-    S->node_bytes = storage_bytes(s, S->dim);
-    S->snap_bytes = S->nodes * S->node_bytes;
+    S->elem = s.storage == GR_STORE_F32 ? 4 : 2;
+    S->snap_bytes = S->nodes * S->dim * S->elem;                  // planar, unpadded
     S->slot_stride = ((S->snap_bytes + 255) / 256) * 256;
     SK(S->ring.alloc((size_t)S->slot_stride * kRing));
-    SK(S->pair.alloc((size_t)S->snap_bytes * 2));
+    SK(S->pair.alloc((size_t)S->nodes * (S->dim == 3 ? 8 : 4) * S->elem));
     SK(S->raw.alloc((size_t)S->nodes * S->dim));
     S->host_snap.assign((size_t)S->n_snap, nullptr);
     for (int k = 0; k < kRing; ++k) S->ring_holds[k] = -1;
@@ -438,13 +475,20 @@ int pack_pair(gr_server *S, int64_t v) {
     const char *back = S->ring.p + (v % kRing) * S->slot_stride;
     const char *front = S->ring.p + ((v + 1) % kRing) * S->slot_stride;
     const int threads = 256, blocks = grid_for(S->nodes, threads);
-    const int e = (int)S->node_bytes;
-    if (e == 16)
-        pair_pack_kernel<uint4><<<blocks, threads, 0, S->cs>>>((const uint4 *)back, (const uint4 *)front, (uint4 *)S->pair.p, S->nodes);
-    else if (e == 8)
-        pair_pack_kernel<uint2><<<blocks, threads, 0, S->cs>>>((const uint2 *)back, (const uint2 *)front, (uint2 *)S->pair.p, S->nodes);
-    else
-        pair_pack_kernel<unsigned><<<blocks, threads, 0, S->cs>>>((const unsigned *)back, (const unsigned *)front, (unsigned *)S->pair.p, S->nodes);
+    switch (S->s.storage) {
+        case GR_STORE_BF16:
+            planar_pair_kernel<__nv_bfloat16><<<blocks, threads, 0, S->cs>>>(
+                (const __nv_bfloat16 *)back, (const __nv_bfloat16 *)front, (__nv_bfloat16 *)S->pair.p, S->nodes, S->dim);
+            break;
+        case GR_STORE_F16:
+            planar_pair_kernel<__half><<<blocks, threads, 0, S->cs>>>((const __half *)back, (const __half *)front,
+                                                                     (__half *)S->pair.p, S->nodes, S->dim);
+            break;
+        default:
+            planar_pair_kernel<float><<<blocks, threads, 0, S->cs>>>((const float *)back, (const float *)front,
+                                                                    (float *)S->pair.p, S->nodes, S->dim);
+            break;
+    }
     SK(cudaGetLastError());
     return GR_OK;
 }
@@ -663,8 +707,11 @@ void work(gr_server *S) {
         std::vector<Req *> fin;
         for (size_t k = 0; k < S->active.size();) {
             Req *r = S->reqs[S->active[k]].get();
-            if (r->end_step <= k1) {
-                // pinned room for its results; wait for earlier copies to drain if needed
+            if (r->ended || r->end_step <= k1) {
+                r->ended = true;
+                // pinned room for its results; wait for earlier copies to drain if needed.  When
+                // this window's own completions fill the staging, the rest stay in the result
+                // arena and are copied in a later window.
                 int64_t stage;
                 while ((stage = S->pin_alloc.take(r->n * (S->dim + 1))) < 0 && !S->returning.empty()) {
                     cudaEvent_t ev = S->reqs[S->returning.front()]->done_ev;
@@ -673,9 +720,10 @@ void work(gr_server *S) {
                     lk.lock();
                     collect(S, false);
                 }
-                if (stage < 0) {   // cannot happen: every request fits the staging alone
-                    S->failure = "result staging exhausted";
-                    break;
+                if (stage < 0) {
+                    ++S->st.staged_later;
+                    ++k;
+                    continue;
                 }
                 r->stage = stage;
                 fin.push_back(r);
@@ -809,7 +857,10 @@ int gr_server_create(const gr_settings *settings, int64_t n_snapshots, int64_t n
     }
     rc = allocate(S.get(), budget);
     if (rc) return rc;
-    S->pin_res_cap = std::min<int64_t>(S->arena_cap * (S->dim + 1), int64_t(64) << 20);
+    // pinned result staging: a quarter of the arena (at most 256 MB), never less than one full
+    // pool, so any admissible request fits; completions beyond it wait a window
+    S->pin_res_cap = std::max<int64_t>(std::min<int64_t>(S->arena_cap * (S->dim + 1) / 4, int64_t(64) << 20),
+                                       S->pools[0].cap * (S->dim + 1));
     SK(cudaMallocHost(&S->pin_res, (size_t)S->pin_res_cap * sizeof(float)));
     S->pin_alloc.reset(S->pin_res_cap);
     SK(cudaStreamSynchronize(S->cs));
@@ -840,9 +891,16 @@ int gr_server_set_snapshot(gr_server *S, int64_t snapshot, const float *const *c
     char *scratch = S->ring.p;   // slot 0 as packing scratch before the server starts
     const int threads = 256, blocks = grid_for(S->nodes, threads);
     switch (S->s.storage) {
-        case GR_STORE_BF16: pack_wind_kernel<__nv_bfloat16><<<blocks, threads, 0, S->cs>>>(src[0], src[1], src[2], scratch, S->nodes, S->dim); break;
-        case GR_STORE_F16: pack_wind_kernel<__half><<<blocks, threads, 0, S->cs>>>(src[0], src[1], src[2], scratch, S->nodes, S->dim); break;
-        default: pack_wind_kernel<float><<<blocks, threads, 0, S->cs>>>(src[0], src[1], src[2], scratch, S->nodes, S->dim); break;
+        case GR_STORE_BF16:
+            planar_pack_kernel<__nv_bfloat16><<<blocks, threads, 0, S->cs>>>(src[0], src[1], src[2], (__nv_bfloat16 *)scratch,
+                                                                             S->nodes, S->dim);
+            break;
+        case GR_STORE_F16:
+            planar_pack_kernel<__half><<<blocks, threads, 0, S->cs>>>(src[0], src[1], src[2], (__half *)scratch, S->nodes, S->dim);
+            break;
+        default:
+            planar_pack_kernel<float><<<blocks, threads, 0, S->cs>>>(src[0], src[1], src[2], (float *)scratch, S->nodes, S->dim);
+            break;
     }
     SK(cudaGetLastError());
     void *&h = S->host_snap[(size_t)snapshot];
