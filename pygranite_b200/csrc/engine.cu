@@ -167,6 +167,9 @@ struct gr_engine {
     };
     State st[2];                       // double-buffered live state (compaction swaps)
     State ret;                         // retired particles (frozen state)
+    State ck;                          // MinimumAliveParticles: state before the current launch
+    DevBuf<unsigned> alive_at;         // per-step alive counts of a launch, 32 shards per step
+    std::vector<unsigned> h_alive;
     int cur = 0;
     bool compacting = false;
     DevBuf<int32_t> d_counts;          // [0] live, [1] live after a pass, [2] retired
@@ -824,6 +827,30 @@ int64_t resident_prefix(const gr_engine *e) {
     return m;
 }
 
+// MinimumAliveParticles: steps per launch are capped so that their alive counts fit alive_at.
+constexpr int64_t kAliveSteps = 256;
+
+// Device copy of the particle state a step launch writes (checkpoint / rollback).
+int copy_state(gr_engine *e, gr_engine::State &d, gr_engine::State &src, int64_t n) {
+    const size_t N = (size_t)e->n, c = (size_t)n;
+    auto cp = [&](auto &dst, auto &from, size_t count) -> cudaError_t {
+        if (!from.p || !dst.p || count == 0) return cudaSuccess;
+        return cudaMemcpyAsync(dst.p, from.p, count * sizeof(*from.p), cudaMemcpyDeviceToDevice, e->cs);
+    };
+    CK(cp(d.px, src.px, c)); CK(cp(d.py, src.py, c)); CK(cp(d.pz, src.pz, c));
+    CK(cp(d.qx, src.qx, c)); CK(cp(d.qy, src.qy, c)); CK(cp(d.qz, src.qz, c));
+    CK(cp(d.kx, src.kx, c)); CK(cp(d.ky, src.ky, c)); CK(cp(d.kz, src.kz, c));
+    CK(cp(d.lx, src.lx, c)); CK(cp(d.ly, src.ly, c)); CK(cp(d.lz, src.lz, c));
+    CK(cp(d.status, src.status, c));
+    CK(cp(d.length, src.length, c)); CK(cp(d.tc, src.tc, c)); CK(cp(d.curv, src.curv, c));
+    const int nv = std::max(1, e->nvol), ne = std::max(1, e->nexpr);
+    for (int k = 0; k < nv; ++k)
+        CK(cudaMemcpyAsync(d.volc.p + k * N, src.volc.p + k * N, c * 4, cudaMemcpyDeviceToDevice, e->cs));
+    for (int k = 0; k < ne; ++k)
+        CK(cudaMemcpyAsync(d.cmpc.p + k * N, src.cmpc.p + k * N, c * 4, cudaMemcpyDeviceToDevice, e->cs));
+    return GR_OK;
+}
+
 // Keeps the first `steps` steps of a schedule.
 void truncate_schedule(Schedule &sc, int64_t steps) {
     if ((int64_t)sc.steps.size() <= steps) return;
@@ -948,6 +975,11 @@ int run_prepare(gr_engine *e, RunPlan &R, bool graph) {
 
     rc = alloc_state(e);
     if (rc) return rc;
+    if (s.minimum_alive > 0) {
+        rc = alloc_set(e, e->ck, false);
+        if (rc) return rc;
+        CK(e->alive_at.alloc((size_t)kAliveSteps * 32));
+    }
     const size_t N = (size_t)e->n;
     CK(e->hpos.alloc(N * e->L * e->dim));
     if (e->Lc > 0) CK(e->hcurv.alloc(N * e->Lc));
@@ -1035,6 +1067,7 @@ KParams make_params(gr_engine *e) {
     P.nexpr = e->nexpr;
     P.prog = e->d_prog.p;
     P.counters = e->counters.p;
+    P.alive_at = e->s.minimum_alive > 0 ? e->alive_at.p : nullptr;
     return P;
 }
 
@@ -1189,6 +1222,8 @@ struct RunCtx {
     size_t ev_used = 2;        // events 0 and 1 bracket the run
     int64_t executed = 0;      // steps enqueued
     int64_t since_sort = 0;    // launches since the last compaction
+    int64_t alive_known = -1;  // particles alive before the next step (-1: all of them)
+    unsigned long long ps_known = 0;   // particle-steps counted before the next launch
 };
 
 int make_ctx(gr_engine *e, RunPlan &R, RunCtx &r) {
@@ -1261,21 +1296,59 @@ int launch_range(RunCtx &r, int64_t b, int64_t t) {
     gr_engine *e = r.e;
     const RunPlan &R = *r.R;
     if (e->s.minimum_alive > 0) {
-        for (int64_t k = b; k < t; ++k) {
-            // alive() before every step (tpp:973-975)
-            unsigned long long alive = e->n;
-            if (k > 0 || r.executed > 0) {
-                CK(cudaMemcpyAsync(e->h_counters, e->counters.p, 2 * sizeof(unsigned long long),
-                                   cudaMemcpyDeviceToHost, e->cs));
-                CK(cudaStreamSynchronize(e->cs));
-                alive = e->h_counters[1];
+        // The reference checks alive() before every step (tpp:973-975).  Each launch here runs
+        // a whole window and counts the particles alive after every step; when the count
+        // falls below the minimum inside the launch, the state saved before the launch is put
+        // back and exactly the steps the reference runs are launched again.
+        const long long minimum = e->s.minimum_alive;
+        for (int64_t k = b; k < t;) {
+            const long long alive = r.alive_known < 0 ? e->n : r.alive_known;
+            if (alive < minimum) return 1;
+            int64_t k1 = std::min({t, k + R.spl, k + kAliveSteps});
+            const int64_t w = R.sched.steps[k].window;
+            if (e->use_pair) k1 = std::min(k1, R.sched.window_begin[w + 1]);
+            const int64_t L = k1 - k;
+            gr_engine::State &S = e->st[e->cur];
+            const int64_t live = r.P.n;   // upper bound of the live prefix
+            if (L > 1) {
+                const int q = copy_state(e, e->ck, S, live);
+                if (q) return q;
             }
-            if ((long long)alive < (long long)e->s.minimum_alive) return 1;
-            int q = launch_steps(r, k, k + 1, R.sched.steps[k].window);
+            CK(cudaMemsetAsync(e->alive_at.p, 0, (size_t)L * 32 * sizeof(unsigned), e->cs));
+            int q = launch_steps(r, k, k1, w);
             if (q) return q;
-            ++r.executed;
-            q = after_launch(r, k + 1);
+            e->h_alive.resize((size_t)L * 32);
+            CK(cudaMemcpyAsync(e->h_alive.data(), e->alive_at.p, (size_t)L * 32 * sizeof(unsigned),
+                               cudaMemcpyDeviceToHost, e->cs));
+            CK(cudaMemcpyAsync(e->h_counters, e->counters.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                               e->cs));
+            CK(cudaStreamSynchronize(e->cs));
+            auto alive_after = [&](int64_t j) {   // alive after step k + j
+                long long a = 0;
+                for (int h = 0; h < 32; ++h) a += e->h_alive[(size_t)j * 32 + h];
+                return a;
+            };
+            int64_t stop = -1;   // first step of the launch the reference does not run
+            for (int64_t j = 1; j < L && stop < 0; ++j)
+                if (alive_after(j - 1) < minimum) stop = k + j;
+            if (stop >= 0) {
+                // roll back, then run steps [k, stop) only
+                q = copy_state(e, S, e->ck, live);
+                if (q) return q;
+                CK(cudaMemcpyAsync(e->counters.p, &r.ps_known, sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                                   e->cs));
+                q = launch_steps(r, k, stop, w);
+                if (q) return q;
+                CK(cudaStreamSynchronize(e->cs));   // the copy above reads r.ps_known
+                r.executed += stop - k;
+                return 1;
+            }
+            r.alive_known = alive_after(L - 1);
+            r.ps_known = e->h_counters[0];
+            r.executed += L;
+            q = after_launch(r, k1);
             if (q) return q;
+            k = k1;
         }
         return 0;
     }

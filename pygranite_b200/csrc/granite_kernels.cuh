@@ -86,6 +86,7 @@ struct KParams {
     int32_t nvol, ncon, nexpr;
     const Program *prog;          // [4]
     unsigned long long *counters; // [0] particle-steps, [1] alive at the end of the launch
+    unsigned *alive_at;           // if set: [step - s0][32 shards] particles alive after each step
 };
 
 // ------------------------------------------------------------------ helpers
@@ -210,20 +211,16 @@ __device__ __forceinline__ Cell3 make_cell3(const KParams &P, float ax, float ay
     const bool x0 = (unsigned)ix < (unsigned)P.nx, x1 = (unsigned)(ix + 1) < (unsigned)P.nx;
     const bool y0 = (unsigned)iy < (unsigned)P.ny, y1 = (unsigned)(iy + 1) < (unsigned)P.ny;
     const bool z0 = (unsigned)iz < (unsigned)P.nz, z1 = (unsigned)(iz + 1) < (unsigned)P.nz;
-    c.valid = 0;
-    c.valid |= (x0 && y0 && z0) << 0;
-    c.valid |= (x1 && y0 && z0) << 1;
-    c.valid |= (x0 && y1 && z0) << 2;
-    c.valid |= (x1 && y1 && z0) << 3;
-    c.valid |= (x0 && y0 && z1) << 4;
-    c.valid |= (x1 && y0 && z1) << 5;
-    c.valid |= (x0 && y1 && z1) << 6;
-    c.valid |= (x1 && y1 && z1) << 7;
+    // bit k = dz*4 + dy*2 + dx: per axis, the corners on each side form a fixed bit pattern
+    const unsigned X = (x0 ? 0x55u : 0u) | (x1 ? 0xAAu : 0u);
+    const unsigned Y = (y0 ? 0x33u : 0u) | (y1 ? 0xCCu : 0u);
+    const unsigned Z = (z0 ? 0x0Fu : 0u) | (z1 ? 0xF0u : 0u);
+    c.valid = X & Y & Z;
     const int cx = min(max(ix, 0), P.nx - 1), cy = min(max(iy, 0), P.ny - 1), cz = min(max(iz, 0), P.nz - 1);
     c.base = (cz * P.ny + cy) * P.nx + cx;
-    c.sx = (ix + 1 >= 0 && ix + 1 < P.nx && ix >= 0) ? 1 : 0;
-    c.sy = (iy + 1 >= 0 && iy + 1 < P.ny && iy >= 0) ? P.nx : 0;
-    c.sz = (iz + 1 >= 0 && iz + 1 < P.nz && iz >= 0) ? P.nx * P.ny : 0;
+    c.sx = (x0 && x1) ? 1 : 0;
+    c.sy = (y0 && y1) ? P.nx : 0;
+    c.sz = (z0 && z1) ? P.nx * P.ny : 0;
     return c;
 }
 
@@ -776,6 +773,14 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
 #pragma unroll
             for (int e = 0; e < GR_MAX_EXPR; ++e)
                 if (e < P.nexpr) P.hcmp[((int64_t)e * P.n_total + pid) * P.Li + E.irec] = cmp[e];
+        }
+
+        // MinimumAliveParticles: particles alive after this step, one atomic per warp, spread
+        // over 32 counters so that one address does not serialise the warps of the grid
+        if (P.alive_at) {
+            const unsigned m = __ballot_sync(0xffffffffu, valid && alive);
+            if ((threadIdx.x & 31) == 0 && m)
+                atomicAdd(P.alive_at + (int64_t)(s - P.s0) * 32 + (blockIdx.x & 31), (unsigned)__popc(m));
         }
     }
 

@@ -233,6 +233,34 @@ def test_minimum_alive_particles():
     assert eng["trajectories"].shape[1] < 1 + 80, "MinimumAliveParticles never stopped the run"
 
 
+@pytest.mark.parametrize("extra", [dict(), dict(SortInterval=1), dict(WindLayout=1, StepsPerLaunch=7),
+                                   dict(CompensatedPositions=True, SortInterval=2)])
+def test_minimum_alive_stops_inside_a_launch(extra):
+    """MinimumAliveParticles with whole-window launches: the engine counts the particles alive
+    after every step, and when the count falls below the minimum inside a launch it restores
+    the state saved before the launch and runs only the steps the reference runs.  The minimum
+    is chosen from the oracle's abort steps so that the stop falls in the middle of a window;
+    every output must equal the float32 oracle's step-by-step check."""
+    base, wind, seeds = problem3d(seed=11)
+    vols = [{"temp": np.random.default_rng(9).standard_normal((12, 20, 24)).astype(np.float32)} for _ in wind]
+    settings = dict(base, CurvatureMode=3, SaveInterval=3, AdditionalVolumeMode=1,
+                    AdditionalCompute=["x + cv*2", "temp - z"])
+    comp = bool(extra.get("CompensatedPositions", False))
+    free = H.run_oracle(settings, wind, seeds, volumes=vols, precision="f32", compensated=comp)
+    ab = free["step_of_abort"]
+    alive_before = lambda k: int(np.sum((ab < 0) | (ab >= k)))  # noqa: E731
+    # a step inside a window (8 steps per window) right after particles were lost
+    stop = next(k for k in range(11, 30) if k % 8 not in (0, 1) and alive_before(k) < alive_before(k - 1))
+    settings["MinimumAliveParticles"] = alive_before(stop) + 1
+    ref = H.run_oracle(settings, wind, seeds, volumes=vols, precision="f32", compensated=comp)
+    assert ref["steps"] == stop
+    eng = H.run_engine(settings, wind, seeds, volumes=vols, **extra)
+    H.assert_same(eng, ref, ("trajectories", "status", "total_curvature", "curvatures"))
+    assert np.array_equal(eng["volume_info"]["temp"], ref["volume_info"]["temp"])
+    for k in range(2):
+        assert np.array_equal(eng["compute_info"][k], ref["compute_info"][k])
+
+
 def test_loader_exhaustion_truncates_like_reference():
     base, wind, seeds = problem3d(seed=8, n_snap=3)
     settings = dict(base, MaximumSimulationTime=100.0)    # needs 25 windows, 2 available
