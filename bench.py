@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-native", action="store_true", help="skip the native-loader run")
     p.add_argument("--cpu-particles", type=int, default=20000)
     p.add_argument("--cpu-steps", type=int, default=100)
     p.add_argument("--workload", default="plain", choices=["plain", "batch", "serve"],
@@ -664,6 +665,38 @@ def main():
         e2e = {"value": e_psa / e_t, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "steps": args.e2e_steps}
 
+    # ---------------- native loader: snapshots evaluated on the device (gr_field_loader) into
+    # the default 3-slot ring; nothing crosses from the host but seeds and results
+    native = None
+    if not args.no_native:
+        field = W.FourierField((64, 192, 192), (250.0, 1000.0, 1000.0), n_modes=32, seed=rank)
+        f = capi.Field.fourier(field, 600.0, n_snap, device=local)
+        ncs = capi.settings_from_reference(settings, storage=storage, device=local,
+                                           steps_per_launch=args.steps_per_launch, sort_interval=args.sort_interval,
+                                           layout=args.layout)
+        n_s, n_ps, n_ms = 0.0, 0, 0.0
+        for k in range(2):
+            ne = capi.Engine(ncs)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ne.set_seeds(seeds)
+            f.load(ne, 0)
+            f.load(ne, 1)
+            ne.load_volume(0, 0, src.volumes[0]["T"])
+            ne.compile_expression(0, settings["AdditionalCompute"][0], ["T"], [])
+            ne.run_native(f)
+            out = ne.results()
+            dt = time.perf_counter() - t0
+            if k == 1:
+                n_s, n_ps, n_ms = dt, ne.stats().particle_steps, ne.stats().run_ms
+            del out
+            ne.close()
+        f.close()
+        nt, nps = combine_ranks(pg_dist, n_s * 1e3, n_ps, "cuda")
+        native = {"value": nps / (nt / 1e3), "unit": "particle-steps/s", "run_ms": n_ms,
+                  "path": "capi.Engine.run_native(capi.Field.fourier): snapshots evaluated on the device into the "
+                          "3-slot ring; seeds in and every record out through host memory"}
+
     if pg_dist:
         pg_dist.barrier()
     if rank != 0:
@@ -695,7 +728,7 @@ def main():
                    "records": int(info.records), "steps_run": int(info.steps),
                    "sort_interval": args.sort_interval, "steps_per_launch": args.steps_per_launch,
                    "wind_layout": ["window-pair", "ring"][args.layout]},
-        "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+        "e2e": e2e, "native_loader": native, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
         "gpu_launches": int(launches + aux), "wall_s": wall,
     }
     print(json.dumps(line), flush=True)

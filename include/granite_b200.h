@@ -317,6 +317,32 @@ int gr_server_cancel(gr_server *server, int64_t request_id);
 int gr_server_stats_get(gr_server *server, gr_server_stats *out);
 void gr_server_destroy(gr_server *server);
 
+/* Native loaders: analytic windfields evaluated on the device.  The reference feeds every
+ * snapshot through a Python DataLoader returning numpy arrays (DataLoader.hpp:26-81,
+ * TrajectoryIntegrator.cpp:146-360); for synthetic fields these generate each snapshot on the
+ * GPU (float64 arithmetic, rounded to float32) and load it with gr_load_windfield_device, so
+ * a run needs no host snapshot memory and no Python.
+ *   double gyre: u = -pi A sin(pi f) cos(pi y), v = pi A cos(pi f) sin(pi y) df/dx with
+ *     f = eps sin(w t) x^2 + (1 - 2 eps sin(w t)) x on nodes x_i = i lx/nx, y_j = j ly/ny, 2D;
+ *   Fourier modes: component c at node (z, y, x) = scale_c * sum_m amp_cm
+ *     cos(phase_cm - omega_cm t + k_cm . (z dz, y dy, x dx)), 2D or 3D; k, amp, phase, omega
+ *     given per component and mode (k in the grid's axis order: (z, y, x) or (y, x)).
+ * Snapshot k is the field at time k * snapshot_dt. */
+typedef struct gr_field gr_field;
+int gr_field_double_gyre(double A, double eps, double omega, int64_t ny, int64_t nx, double lx, double ly,
+                         double snapshot_dt, int64_t n_snapshots, int32_t device, gr_field **out);
+int gr_field_fourier(int32_t dim, const int64_t *shape, const double *spacing, int32_t n_modes,
+                     const double *k, const double *amp, const double *phase, const double *omega,
+                     const double *scale, double snapshot_dt, int64_t n_snapshots, int32_t device,
+                     gr_field **out);
+/* Evaluates snapshot k and loads it into the engine's ring (the engine's device). */
+int gr_field_load(gr_field *field, gr_engine *engine, int64_t snapshot);
+/* A gr_loader_fn for gr_run: user = the gr_field; returns 0 past its last snapshot. */
+int gr_field_loader(void *user, gr_engine *engine, int64_t snapshot);
+/* Snapshot k's planes copied to host memory, (dim, nz, ny, nx) float32. */
+int gr_field_snapshot(gr_field *field, int64_t snapshot, float *out, int64_t capacity_floats);
+void gr_field_destroy(gr_field *field);
+
 /* Allocation-free advance of particles between two snapshots.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc — code running while a CUDA
  * graph is being captured, hosts whose device memory belongs to their own pool allocator,

@@ -27,7 +27,8 @@ EXPORTS = [
     "gr_set_lifetimes", "gr_batch_create", "gr_batch_destroy", "gr_batch_run", "gr_batch_stats_get", "gr_tune",
     "gr_fetch_final_positions", "gr_server_create", "gr_server_set_snapshot", "gr_server_start",
     "gr_server_submit", "gr_server_wait", "gr_server_result", "gr_server_release", "gr_server_cancel",
-    "gr_server_stats_get", "gr_server_destroy",
+    "gr_server_stats_get", "gr_server_destroy", "gr_field_double_gyre", "gr_field_fourier", "gr_field_load",
+    "gr_field_loader", "gr_field_snapshot", "gr_field_destroy",
 ]
 
 GR_REQ_PENDING, GR_REQ_ACTIVE, GR_REQ_DONE, GR_REQ_CANCELLED, GR_REQ_FAILED = 0, 1, 2, 3, 4
@@ -155,6 +156,14 @@ def lib():
             "gr_server_cancel": (ctypes.c_int, [P, I64]),
             "gr_server_stats_get": (ctypes.c_int, [P, ctypes.POINTER(ServerStats)]),
             "gr_server_destroy": (None, [P]),
+            "gr_field_double_gyre": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, ctypes.c_double, I64, I64, ctypes.c_double, ctypes.c_double, ctypes.c_double, I64, I32,
+                                                    ctypes.POINTER(P)]),
+            "gr_field_fourier": (ctypes.c_int, [I32, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double), I32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.c_double, I64,
+                                                I32, ctypes.POINTER(P)]),
+            "gr_field_load": (ctypes.c_int, [P, P, I64]),
+            "gr_field_loader": (ctypes.c_int, [P, P, I64]),
+            "gr_field_snapshot": (ctypes.c_int, [P, I64, FP, I64]),
+            "gr_field_destroy": (None, [P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -361,6 +370,11 @@ class Engine:
         self._keep.append(fn)
         _check(lib().gr_run(self.h, fn, None))
 
+    def run_native(self, field):
+        """gr_run fed by a native device loader (gr_field_loader): no Python in the loop."""
+        fn = LOADER_FN(ctypes.cast(lib().gr_field_loader, ctypes.c_void_p).value)
+        _check(lib().gr_run(self.h, fn, field.h))
+
     def info(self) -> ResultInfo:
         r = ResultInfo()
         _check(lib().gr_result_info_get(self.h, ctypes.byref(r)))
@@ -496,6 +510,57 @@ class Server:
     def close(self):
         if self.h:
             lib().gr_server_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Field:
+    """gr_field: an analytic windfield evaluated on the device, snapshot by snapshot."""
+
+    def __init__(self, handle, shape):
+        self.h, self.shape = handle, tuple(shape)
+
+    @classmethod
+    def double_gyre(cls, A=0.1, eps=0.25, omega=2 * np.pi / 10, ny=128, nx=256, lx=2.0, ly=1.0, dt=1.0,
+                    n_snapshots=16, device=0):
+        h = ctypes.c_void_p()
+        _check(lib().gr_field_double_gyre(A, eps, omega, ny, nx, lx, ly, dt, n_snapshots, device, ctypes.byref(h)))
+        return cls(h, (ny, nx))
+
+    @classmethod
+    def fourier(cls, field, dt, n_snapshots, device=0):
+        """From a workloads.FourierField: the same wave vectors, amplitudes, phases and scaling."""
+        dim, m = field.dim, len(field.comps[0]["amp"])
+        k = np.ascontiguousarray(np.stack([c["kvec"] for c in field.comps]), np.float64)      # (dim, m, dim)
+        amp = np.ascontiguousarray(np.stack([c["amp"] for c in field.comps]), np.float64)
+        ph = np.ascontiguousarray(np.stack([c["phase0"] for c in field.comps]), np.float64)
+        om = np.ascontiguousarray(np.stack([c["omega"] for c in field.comps]), np.float64)
+        sc = np.ascontiguousarray([c["scale"] for c in field.comps], np.float64)
+        shape = np.ascontiguousarray(field.shape, np.int64)
+        sp = np.ascontiguousarray(field.spacing, np.float64)
+        dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
+        h = ctypes.c_void_p()
+        _check(lib().gr_field_fourier(dim, shape.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), dp(sp), m, dp(k),
+                                      dp(amp), dp(ph), dp(om), dp(sc), dt, n_snapshots, device, ctypes.byref(h)))
+        return cls(h, field.shape)
+
+    def load(self, engine, snapshot):
+        _check(lib().gr_field_load(self.h, engine.h, snapshot))
+
+    def snapshot(self, k):
+        """Snapshot k as float32 planes, (dim, *shape)."""
+        out = np.empty((len(self.shape),) + self.shape, np.float32)
+        _check(lib().gr_field_snapshot(self.h, k, _fp(out), out.size))
+        return out
+
+    def close(self):
+        if self.h:
+            lib().gr_field_destroy(self.h)
             self.h = ctypes.c_void_p()
 
     def __del__(self):

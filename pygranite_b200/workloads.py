@@ -81,7 +81,7 @@ class FourierField:
             phase0 = rng.uniform(0, 2 * math.pi, n_modes)
             omega = kvec @ adv
             factors = [np.exp(1j * np.outer(kvec[:, a], axes[a])) for a in range(self.dim)]
-            self.comps.append(dict(amp=amp, phase0=phase0, omega=omega, factors=factors, scale=1.0))
+            self.comps.append(dict(amp=amp, phase0=phase0, omega=omega, factors=factors, scale=1.0, kvec=kvec))
         for c in range(self.dim):
             r = float(np.sqrt(np.mean(self._eval(c, 0.0).astype(np.float64) ** 2)))
             self.comps[c]["scale"] = (rms[c] / r) if r > 0 else 0.0
