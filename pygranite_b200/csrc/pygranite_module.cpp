@@ -19,6 +19,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include "copy_pool.h"
+
 #include "../../include/granite_b200.h"
 
 namespace py = pybind11;
@@ -167,13 +169,13 @@ class TrajectorySet {
 
     py::array_t<float> trajectories() const {
         py::array_t<float> out({static_cast<py::ssize_t>(n), static_cast<py::ssize_t>(records()), static_cast<py::ssize_t>(dim)});
-        if (out.size()) std::memcpy(out.mutable_data(), traj.data(), out.size() * sizeof(float));
+        if (out.size()) granite_b200::parallel_memcpy(out.mutable_data(), traj.data(), out.size() * sizeof(float));
         return out;
     }
 
     py::array_t<float> cloud() const {
         py::array_t<float> out({static_cast<py::ssize_t>(n * records()), static_cast<py::ssize_t>(dim)});
-        if (out.size()) std::memcpy(out.mutable_data(), traj.data(), out.size() * sizeof(float));
+        if (out.size()) granite_b200::parallel_memcpy(out.mutable_data(), traj.data(), out.size() * sizeof(float));
         return out;
     }
 
@@ -185,7 +187,7 @@ class TrajectorySet {
 
     static py::array_t<float> copy2(const py::array_t<float> &a) {
         py::array_t<float> out({a.shape(0), a.shape(1)});
-        if (out.size()) std::memcpy(out.mutable_data(), a.data(), out.size() * sizeof(float));
+        if (out.size()) granite_b200::parallel_memcpy(out.mutable_data(), a.data(), out.size() * sizeof(float));
         return out;
     }
 
