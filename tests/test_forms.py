@@ -69,3 +69,21 @@ def test_trajectory_server_matches_a_plain_run():
     ref = H.run_engine(dict(settings, MaximumSimulationTime=60.0 * 45), src.wind, seeds)
     assert np.array_equal(st, ref["status"])
     assert np.array_equal(pos, ref["trajectories"][:, -1])
+
+
+@pytest.mark.gpu
+def test_batch_integrator_with_compensation_and_fast_curvature():
+    settings, src, seeds = small_problem(CurvatureMode=2)
+    sets, lives = [seeds[:400], seeds[400:]], [80, 23]
+    s = W.apply_settings(pg.IntegratorSettings(), settings, H.enums(pg))
+    s.CompensatedPositions = True
+    s.WindStorage = pg.WindStorage.Float16
+    b = forms.BatchIntegrator(s, W.make_loader(pg.DataLoader, src), sets, lives)
+    out = b.compute()
+    for j, (x, L) in enumerate(zip(sets, lives)):
+        ref = H.run_engine(dict(settings, MaximumSimulationTime=60.0 * L), src.wind, x, volumes=src.volumes,
+                           CompensatedPositions=True, WindStorage=pg.WindStorage.Float16)
+        assert np.array_equal(out[j].abortReasons(), ref["status"]), j
+        assert np.array_equal(out[j].finalPositions(), ref["trajectories"][:, -1]), j
+        assert np.array_equal(out[j].totalCurvatures(), ref["total_curvature"]), j
+    b.close()

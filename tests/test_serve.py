@@ -154,3 +154,29 @@ def test_server_rejects_unsupported_settings_without_gpu():
         capi.Server(settings(CurvatureMode=1), N_SNAP, GRID)
     with pytest.raises(capi.GraniteError, match="at least two snapshots"):
         capi.Server(settings(), 1, GRID)
+
+
+@pytest.mark.gpu
+def test_two_dimensional_field_alone_and_in_the_mix():
+    grid2 = (32, 48)
+    f = W.FourierField(grid2, (1000.0, 1000.0), n_modes=32, seed=8, rms=(7.0710678, 7.0710678))
+    snaps = [f.snapshot(600.0 * k) for k in range(N_SNAP)]
+    st = capi.settings_from_reference(dict(Space=1, Integrator=1, WindfieldMode=1, DeltaT=60.0, DataTimeDistance=600.0,
+                                           GridScale=[1000.0, 1000.0], Offset=[0.0, 0.0], SaveInterval=0,
+                                           BorderMode=3, MaximumSimulationTime=600.0 * (N_SNAP - 1)), storage=2)
+    srv = capi.Server(st, N_SNAP, grid2)
+    for k, s in enumerate(snaps):
+        srv.set_snapshot(k, s)
+    srv.start()
+    rng = np.random.default_rng(3)
+    reqs = [dict(seeds=W.uniform_seeds(int(rng.integers(20, 800)), 50 + j, [0.0, 0.0], [48000.0, 32000.0]),
+                 start=float(rng.integers(0, 100)) * 60.0, steps=int(rng.integers(5, 120)), integrator=j % 2)
+            for j in range(10)]
+    alone = [run_alone(srv, r) for r in reqs[:3]]
+    ids = [srv.submit(r["seeds"], r["start"], r["steps"], r["integrator"]) for r in reqs]
+    for j, rid in enumerate(ids):
+        assert srv.wait(rid, 120.0) == capi.GR_REQ_DONE
+        if j < 3:
+            pos, status, _ = srv.result(rid)
+            assert np.array_equal(status, alone[j][1]) and np.array_equal(pos, alone[j][0]), j
+    srv.close()
