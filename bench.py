@@ -55,9 +55,12 @@ def parse():
     p.add_argument("--no-native", action="store_true", help="skip the native-loader run")
     p.add_argument("--cpu-particles", type=int, default=20000)
     p.add_argument("--cpu-steps", type=int, default=100)
-    p.add_argument("--workload", default="plain", choices=["plain", "batch", "serve"],
+    p.add_argument("--workload", default="plain", choices=["plain", "batch", "serve", "precision"],
                    help="plain: the 3D RK4 configuration; batch: 512 seed sets of uneven size and lifetime; "
                         "serve: a Poisson stream of requests on the request server")
+    p.add_argument("--prec-particles", type=int, default=4_000_000)
+    p.add_argument("--prec-steps", type=int, default=5000)
+    p.add_argument("--prec-sample", type=int, default=256, help="particles checked against the float64 oracle")
     p.add_argument("--serve-rate", type=float, default=200.0, help="requests per second")
     p.add_argument("--serve-seconds", type=float, default=60.0, help="length of the arrival stream")
     p.add_argument("--serve-storage", default="bf16", choices=["f32", "bf16", "f16"])
@@ -452,6 +455,97 @@ def run_batch(args, world, rank, local, pg_dist):
     }
 
 
+PRECISION_WORKLOAD = "precision-3d-rk4-4e6x5000"
+
+
+def run_precision(args, world, rank, local, pg_dist):
+    """The plain 3D configuration at 4e6 particles x 5,000 steps: float32 wind, and BF16 / FP16
+    wind with Kahan-compensated positions and float64 time weights.  Snapshots are evaluated on
+    the device (gr_field) and the float64 oracle gets host copies of the same snapshots."""
+    import torch
+    from oracle import oracle as orc
+    from pygranite_b200 import capi
+    from pygranite_b200 import workloads as W
+
+    steps = args.prec_steps
+    settings, _, seeds = W.config2(n_particles=args.prec_particles, n_snapshots=2, steps=steps, seed=rank)
+    settings = dict(settings, SaveInterval=100, AdditionalVolumeMode=0, AdditionalCompute=[])
+    n_snap = steps // 10 + 1
+    field = W.FourierField((64, 192, 192), (250.0, 1000.0, 1000.0), n_modes=32, seed=rank)
+    fld = capi.Field.fourier(field, 600.0, n_snap, device=local)
+    # record r >= 1 holds the state after 100 (r - 1) + 1 steps (records after every 100th step)
+    checks = [r for r in (2, 11, 50) if 100 * (r - 1) + 1 <= steps]
+    forms = {"f32": dict(storage=0), "bf16": dict(storage=1, compensated=1, time_mode=1),
+             "f16": dict(storage=2, compensated=1, time_mode=1)}
+    out, hist = {}, {}
+    for name, opt in forms.items():
+        e = capi.Engine(capi.settings_from_reference(settings, ring_slots=n_snap, device=local, sort_interval=4,
+                                                     **opt))
+        e.set_seeds(seeds)
+        for k in range(n_snap):
+            fld.load(e, k)
+        resident = lambda k: 1 if k < n_snap else 0  # noqa: E731
+        e.run(resident)   # warm-up
+        torch.cuda.synchronize()
+        e.run(resident)
+        st = e.stats()
+        t_max, ps_all = combine_ranks(pg_dist, st.run_ms, st.particle_steps, "cuda")
+        res = e.results(volumes=False, compute=False)
+        m = args.prec_sample
+        hist[name] = (res["trajectories"][:m, checks], res["status"][:m])
+        out[name] = {"value": ps_all / (t_max / 1e3), "run_ms": t_max, "particle_steps": ps_all,
+                     "settings": opt}
+        del res
+        e.close()
+    acc = None
+    if rank == 0:
+        m = args.prec_sample
+        snaps = []
+        for k in range(n_snap):
+            a = fld.snapshot(k)
+            snaps.append([a[0], a[1], a[2]])
+        ref = orc.run(orc.settings(**settings), orc.Inputs(wind=snaps, seeds=seeds[:m]), precision="f64")
+        cell = np.array([1000.0, 1000.0, 250.0])
+        acc = {}
+        ab = ref["step_of_abort"]
+        for name in forms:
+            traj, status = hist[name]
+            rows = {"final_status_mismatch": int(np.sum(status != ref["status"]))}
+            for j, r in enumerate(checks):
+                k = 100 * (r - 1) + 1                 # steps the record holds
+                live = (ab < 0) | (ab >= k)           # not yet aborted in the float64 run
+                d = (np.abs(traj[live, j] - ref["trajectories"][live, r]) / cell).max(axis=1)
+                rows[f"after_{k}_steps"] = {
+                    "cell_rms": float(np.sqrt(np.mean(d ** 2))) if d.size else None,
+                    "cell_p50": float(np.median(d)) if d.size else None,
+                    "cell_p99": float(np.percentile(d, 99)) if d.size else None,
+                    "cell_max": float(d.max()) if d.size else None, "particles": int(d.size)}
+            acc[name] = rows
+    fld.close()
+    if pg_dist:
+        pg_dist.barrier()
+    if rank != 0:
+        return None
+    peak, peak_src = load_peaks()
+    return {
+        "metric": "particle-steps/s", "value": out["bf16"]["value"], "unit": "particle-steps/s", "n_gpus": world,
+        "steps": 1, "warmup": 1, "ms_per_step": out["bf16"]["run_ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16",
+        "data": "synthetic (seeded Fourier-mode field evaluated on the device)",
+        "config": {"workload": PRECISION_WORKLOAD, "particles_per_gpu": args.prec_particles, "sim_steps": steps,
+                   "snapshots": n_snap, "grid": [192, 192, 64], "records_every": 100,
+                   "l2": f"inputs larger than L2 ({n_snap} snapshots resident)"},
+        "per_storage": out, "error_vs_f64": acc,
+        "error_note": "position error in grid cells of the first particles against the float64 oracle on the same "
+                      "float32 snapshots, over particles not yet aborted in the float64 run at that record; the f32 "
+                      "row is the plain float32 path.  Particle-step counts differ between rows: in float32 "
+                      "arithmetic a particle creeping toward an upper face freezes once its displacement drops below "
+                      "half an ulp of its position yet stays above the Wind threshold, and stays alive; compensated "
+                      "positions keep creeping like float64 and end with a Wind abort",
+        "e2e": None, "roofline": None, "clocks": None, "gpu_launches": None, "peak_source": peak_src, "peak": peak,
+    }
+
+
 SERVE_WORKLOAD = "serve-poisson-3d-512x512x96"
 
 
@@ -548,7 +642,7 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
-    if args.workload in ("batch", "serve"):
+    if args.workload in ("batch", "serve", "precision"):
         world, rank, local = dist_env()
         import torch
         torch.cuda.set_device(local)
@@ -559,7 +653,7 @@ def main():
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                     device_id=torch.device("cuda", local))
             pg_dist = dist
-        run = run_batch if args.workload == "batch" else run_serve
+        run = {"batch": run_batch, "serve": run_serve, "precision": run_precision}[args.workload]
         line = run(args, world, rank, local, pg_dist)
         if line is not None:
             print(json.dumps(line), flush=True)
