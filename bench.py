@@ -30,7 +30,10 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-BYTES_PER_PARTICLE_STEP = {  # algorithmic bytes per particle-step (roofline section)
+# algorithmic bytes per particle-step of the plain 3D configuration: 4 stages x 2 snapshots x
+# 3 components x 8 corners x element bytes, + 8 corners x 4 B of the volume, + position read /
+# write and status (28 B), + previous position and curvature (20 B), + records every 10 steps
+BYTES_PER_PARTICLE_STEP = {
     "f32": 850, "bf16": 466, "f16": 466,
 }
 WORKLOAD = "trajectory-3d-rk4-curvature-volume-expr"
