@@ -401,3 +401,29 @@ def test_loader_exception_propagates():
     integ = pg.TrajectoryIntegrator(s, BadLoader(), pg.TrajectorySet(seeds))
     with pytest.raises(Boom):
         integ.compute()
+
+
+EDGE_CASES = {
+    "one_particle": dict(n=1),
+    "zero_steps": dict(MaximumSimulationTime=0.0),
+    "shorter_than_a_step": dict(MaximumSimulationTime=0.25),
+    "save_interval_longer_than_run": dict(SaveInterval=1000),
+    "window_equals_step": dict(DeltaT=4.0, MaximumSimulationTime=16.0),
+    "single_snapshot_constant": dict(WindfieldMode=0, n_snap=1),
+}
+
+
+@pytest.mark.parametrize("name", sorted(EDGE_CASES))
+@pytest.mark.parametrize("space", [2, 3])
+def test_edge_cases_bitexact(name, space):
+    """Degenerate sizes and schedules: one particle, no step at all, a run shorter than one
+    step, records rarer than the run, one step per window, one constant snapshot."""
+    case = dict(EDGE_CASES[name])
+    n = case.pop("n", 500)
+    n_snap = case.pop("n_snap", 6)
+    base, wind, seeds = (problem2d if space == 2 else problem3d)(n=max(n, 2), n_snap=n_snap, seed=31)
+    seeds = seeds[:n]
+    settings = dict(base, **case)
+    eng = H.run_engine(settings, wind, seeds)
+    ref = H.run_oracle(settings, wind, seeds, precision="f32")
+    H.assert_same(eng, ref)
