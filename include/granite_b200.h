@@ -229,7 +229,8 @@ int gr_set_lifetimes(gr_engine *engine, const int32_t *steps, int64_t n);
  * before the first gr_batch_run; the loader is not called).  MinimumAliveParticles is not
  * supported (it needs host decisions between steps).  A call that changes an engine (loads,
  * seeds, lifetimes, settings, expressions, gr_run) makes the next gr_batch_run capture again.
- * All engines must use the same device. */
+ * All engines must use the same device.  A batch keeps pointers to its engines: destroy the
+ * batch before any of them. */
 typedef struct gr_batch gr_batch;
 typedef struct gr_batch_stats {
     double graph_ms;             /* device time of the last replay (CUDA events) */
