@@ -5,7 +5,7 @@
  * classes directly with pybind11 (source/pygranite.cpp:41-152); it has no C ABI.  Each
  * entry point below states which reference interface it replaces.  The pybind11 module
  * pygranite_b200/_pygranite (same class, method and enum names as the reference) is one
- * caller; ctypes, cgo or JNI callers bind the same symbols (INTEGRATION.md).
+ * caller; ctypes, cgo or JNI callers bind the same symbols.
  *
  * Conventions: every call returns GR_OK (0) or a negative status; no call exits the
  * process or throws.  gr_last_error() returns the message of the last failure on the
