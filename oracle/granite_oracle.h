@@ -1,9 +1,9 @@
 /*
  * granite_oracle.h — CPU restatement of pygranite's trajectory step path.
  *
- * TEST INFRASTRUCTURE ONLY.  This oracle is the checker for the CUDA engine in
- * pygranite_b200/; only tests/, __graft_entry__.smoke() and bench.py's CPU
- * baseline leg may load it.  It is never the thing measured or shipped.
+ * TEST INFRASTRUCTURE ONLY.  The CUDA engine in pygranite_b200/ is verified against
+ * this oracle; only tests/, __graft_entry__.smoke() and bench.py's CPU baseline leg may
+ * load it.  It is never the thing measured or shipped.
  *
  * Parity pins: the reference (catheart97/pygranite v1.5.0) ships no tests, golden
  * vectors or known-answer tests (its PYGRANITE_TEST hook points at a file that does
@@ -13,7 +13,7 @@
  * kernel built from its sources and run on a B200 (tests/golden/, tests/test_golden.py).
  *
  * One source, both precisions in liboracle.so:
- *   *_f64  REAL = double : the judge (ideal arithmetic, exact 1/scale).
+ *   *_f64  REAL = double : the accuracy reference (ideal arithmetic, exact 1/scale).
  *   *_f32  REAL = float  : follows the CUDA kernel's float operation order (explicit
  *                          fmaf, no contraction) so positions, status, lengths and
  *                          curvature compare bit for bit.

@@ -5,7 +5,7 @@ CPU oracle.  Against the float32 oracle build, which follows the kernel's float 
 order, positions, abort codes, lengths, curvature, volume samples and expression values are
 compared bit for bit; only cases that call transcendental functions (cosf in the sphere
 transform, acosf in FastTotalCurvature, exp/sin/... in expressions) use a tolerance, written
-in the test.  Against the float64 oracle (the judge) errors are reported in grid cells.
+in the test.  Against the float64 oracle (the accuracy reference) errors are reported in grid cells.
 """
 import numpy as np
 import pytest
