@@ -158,7 +158,7 @@ int64_t oracle_schedule(const or_input *in, or_step *steps, int64_t cap, int64_t
     return k;
 }
 
-/* ---------------------------------------------------------------- float64 judge */
+/* ---------------------------------------------------------------- float64 reference */
 #define REAL double
 #define SUF(x) x##_f64
 #define OR_IS_DOUBLE 1
