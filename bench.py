@@ -12,8 +12,10 @@ advanced by one integrator step.
 value : device-resident — every snapshot already packed in HBM (ring of 201 slots), seeds
         on the device; timed with the engine's CUDA events (max over ranks).
 e2e   : the pygranite API, TrajectoryIntegrator(settings, loader, TrajectorySet(seeds))
-        .compute(), with the loader serving host numpy snapshots into a 3-slot device ring;
-        every H2D upload and the D2H copy of the records are inside the timed region.
+        .compute(), with the loader serving host snapshots into a 3-slot device ring; every
+        H2D upload and the D2H copy of the records are inside the timed region.  Loader arrays
+        and results in page-locked host memory (pinned_empty, PinnedResults); the defaults
+        (pageable numpy both ways) are reported beside it as e2e.pageable.
 --impl reference : the reference has no CPU implementation of the path; the CPU oracle port
         (float64, OpenMP on all host cores) runs bounded samples of the same workload.
 """
@@ -727,40 +729,72 @@ def main():
     eng.close()
 
     # ---------------- end to end through the pygranite API (host snapshots, 3-slot ring)
+    # Timed per step: the TrajectoryIntegrator constructor, compute() with every snapshot
+    # uploaded from host memory through the Python loader, and every record copied out to host
+    # arrays.  Headline: the loader serves page-locked arrays (pinned_empty) and the results land
+    # in page-locked arrays (PinnedResults), so both directions are single DMAs.  Beside it, the
+    # defaults: pageable numpy in, fresh numpy arrays out (staging copies on host cores).
     e2e = None
     if not args.no_e2e:
         enums = dict(Space=pg.Space, Integrator=pg.Integrator, WindfieldMode=pg.WindfieldMode,
                      AdditionalVolumeMode=pg.AdditionalVolumeMode, BorderMode=pg.BorderMode,
                      CurvatureMode=pg.CurvatureMode)
-        s = W.apply_settings(pg.IntegratorSettings(), settings, enums)
-        s.WindStorage = [pg.WindStorage.Float32, pg.WindStorage.BFloat16, pg.WindStorage.Float16][storage]
-        s.Device = local
-        s.SortInterval = args.sort_interval
-        s.StepsPerLaunch = args.steps_per_launch
-        s.WindLayout = args.layout
         h2d = seeds.nbytes + sum(p.nbytes for snap in src.wind for p in snap) + src.volumes[0]["T"].nbytes
-        e_ps, e_s, d2h = 0, 0.0, 0
-        for k in range(1 + args.e2e_steps):
-            torch.cuda.synchronize()
-            if pg_dist:
-                pg_dist.barrier()
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            t0 = time.perf_counter()
-            ev0.record()
-            loader = W.make_loader(pg.DataLoader, src)
-            res = pg.TrajectoryIntegrator(s, loader, pg.TrajectorySet(seeds)).compute()
-            ev1.record()
-            torch.cuda.synchronize()
-            dt = max(time.perf_counter() - t0, ev0.elapsed_time(ev1) / 1e3)
-            if k >= 1:
-                e_s += dt
-                e_ps += info.particle_steps
-                d2h = res.trajectories().nbytes + res.computeInfo(0).nbytes + res.volumeInfo("T").nbytes + \
-                    res.totalCurvatures().nbytes + 4 * seeds.shape[0]
-            del res
-        e_t, e_psa = combine_ranks(pg_dist, e_s, e_ps, "cuda")
-        e2e = {"value": e_psa / e_t, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "steps": args.e2e_steps}
+
+        def e2e_run(source, pinned_results):
+            s = W.apply_settings(pg.IntegratorSettings(), settings, enums)
+            s.WindStorage = [pg.WindStorage.Float32, pg.WindStorage.BFloat16, pg.WindStorage.Float16][storage]
+            s.Device = local
+            s.SortInterval = args.sort_interval
+            s.StepsPerLaunch = args.steps_per_launch
+            s.WindLayout = args.layout
+            s.PinnedResults = pinned_results
+            e_ps, e_s, d2h, reps = 0, 0.0, 0, []
+            for k in range(1 + args.e2e_steps):
+                torch.cuda.synchronize()
+                if pg_dist:
+                    pg_dist.barrier()
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                t0 = time.perf_counter()
+                ev0.record()
+                loader = W.make_loader(pg.DataLoader, source)
+                integ = pg.TrajectoryIntegrator(s, loader, pg.TrajectorySet(seeds))
+                t1 = time.perf_counter()
+                res = integ.compute()
+                t2 = time.perf_counter()
+                del integ   # engine teardown is part of the step
+                ev1.record()
+                torch.cuda.synchronize()
+                dt = max(time.perf_counter() - t0, ev0.elapsed_time(ev1) / 1e3)
+                reps.append({"ctor_ms": round(1e3 * (t1 - t0), 1), "compute_ms": round(1e3 * (t2 - t1), 1),
+                             "total_ms": round(1e3 * dt, 1)})
+                if k >= 1:
+                    e_s += dt
+                    e_ps += info.particle_steps
+                    d2h = res.trajectories().nbytes + res.computeInfo(0).nbytes + res.volumeInfo("T").nbytes + \
+                        res.totalCurvatures().nbytes + 4 * seeds.shape[0]
+                del res
+            e_t, e_psa = combine_ranks(pg_dist, e_s, e_ps, "cuda")
+            return {"value": e_psa / e_t, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "steps": args.e2e_steps,
+                    "ms_per_step": 1e3 * e_t / max(1, args.e2e_steps), "reps": reps}
+
+        # the same snapshots and volume, copied once into page-locked memory (data preparation,
+        # outside the timed region)
+        nz_, ny_, nx_ = src.wind[0][0].shape
+        pinned_wind = capi.pinned_empty((n_snap, 3, nz_, ny_, nx_))
+        for k, snap in enumerate(src.wind):
+            for c in range(3):
+                pinned_wind[k, c] = snap[c]
+        pinned_T = capi.pinned_empty(src.volumes[0]["T"].shape)
+        pinned_T[...] = src.volumes[0]["T"]
+        psrc = W.SnapshotSource([[pinned_wind[k, c] for c in range(3)] for k in range(n_snap)],
+                                volumes=[{"T": pinned_T}])
+        e2e = e2e_run(psrc, True)
+        e2e["host_buffers"] = "page-locked: loader arrays from pinned_empty, IntegratorSettings.PinnedResults = True"
+        e2e["pageable"] = e2e_run(src, False)
+        e2e["pageable"]["host_buffers"] = "pageable numpy loader arrays, results in fresh numpy arrays (the defaults)"
+        del psrc, pinned_wind, pinned_T
 
     # ---------------- native loader: snapshots evaluated on the device (gr_field_loader) into
     # the default 3-slot ring; nothing crosses from the host but seeds and results
@@ -782,7 +816,7 @@ def main():
             ne.load_volume(0, 0, src.volumes[0]["T"])
             ne.compile_expression(0, settings["AdditionalCompute"][0], ["T"], [])
             ne.run_native(f)
-            out = ne.results()
+            out = ne.results(pinned=True)
             dt = time.perf_counter() - t0
             if k == 1:
                 n_s, n_ps, n_ms = dt, ne.stats().particle_steps, ne.stats().run_ms
@@ -792,7 +826,7 @@ def main():
         nt, nps = combine_ranks(pg_dist, n_s * 1e3, n_ps, "cuda")
         native = {"value": nps / (nt / 1e3), "unit": "particle-steps/s", "run_ms": n_ms,
                   "path": "capi.Engine.run_native(capi.Field.fourier): snapshots evaluated on the device into the "
-                          "3-slot ring; seeds in and every record out through host memory"}
+                          "3-slot ring; seeds in and every record out to page-locked host arrays"}
 
     if pg_dist:
         pg_dist.barrier()

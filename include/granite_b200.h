@@ -197,6 +197,42 @@ int gr_fetch_compute_info(gr_engine *engine, int32_t index, float *out, int64_t 
 /* The last position record of every particle, (n, dim). */
 int gr_fetch_final_positions(gr_engine *engine, float *out, int64_t capacity_floats);
 
+/* Page-locked host memory.  No counterpart in the reference, whose uploads and result copies
+ * are synchronous copies from and to pageable memory (TrajectoryIntegrator.cpp:444-609,
+ * TrajectoryIntegrator.tpp:997-1049).  Every load above whose source, and every fetch whose
+ * destination, lies wholly in page-locked memory (from gr_host_alloc, cudaHostAlloc or
+ * cudaHostRegister) is one DMA with no staging copy; a load from such memory returns once the
+ * DMA has read it.  Other buffers go through the engine's pinned staging and a parallel host
+ * copy.
+ * gr_host_alloc rounds up to 2 MiB and hands out a cached block when one of the size (up to a
+ * quarter larger) is free; gr_host_free returns a block to the cache while the cached total
+ * stays within the limit (default: a quarter of physical memory; gr_host_cache_limit), and
+ * frees it otherwise.  gr_host_free of a pointer not from gr_host_alloc is GR_ERR_USER.
+ * gr_host_is_pinned returns 1 if `p` lies in page-locked memory known to CUDA, else 0. */
+typedef struct gr_host_cache_stats {
+    int64_t live_bytes;     /* handed out, not yet freed */
+    int64_t cached_bytes;   /* freed, kept for reuse */
+    int64_t limit_bytes;
+    int64_t allocations;    /* page-locked allocations made */
+    int64_t reuses;         /* requests served from the cache */
+} gr_host_cache_stats;
+
+int gr_host_alloc(int64_t bytes, void **out);
+int gr_host_free(void *p);
+int gr_host_cache_limit(int64_t bytes);
+int gr_host_cache_trim(void);
+int gr_host_cache_stats_get(gr_host_cache_stats *out);
+int gr_host_is_pinned(const void *p);
+
+/* Device memory.  Every device buffer of engines, servers and fields comes from one CUDA memory
+ * pool per device that keeps freed memory mapped for reuse (the reference calls cudaMalloc /
+ * cudaFree per run and per integrator, TrajectoryIntegrator.tpp:477-503, 577-771 and
+ * TrajectoryIntegrator.cpp:362-422).  A failed allocation trims the pool and retries once.
+ * gr_device_cache_stats_get reports the pool's mapped and in-use bytes (0 / 0 before its first
+ * use); gr_device_cache_trim returns the idle memory of every pool to the driver. */
+int gr_device_cache_stats_get(int32_t device, int64_t *reserved_bytes, int64_t *used_bytes);
+int gr_device_cache_trim(void);
+
 /* Device-resident variants for callers that keep data on the GPU: the same loads and
  * seeds from device pointers (no host copy). */
 int gr_load_windfield_device(gr_engine *engine, int64_t snapshot, const float *const *components,

@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
@@ -28,7 +29,9 @@ EXPORTS = [
     "gr_fetch_final_positions", "gr_server_create", "gr_server_set_snapshot", "gr_server_start",
     "gr_server_submit", "gr_server_wait", "gr_server_result", "gr_server_release", "gr_server_cancel",
     "gr_server_stats_get", "gr_server_destroy", "gr_field_double_gyre", "gr_field_fourier", "gr_field_load",
-    "gr_field_loader", "gr_field_snapshot", "gr_field_destroy",
+    "gr_field_loader", "gr_field_snapshot", "gr_field_destroy", "gr_host_alloc", "gr_host_free",
+    "gr_host_cache_limit", "gr_host_cache_trim", "gr_host_cache_stats_get", "gr_host_is_pinned",
+    "gr_device_cache_stats_get", "gr_device_cache_trim",
 ]
 
 GR_REQ_PENDING, GR_REQ_ACTIVE, GR_REQ_DONE, GR_REQ_CANCELLED, GR_REQ_FAILED = 0, 1, 2, 3, 4
@@ -90,6 +93,10 @@ class ServerStats(ctypes.Structure):
         "submitted", "admitted", "completed", "cancelled", "deferred", "windows", "sweeps", "jumps",
         "particle_steps", "capacity_particles", "peak_particles", "h2d_bytes", "d2h_bytes", "pending", "active",
         "clock_steps", "windows_per_sweep", "staged_later")]
+
+
+class HostCacheStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int64) for k in ("live_bytes", "cached_bytes", "limit_bytes", "allocations", "reuses")]
 
 
 LOADER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64)
@@ -164,6 +171,15 @@ def lib():
             "gr_field_loader": (ctypes.c_int, [P, P, I64]),
             "gr_field_snapshot": (ctypes.c_int, [P, I64, FP, I64]),
             "gr_field_destroy": (None, [P]),
+            "gr_host_alloc": (ctypes.c_int, [I64, ctypes.POINTER(P)]),
+            "gr_host_free": (ctypes.c_int, [P]),
+            "gr_host_cache_limit": (ctypes.c_int, [I64]),
+            "gr_host_cache_trim": (ctypes.c_int, []),
+            "gr_host_cache_stats_get": (ctypes.c_int, [ctypes.POINTER(HostCacheStats)]),
+            "gr_host_is_pinned": (ctypes.c_int, [P]),
+            "gr_device_cache_stats_get": (ctypes.c_int, [I32, ctypes.POINTER(ctypes.c_int64),
+                                                         ctypes.POINTER(ctypes.c_int64)]),
+            "gr_device_cache_trim": (ctypes.c_int, []),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -257,6 +273,54 @@ def evaluate_expression(code, ref, volume_names=(), constant_names=(), dim=3, cu
     _check(lib().gr_expression_evaluate(code.encode(), vn, len(volume_names), cn, len(constant_names), dim,
                                         curvature_mode, _fp(r), ctypes.byref(out)))
     return out.value
+
+
+def pinned_empty(shape, dtype=np.float32):
+    """Uninitialised array in page-locked host memory from gr_host_alloc; the block returns to the
+    library's cache when the array is released.  Loads from and fetches into such arrays are
+    single DMAs."""
+    dtype = np.dtype(dtype)
+    shape = tuple(int(d) for d in (shape if isinstance(shape, (tuple, list)) else (shape,)))
+    nbytes = int(np.prod(shape, dtype=np.int64)) * dtype.itemsize
+    if nbytes == 0:
+        return np.empty(shape, dtype)
+    p = ctypes.c_void_p()
+    _check(lib().gr_host_alloc(nbytes, ctypes.byref(p)))
+    buf = (ctypes.c_char * nbytes).from_address(p.value)
+    weakref.finalize(buf, lib().gr_host_free, ctypes.c_void_p(p.value))
+    return np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+
+def is_pinned(a) -> bool:
+    """True when the array's data lies in page-locked host memory known to CUDA."""
+    a = np.asarray(a)
+    return a.nbytes > 0 and bool(lib().gr_host_is_pinned(ctypes.c_void_p(a.ctypes.data))) and \
+        bool(lib().gr_host_is_pinned(ctypes.c_void_p(a.ctypes.data + a.nbytes - 1)))
+
+
+def host_cache_stats() -> HostCacheStats:
+    out = HostCacheStats()
+    _check(lib().gr_host_cache_stats_get(ctypes.byref(out)))
+    return out
+
+
+def host_cache_limit(nbytes: int):
+    _check(lib().gr_host_cache_limit(int(nbytes)))
+
+
+def host_cache_trim():
+    _check(lib().gr_host_cache_trim())
+
+
+def device_cache_stats(device=0):
+    """(reserved, used) bytes of the library's device memory pool on `device`."""
+    r, u = ctypes.c_int64(), ctypes.c_int64()
+    _check(lib().gr_device_cache_stats_get(device, ctypes.byref(r), ctypes.byref(u)))
+    return r.value, u.value
+
+
+def device_cache_trim():
+    _check(lib().gr_device_cache_trim())
 
 
 class Engine:
@@ -385,10 +449,13 @@ class Engine:
         _check(lib().gr_stats_get(self.h, ctypes.byref(s)))
         return s
 
-    def results(self, volumes=True, compute=True):
+    def results(self, volumes=True, compute=True, pinned=False):
+        """Every result array; pinned=True places the record arrays in page-locked memory
+        (pinned_empty), which the engine fills by one DMA each."""
         info = self.info()
         n, L, D = info.n, info.records, info.dim
-        pos = np.empty((n, L, D), np.float32)
+        alloc = pinned_empty if pinned else np.empty
+        pos = alloc((n, L, D), np.float32)
         _check(lib().gr_fetch_positions(self.h, _fp(pos), pos.size))
         st = np.empty(n, np.int32)
         _check(lib().gr_fetch_status(self.h, st.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), n))
@@ -404,14 +471,14 @@ class Engine:
         if volumes:
             vols = []
             for k in range(info.n_volumes):
-                a = np.empty((n, info.info_records), np.float32)
+                a = alloc((n, info.info_records), np.float32)
                 _check(lib().gr_fetch_volume_info(self.h, k, _fp(a), a.size))
                 vols.append(a)
             out["volume_info"] = vols
         if compute:
             cmps = []
             for k in range(info.n_expressions):
-                a = np.empty((n, info.info_records), np.float32)
+                a = alloc((n, info.info_records), np.float32)
                 _check(lib().gr_fetch_compute_info(self.h, k, _fp(a), a.size))
                 cmps.append(a)
             out["compute_info"] = cmps

@@ -151,6 +151,7 @@ struct gr_engine {
     DevBuf<float> raw;                 // device staging of one snapshot's planes
     PinnedBuf pin[2];
     int pin_next = 0;
+    cudaEvent_t upload_done = nullptr; // end of a DMA straight from a caller's page-locked buffer
     PinnedBuf bounce[2];               // pinned staging of result copies
 
     // expressions
@@ -214,6 +215,7 @@ struct gr_engine {
         if (h_counters) cudaFreeHost(h_counters);
         if (h_live) cudaFreeHost(h_live);
         if (live_ready) cudaEventDestroy(live_ready);
+        if (upload_done) cudaEventDestroy(upload_done);
         if (cs) cudaStreamDestroy(cs);
         if (xs) cudaStreamDestroy(xs);
     }
@@ -238,6 +240,33 @@ int ensure_pinned(gr_engine *e, size_t bytes, PinnedBuf *&out) {
     }
     if (!b.done) CK(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
     out = &b;
+    return GR_OK;
+}
+
+// True when [p, p + bytes) lies in page-locked host memory known to CUDA (cudaHostAlloc,
+// cudaHostRegister, gr_host_alloc): the DMA engines read and write it directly.
+bool pinned_range(const void *p, size_t bytes) {
+    return bytes > 0 && gr_host_is_pinned(p) && gr_host_is_pinned(static_cast<const char *>(p) + bytes - 1);
+}
+
+// Host -> device copy on the copy stream, after whatever the stream already holds.  A
+// page-locked source is read by the DMA engine directly, and the call returns once that copy
+// is done (the caller may release the source); any other source is staged through the
+// double-buffered pinned staging by a parallel host copy.
+int upload(gr_engine *e, void *dst, const void *src, size_t bytes) {
+    if (pinned_range(src, bytes)) {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, e->xs));
+        CK(cudaEventRecord(e->upload_done, e->xs));
+        CK(cudaEventSynchronize(e->upload_done));
+    } else {
+        PinnedBuf *pb = nullptr;
+        int rc = ensure_pinned(e, bytes, pb);
+        if (rc) return rc;
+        parallel_memcpy(pb->p, src, bytes);
+        CK(cudaMemcpyAsync(dst, pb->p, bytes, cudaMemcpyHostToDevice, e->xs));
+        CK(cudaEventRecord(pb->done, e->xs));
+    }
+    e->stats.h2d_bytes += (int64_t)bytes;
     return GR_OK;
 }
 
@@ -324,12 +353,19 @@ int load_wind(gr_engine *e, int64_t snapshot, const float *const *comps, int32_t
         if (rc) return rc;
     }
     const int slot = (int)(snapshot % e->K);
-    rc = wait_slot_free(e, slot);
-    if (rc) return rc;
     const size_t plane = (size_t)e->nodes;
     float *raw[3] = {e->raw.p, e->raw.p + plane, e->raw.p + 2 * plane};
+    // The planes go to the device staging `raw` first (free once the previous pack on this
+    // stream has run); only the pack into the ring slot waits for the slot to be released.
+    bool pinned = !device_src;
+    for (int c = 0; c < ncomp && pinned; ++c) pinned = pinned_range(comps[c], plane * sizeof(float));
     if (device_src) {
         for (int c = 0; c < ncomp; ++c) raw[c] = const_cast<float *>(comps[c]);
+    } else if (pinned) {
+        for (int c = 0; c < ncomp; ++c)
+            CK(cudaMemcpyAsync(raw[c], comps[c], plane * sizeof(float), cudaMemcpyHostToDevice, e->xs));
+        CK(cudaEventRecord(e->upload_done, e->xs));
+        e->stats.h2d_bytes += (int64_t)(plane * ncomp * sizeof(float));
     } else {
         PinnedBuf *pb = nullptr;
         rc = ensure_pinned(e, plane * ncomp * sizeof(float), pb);
@@ -340,10 +376,13 @@ int load_wind(gr_engine *e, int64_t snapshot, const float *const *comps, int32_t
         CK(cudaEventRecord(pb->done, e->xs));
         e->stats.h2d_bytes += (int64_t)(plane * ncomp * sizeof(float));
     }
+    rc = wait_slot_free(e, slot);
+    if (rc) return rc;
     rc = pack_launch(e, raw[0], raw[1], e->dim == 3 ? raw[2] : raw[1], slot);
     if (rc) return rc;
     CK(cudaEventRecord(e->slot_ready[slot], e->xs));
     if (device_src) CK(cudaStreamSynchronize(e->xs));
+    if (pinned) CK(cudaEventSynchronize(e->upload_done));   // the caller may release its planes
     e->wind_holds[slot] = snapshot;
     return GR_OK;
 }
@@ -406,6 +445,7 @@ int gr_create(const gr_settings *settings, gr_engine **out) {
         CK(cudaEventCreateWithFlags(&e->slot_free[k], cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&e->slot_ready[k], cudaEventDisableTiming));
     }
+    CK(cudaEventCreateWithFlags(&e->upload_done, cudaEventDisableTiming));
     e->wind_holds.assign(e->K, -1);
     e->vol_holds.assign(e->K, -1);
     e->cons_holds.assign(e->K, -1);
@@ -443,16 +483,10 @@ int gr_load_volume(gr_engine *e, int64_t snapshot, int32_t index, const float *d
     const int slot = (int)(snapshot % e->K);
     rc = wait_slot_free(e, slot);
     if (rc) return rc;
-    PinnedBuf *pb = nullptr;
-    const size_t bytes = (size_t)e->nodes * sizeof(float);
-    rc = ensure_pinned(e, bytes, pb);
-    if (rc) return rc;
-    parallel_memcpy(pb->p, data, bytes);
     float *dst = e->vol.p + ((int64_t)slot * GR_MAX_VOLUMES + index) * e->nodes;
-    CK(cudaMemcpyAsync(dst, pb->p, bytes, cudaMemcpyHostToDevice, e->xs));
-    CK(cudaEventRecord(pb->done, e->xs));
+    rc = upload(e, dst, data, (size_t)e->nodes * sizeof(float));
+    if (rc) return rc;
     CK(cudaEventRecord(e->slot_ready[slot], e->xs));
-    e->stats.h2d_bytes += (int64_t)bytes;
     if (snapshot == 0 && index + 1 > e->nvol) e->nvol = index + 1;
     e->vol_holds[slot] = snapshot;
     return GR_OK;
@@ -470,16 +504,9 @@ int gr_load_constant(gr_engine *e, int64_t snapshot, int32_t index, const float 
     const int slot = (int)(snapshot % e->K);
     rc = wait_slot_free(e, slot);
     if (rc) return rc;
-    PinnedBuf *pb = nullptr;
-    const size_t bytes = (size_t)n * sizeof(float);
-    rc = ensure_pinned(e, bytes, pb);
+    rc = upload(e, e->cons.p + ((int64_t)slot * GR_MAX_CONSTANTS + index) * e->n, data, (size_t)n * sizeof(float));
     if (rc) return rc;
-    parallel_memcpy(pb->p, data, bytes);
-    CK(cudaMemcpyAsync(e->cons.p + ((int64_t)slot * GR_MAX_CONSTANTS + index) * e->n, pb->p, bytes,
-                       cudaMemcpyHostToDevice, e->xs));
-    CK(cudaEventRecord(pb->done, e->xs));
     CK(cudaEventRecord(e->slot_ready[slot], e->xs));
-    e->stats.h2d_bytes += (int64_t)bytes;
     if (snapshot == 0 && index + 1 > e->ncon) e->ncon = index + 1;
     e->cons_holds[slot] = snapshot;
     return GR_OK;
@@ -498,15 +525,9 @@ int gr_load_uplift(gr_engine *e, int64_t snapshot, const float *data, int64_t n,
     const int slot = (int)(snapshot % e->K);
     rc = wait_slot_free(e, slot);
     if (rc) return rc;
-    PinnedBuf *pb = nullptr;
-    const size_t bytes = (size_t)n * 3 * sizeof(float);
-    rc = ensure_pinned(e, bytes, pb);
+    rc = upload(e, e->lift.p + (int64_t)slot * e->n * 3, data, (size_t)n * 3 * sizeof(float));
     if (rc) return rc;
-    parallel_memcpy(pb->p, data, bytes);
-    CK(cudaMemcpyAsync(e->lift.p + (int64_t)slot * e->n * 3, pb->p, bytes, cudaMemcpyHostToDevice, e->xs));
-    CK(cudaEventRecord(pb->done, e->xs));
     CK(cudaEventRecord(e->slot_ready[slot], e->xs));
-    e->stats.h2d_bytes += (int64_t)bytes;
     e->has_uplift = true;
     e->lift_holds[slot] = snapshot;
     return GR_OK;
@@ -1630,6 +1651,12 @@ static int fetch_rows(gr_engine *e, void *out, int64_t capacity, const void *src
     if (rc) return rc;
     const size_t row_bytes = (size_t)row_used * elem, total = row_bytes * (size_t)rows;
     e->stats.d2h_bytes += (int64_t)total;
+    if (pinned_range(out, total)) {
+        // page-locked destination: one DMA, no staging
+        CK(cudaMemcpy2DAsync(out, row_bytes, src, row_stride * elem, row_bytes, rows, cudaMemcpyDeviceToHost, e->cs));
+        CK(cudaStreamSynchronize(e->cs));
+        return GR_OK;
+    }
     constexpr size_t kBounce = size_t(64) << 20;
     if (total < 2 * kBounce || row_bytes > kBounce) {
         CK(cudaMemcpy2D(out, row_bytes, src, row_stride * elem, row_bytes, rows, cudaMemcpyDeviceToHost));

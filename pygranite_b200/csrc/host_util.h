@@ -18,6 +18,12 @@
 
 namespace granite_b200 {
 
+// Device memory from the library's per-device pool (memory.cu): freed blocks stay mapped and
+// are reused, so repeated runs do not pay cudaMalloc / cudaFree.
+cudaError_t dev_alloc(void **p, size_t bytes);
+void dev_free(void *p);
+size_t dev_pool_idle_bytes();
+
 inline int grid_for(int64_t n, int threads) {
     int64_t b = (n + threads - 1) / threads;
     if (b < 1) b = 1;
@@ -31,7 +37,7 @@ struct DevBuf {
     size_t count = 0;
     ~DevBuf() { reset(); }
     void reset() {
-        if (p) cudaFree(p);
+        if (p) dev_free(p);
         p = nullptr;
         count = 0;
     }
@@ -39,7 +45,7 @@ struct DevBuf {
         if (n <= count && p) return cudaSuccess;
         reset();
         if (n == 0) return cudaSuccess;
-        cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+        cudaError_t e = dev_alloc(reinterpret_cast<void **>(&p), n * sizeof(T));
         if (e == cudaSuccess) count = n;
         else p = nullptr;
         return e;

@@ -78,7 +78,24 @@ struct IntegratorSettings {
     int32_t BlockSize{0};
     int32_t Device{0};
     int32_t WindLayout{0};
+    bool PinnedResults{false};
 };
+
+// float32 array of `shape` in page-locked host memory (gr_host_alloc); the block returns to the
+// library's cache when the array is released.  The engine's uploads from, and result copies
+// into, such arrays are single DMAs without staging copies.
+py::array_t<float> pinned_empty(const std::vector<py::ssize_t> &shape) {
+    size_t count = 1;
+    for (auto d : shape) {
+        if (d < 0) user_error("negative dimension");
+        count *= static_cast<size_t>(d);
+    }
+    if (count == 0) return py::array_t<float>(shape);
+    void *p = nullptr;
+    if (gr_host_alloc(static_cast<int64_t>(count * sizeof(float)), &p) != GR_OK) throw std::runtime_error(gr_last_error());
+    py::capsule owner(p, [](void *q) { gr_host_free(q); });
+    return py::array_t<float>(shape, static_cast<float *>(p), owner);
+}
 
 class DataLoader {
   public:
@@ -437,6 +454,11 @@ class TrajectoryIntegrator {
         }
     }
 
+    // Result storage: page-locked (one DMA per result) with PinnedResults, else plain numpy.
+    py::array_t<float> result_array(const std::vector<py::ssize_t> &shape) const {
+        return settings_.PinnedResults ? pinned_empty(shape) : py::array_t<float>(shape);
+    }
+
     std::unique_ptr<TrajectorySet> collect(bool comp) {
         gr_result_info info;
         check(gr_result_info_get(engine_, &info));
@@ -445,7 +467,7 @@ class TrajectoryIntegrator {
         set->n = n_;
         set->dim = static_cast<size_t>(dim_);
         const auto N = static_cast<py::ssize_t>(n_);
-        set->traj = py::array_t<float>({N, static_cast<py::ssize_t>(info.records), static_cast<py::ssize_t>(dim_)});
+        set->traj = result_array({N, static_cast<py::ssize_t>(info.records), static_cast<py::ssize_t>(dim_)});
         check(gr_fetch_positions(engine_, set->traj.mutable_data(), static_cast<int64_t>(set->traj.size())));
         std::vector<int32_t> st(n_);
         check(gr_fetch_status(engine_, st.data(), static_cast<int64_t>(n_)));
@@ -459,12 +481,12 @@ class TrajectoryIntegrator {
             set->total_curvature.resize(n_);
             check(gr_fetch_total_curvature(engine_, set->total_curvature.data(), static_cast<int64_t>(n_)));
         }
-        set->curv = py::array_t<float>({N, static_cast<py::ssize_t>(info.curvature_records)});
+        set->curv = result_array({N, static_cast<py::ssize_t>(info.curvature_records)});
         if (info.curvature_records > 0)
             check(gr_fetch_curvatures(engine_, set->curv.mutable_data(), static_cast<int64_t>(set->curv.size())));
         if (settings_.AdditionalVolumeMode != AdditionalVolumeMode::Off) {
             for (size_t k = 0; k < vol_keys_.size(); ++k) {
-                py::array_t<float> a({N, static_cast<py::ssize_t>(info.info_records)});
+                py::array_t<float> a = result_array({N, static_cast<py::ssize_t>(info.info_records)});
                 check(gr_fetch_volume_info(engine_, static_cast<int32_t>(k), a.mutable_data(), static_cast<int64_t>(a.size())));
                 set->volume_data.emplace_back(vol_keys_[k], a);
             }
@@ -472,7 +494,7 @@ class TrajectoryIntegrator {
         if (comp) {
             set->num_compute = settings_.AdditionalCompute.size();
             for (size_t e = 0; e < set->num_compute; ++e) {
-                py::array_t<float> a({N, static_cast<py::ssize_t>(info.info_records)});
+                py::array_t<float> a = result_array({N, static_cast<py::ssize_t>(info.info_records)});
                 check(gr_fetch_compute_info(engine_, static_cast<int32_t>(e), a.mutable_data(), static_cast<int64_t>(a.size())));
                 set->compute_data.push_back(a);
             }
@@ -576,7 +598,12 @@ PYBIND11_MODULE(_pygranite, m) {
         .def_readwrite("SortInterval", &IntegratorSettings::SortInterval)
         .def_readwrite("BlockSize", &IntegratorSettings::BlockSize)
         .def_readwrite("Device", &IntegratorSettings::Device)
-        .def_readwrite("WindLayout", &IntegratorSettings::WindLayout);
+        .def_readwrite("WindLayout", &IntegratorSettings::WindLayout)
+        .def_readwrite("PinnedResults", &IntegratorSettings::PinnedResults);
+
+    m.def("pinned_empty", &pinned_empty, py::arg("shape"),
+          "Uninitialised float32 array in page-locked host memory (engine extension).  Loader data "
+          "and results in such arrays move by one DMA, without staging copies.");
 
     py::class_<TrajectoryIntegrator>(m, "TrajectoryIntegrator")
         .def(py::init<IntegratorSettings &, DataLoader &, TrajectorySet &>(), py::keep_alive<1, 3>())

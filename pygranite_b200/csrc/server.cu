@@ -853,7 +853,7 @@ int gr_server_create(const gr_settings *settings, int64_t n_snapshots, int64_t n
     if (budget <= 0) {
         size_t fr = 0, tot = 0;
         SK(cudaMemGetInfo(&fr, &tot));
-        budget = (int64_t)(fr / 4);
+        budget = (int64_t)((fr + dev_pool_idle_bytes()) / 4);   // the pool's idle memory is ours to use
     }
     rc = allocate(S.get(), budget);
     if (rc) return rc;

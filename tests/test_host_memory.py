@@ -1,0 +1,179 @@
+"""Page-locked host memory (gr_host_*, pinned_empty, IntegratorSettings.PinnedResults).
+
+Loads from and fetches into page-locked buffers are single DMAs without staging copies; the
+results must be bit-for-bit those of the staged path, and a load must be finished with the
+caller's buffer when it returns (a loader may overwrite its buffer for the next snapshot)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import pygranite_b200 as pg
+from pygranite_b200 import capi
+from pygranite_b200 import workloads as W
+from tests import harness as H
+
+
+def test_settings_field_defaults_off():
+    assert pg.IntegratorSettings().PinnedResults is False
+
+
+def test_host_cache_rejects_foreign_pointers_and_bad_sizes():
+    L = capi.lib()
+    a = np.zeros(16, np.float32)
+    assert L.gr_host_free(ctypes.c_void_p(a.ctypes.data)) == -1
+    assert b"not from gr_host_alloc" in L.gr_last_error()
+    assert L.gr_host_free(None) == 0
+    p = ctypes.c_void_p(1)
+    assert L.gr_host_alloc(0, ctypes.byref(p)) == 0 and not p.value
+    assert L.gr_host_alloc(-5, ctypes.byref(p)) == -1
+    assert L.gr_host_cache_limit(-1) == -1
+    assert L.gr_host_is_pinned(None) == 0
+    s = capi.host_cache_stats()
+    assert s.live_bytes >= 0 and s.cached_bytes >= 0 and s.limit_bytes > 0
+
+
+@pytest.mark.gpu
+def test_pinned_arrays_are_page_locked_and_reused():
+    a = capi.pinned_empty((1000, 3))
+    assert capi.is_pinned(a) and a.shape == (1000, 3) and a.dtype == np.float32
+    assert not capi.is_pinned(np.empty((1000, 3), np.float32))
+    b = pg.pinned_empty([7, 5])
+    assert capi.is_pinned(b) and b.shape == (7, 5)
+    s0 = capi.host_cache_stats()
+    del a   # its 2 MiB block goes back to the cache
+    s1 = capi.host_cache_stats()
+    assert s1.cached_bytes == s0.cached_bytes + (2 << 20) and s1.live_bytes == s0.live_bytes - (2 << 20)
+    c = capi.pinned_empty(2999)   # fits a cached 2 MiB block
+    s2 = capi.host_cache_stats()
+    assert s2.reuses == s1.reuses + 1 and s2.allocations == s1.allocations and capi.is_pinned(c)
+    assert capi.pinned_empty(0).size == 0
+
+
+def _pinned_source(src):
+    """The same snapshots, each array copied into page-locked memory."""
+    def pin(a):
+        p = capi.pinned_empty(a.shape)
+        p[...] = a
+        return p
+    wind = [[pin(c) for c in snap] for snap in src.wind]
+    vols = [{k: pin(v) for k, v in d.items()} for d in src.volumes]
+    cons = [{k: pin(v) for k, v in d.items()} for d in src.constants]
+    lift = [pin(u) for u in src.uplift]
+    return W.SnapshotSource(wind, volumes=vols, constants=cons, uplift=lift)
+
+
+class _OneBufferLoader:
+    """A loader that serves every snapshot from ONE set of page-locked buffers, overwritten when
+    the next snapshot is requested: correct only if each load has finished reading its source
+    when it returns."""
+
+    def __new__(cls, src):
+        bufs = dict(wind=[capi.pinned_empty(c.shape) for c in src.wind[0]],
+                    vols={k: capi.pinned_empty(v.shape) for k, v in src.volumes[0].items()},
+                    cons={k: capi.pinned_empty(v.shape) for k, v in src.constants[0].items()},
+                    lift=capi.pinned_empty(src.uplift[0].shape))
+
+        class Loader(pg.DataLoader):
+            def __init__(self):
+                pg.DataLoader.__init__(self)
+                self.k = -1
+                self.fill(0)
+
+            def fill(self, k):
+                self.k = k
+                for dst, c in zip(bufs["wind"], src.wind[k]):
+                    dst[...] = c
+                for name, v in src.volumes[k].items():
+                    bufs["vols"][name][...] = v
+                for name, v in src.constants[k].items():
+                    bufs["cons"][name][...] = v
+                bufs["lift"][...] = src.uplift[k]
+
+            def step(self):
+                if self.k + 1 < len(src.wind):
+                    self.fill(self.k + 1)
+                    return True
+                return False
+
+            def windfield(self):
+                return bufs["wind"]
+
+            def additionalVolumes(self):
+                return bufs["vols"]
+
+            def constants(self):
+                return bufs["cons"]
+
+            def uplift(self):
+                return bufs["lift"]
+
+        return Loader()
+
+
+def _problem(n=3000, n_snap=6, seed=0):
+    rng = np.random.default_rng(seed)
+    shape = (12, 20, 24)
+    wind = [[(rng.standard_normal(shape) * (1.0 if c < 2 else 0.2)).astype(np.float32) for c in range(3)]
+            for _ in range(n_snap)]
+    seeds = rng.uniform([0, 0, 0], [24, 20, 12], (n, 3)).astype(np.float32)
+    vols = [{"temp": rng.standard_normal(shape).astype(np.float32)} for _ in range(n_snap)]
+    cons = [{"ka": rng.standard_normal(n).astype(np.float32)} for _ in range(n_snap)]
+    lift = [(rng.standard_normal((n, 3)) * 0.05).astype(np.float32) for _ in range(n_snap)]
+    settings = dict(Space=0, Integrator=1, WindfieldMode=1, DeltaT=0.5, DataTimeDistance=4.0,
+                    GridScale=[1.0, 1.0, 1.0], Offset=[0.0, 0.0, 0.0], SaveInterval=1, MaximumSimulationTime=16.0,
+                    CurvatureMode=3, AdditionalVolumeMode=2, ConstantsMode=2, UpLiftMode=2,
+                    AdditionalCompute=["temp*ka + z", "sqrt(u*u+v*v)"])
+    return settings, W.SnapshotSource(wind, volumes=vols, constants=cons, uplift=lift), seeds
+
+
+def _run(settings, loader, seeds, pinned_results):
+    s = W.apply_settings(pg.IntegratorSettings(), settings, H.enums(pg))
+    s.PinnedResults = pinned_results
+    res = pg.TrajectoryIntegrator(s, loader, pg.TrajectorySet(seeds)).compute()
+    return dict(trajectories=res.trajectories(), status=np.array([int(a) for a in res.abortReasons()], np.int32),
+                total_curvature=res.totalCurvatures(), curvatures=res.curvatures(),
+                volume_info={"temp": res.volumeInfo("temp")},
+                compute_info=[res.computeInfo(0), res.computeInfo(1)])
+
+
+@pytest.mark.gpu
+def test_pinned_loads_and_results_match_the_oracle():
+    settings, src, seeds = _problem()
+    ref = H.run_oracle(settings, src.wind, seeds, volumes=src.volumes, constants=src.constants,
+                       uplift=src.uplift, precision="f32")
+    runs = {
+        "staged": _run(settings, W.make_loader(pg.DataLoader, src), seeds, False),
+        "pinned source": _run(settings, W.make_loader(pg.DataLoader, _pinned_source(src)), seeds, True),
+        "one reused buffer": _run(settings, _OneBufferLoader(src), seeds, True),
+    }
+    for name, eng in runs.items():
+        H.assert_same(eng, ref, ("trajectories", "status", "total_curvature", "curvatures"))
+        assert np.array_equal(eng["volume_info"]["temp"], ref["volume_info"]["temp"]), name
+        for e in range(2):
+            assert np.array_equal(eng["compute_info"][e], ref["compute_info"][e]), (name, e)
+
+
+@pytest.mark.gpu
+def test_pinned_fetch_matches_staged_fetch_for_large_and_pitched_results():
+    # 300,000 particles x 41 records x 3 floats = 148 MB: the staged path bounces through
+    # pinned buffers.  The loader runs dry after 40 of 60 windows, so 41 of the 61 planned
+    # records of each particle are filled (a pitched copy).
+    settings, src, seeds = W.config2(n_particles=300_000, n_snapshots=41, grid=(16, 24, 24), steps=600)
+    eng = capi.Engine(capi.settings_from_reference(settings))
+    eng.set_seeds(seeds)
+    for k in (0, 1):
+        eng.load_windfield(k, src.wind[k])
+    eng.load_volume(0, 0, src.volumes[0]["T"])
+    eng.compile_expression(0, settings["AdditionalCompute"][0], ["T"], [])
+    eng.run(lambda k: (eng.load_windfield(k, src.wind[k]), 1)[1] if k < len(src.wind) else 0)
+    staged = eng.results()
+    pinned = eng.results(pinned=True)
+    assert capi.is_pinned(pinned["trajectories"]) and not capi.is_pinned(staged["trajectories"])
+    info = staged["info"]
+    assert info.records == 41, info.records
+    for k in ("trajectories", "status", "total_curvature"):
+        assert np.array_equal(staged[k], pinned[k]), k
+    assert np.array_equal(staged["volume_info"][0], pinned["volume_info"][0])
+    assert np.array_equal(staged["compute_info"][0], pinned["compute_info"][0])
+    eng.close()
