@@ -197,6 +197,32 @@ int gr_fetch_compute_info(gr_engine *engine, int32_t index, float *out, int64_t 
 /* The last position record of every particle, (n, dim). */
 int gr_fetch_final_positions(gr_engine *engine, float *out, int64_t capacity_floats);
 
+/* Result streaming.  The reference copies every saved step to the host synchronously inside
+ * its step loop (copyParticleInfo, TrajectoryIntegrator.tpp:997-1049).  Here the records stay
+ * in a device history, and with destinations set, gr_run also copies the position, volume and
+ * compute records into these caller arrays while it runs: whenever enough records are complete
+ * (rows of at least 256 bytes per particle), one pitched DMA per array on a separate stream,
+ * overlapped with the steps and the snapshot uploads; the remainder when the run ends.  When
+ * gr_run returns, record r of particle i is at positions[(i * records_capacity + r) * dim + d]
+ * for r < records (gr_result_info_get), volume k's record r at
+ * volume_info[k][i * info_capacity + r] and expression e's at compute_info[e][i *
+ * info_capacity + r] for r < info_records.  The capacities must cover the run's records (the
+ * counts of gr_plan for the same settings), and every non-null array must lie in page-locked
+ * host memory (gr_host_alloc, cudaHostAlloc, cudaHostRegister): GR_ERR_USER at gr_run
+ * otherwise.  Null arrays are not copied.  Runs with MinimumAliveParticles copy at the end
+ * only; graph runs (gr_batch_*) do not stream.  The device history stays valid, so the
+ * gr_fetch_* calls still work.  The destinations apply to every later gr_run of the engine
+ * until gr_set_result_destinations(engine, NULL). */
+typedef struct gr_result_destinations {
+    float *positions;                           /* (n, records_capacity, dim) */
+    int64_t records_capacity;
+    float *volume_info[GR_MAX_VOLUMES];         /* (n, info_capacity) each */
+    float *compute_info[GR_MAX_EXPRESSIONS];    /* (n, info_capacity) each */
+    int64_t info_capacity;
+} gr_result_destinations;
+
+int gr_set_result_destinations(gr_engine *engine, const gr_result_destinations *dest);
+
 /* Page-locked host memory.  No counterpart in the reference, whose uploads and result copies
  * are synchronous copies from and to pageable memory (TrajectoryIntegrator.cpp:444-609,
  * TrajectoryIntegrator.tpp:997-1049).  Every load above whose source, and every fetch whose

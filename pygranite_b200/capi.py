@@ -31,7 +31,7 @@ EXPORTS = [
     "gr_server_stats_get", "gr_server_destroy", "gr_field_double_gyre", "gr_field_fourier", "gr_field_load",
     "gr_field_loader", "gr_field_snapshot", "gr_field_destroy", "gr_host_alloc", "gr_host_free",
     "gr_host_cache_limit", "gr_host_cache_trim", "gr_host_cache_stats_get", "gr_host_is_pinned",
-    "gr_device_cache_stats_get", "gr_device_cache_trim",
+    "gr_device_cache_stats_get", "gr_device_cache_trim", "gr_set_result_destinations",
 ]
 
 GR_REQ_PENDING, GR_REQ_ACTIVE, GR_REQ_DONE, GR_REQ_CANCELLED, GR_REQ_FAILED = 0, 1, 2, 3, 4
@@ -93,6 +93,12 @@ class ServerStats(ctypes.Structure):
         "submitted", "admitted", "completed", "cancelled", "deferred", "windows", "sweeps", "jumps",
         "particle_steps", "capacity_particles", "peak_particles", "h2d_bytes", "d2h_bytes", "pending", "active",
         "clock_steps", "windows_per_sweep", "staged_later")]
+
+
+class ResultDestinations(ctypes.Structure):
+    _fields_ = [("positions", ctypes.c_void_p), ("records_capacity", ctypes.c_int64),
+                ("volume_info", ctypes.c_void_p * 8), ("compute_info", ctypes.c_void_p * 4),
+                ("info_capacity", ctypes.c_int64)]
 
 
 class HostCacheStats(ctypes.Structure):
@@ -180,6 +186,7 @@ def lib():
             "gr_device_cache_stats_get": (ctypes.c_int, [I32, ctypes.POINTER(ctypes.c_int64),
                                                          ctypes.POINTER(ctypes.c_int64)]),
             "gr_device_cache_trim": (ctypes.c_int, []),
+            "gr_set_result_destinations": (ctypes.c_int, [P, ctypes.POINTER(ResultDestinations)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -448,6 +455,27 @@ class Engine:
         s = Stats()
         _check(lib().gr_stats_get(self.h, ctypes.byref(s)))
         return s
+
+    def stream_results(self, positions=None, volume_info=(), compute_info=()):
+        """Page-locked arrays that later runs fill while they go (gr_set_result_destinations):
+        positions (n, records_capacity, dim), volume / compute info (n, info_capacity) each.
+        No arguments turns streaming off."""
+        if positions is None and not volume_info and not compute_info:
+            self._streamed = None
+            _check(lib().gr_set_result_destinations(self.h, None))
+            return
+        d = ResultDestinations()
+        if positions is not None:
+            d.positions = positions.ctypes.data
+            d.records_capacity = positions.shape[1]
+        caps = [a.shape[1] for a in list(volume_info) + list(compute_info) if a is not None]
+        d.info_capacity = caps[0] if caps else 0
+        for k, a in enumerate(volume_info):
+            d.volume_info[k] = a.ctypes.data if a is not None and a.size else None
+        for k, a in enumerate(compute_info):
+            d.compute_info[k] = a.ctypes.data if a is not None and a.size else None
+        self._streamed = (positions, list(volume_info), list(compute_info))   # kept alive
+        _check(lib().gr_set_result_destinations(self.h, ctypes.byref(d)))
 
     def results(self, volumes=True, compute=True, pinned=False):
         """Every result array; pinned=True places the record arrays in page-locked memory

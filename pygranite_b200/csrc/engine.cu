@@ -200,6 +200,15 @@ struct gr_engine {
     uint64_t gen = 0;                  // bumped by every call that may move device buffers
     int64_t graph_executed = 0, graph_records = 0;
 
+    // result streaming (gr_set_result_destinations)
+    gr_result_destinations dest{};
+    bool dest_set = false;
+    bool dest_run = false;             // this run copies into the destinations
+    bool dest_during = false;          // ... already while it runs
+    int32_t streamed = 0;              // records [0, streamed) are copied or on their way
+    cudaStream_t ds = nullptr;         // stream of those copies
+    cudaEvent_t ds_ev = nullptr;
+
     // results
     bool have_result = false;
     gr_result_info info{};
@@ -216,6 +225,9 @@ struct gr_engine {
         if (h_live) cudaFreeHost(h_live);
         if (live_ready) cudaEventDestroy(live_ready);
         if (upload_done) cudaEventDestroy(upload_done);
+        if (ds) cudaStreamSynchronize(ds);
+        if (ds_ev) cudaEventDestroy(ds_ev);
+        if (ds) cudaStreamDestroy(ds);
         if (cs) cudaStreamDestroy(cs);
         if (xs) cudaStreamDestroy(xs);
     }
@@ -928,6 +940,8 @@ int run_prepare(gr_engine *e, RunPlan &R, bool graph) {
         return USER_ERR("MinimumAliveParticles needs host decisions between steps; it cannot run in a graph. >");
     e->have_result = false;
     ++e->gen;
+    e->streamed = 0;   // records copied out by result streaming (stream_begin turns it on)
+    e->dest_run = e->dest_during = false;
     {
         const int64_t h2d = e->stats.h2d_bytes, d2h = e->stats.d2h_bytes;
         e->stats = gr_stats{};
@@ -1151,13 +1165,15 @@ int compact_pass(gr_engine *e, int32_t rec_now, int32_t k_end, bool graph) {
 
 // Records a retired particle would have written after it left the live set: its frozen
 // state, for records retire .. rec_end-1.
+// Position / volume / compute records [max(retire, rec_lo), rec_end) of every retired particle,
+// and with a table its per-step curvature records from its retirement on.
 __global__ void fill_forward_kernel(const __grid_constant__ KParams P, StateView R, const int32_t *n_ret,
-                                    const int32_t *crec_of_rec, int32_t rec_end) {
+                                    const int32_t *crec_of_rec, int32_t rec_lo, int32_t rec_end) {
     const int64_t nr = *n_ret;
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nr; j += (int64_t)gridDim.x * blockDim.x) {
         const int64_t pid = R.id[j];
         const float x = R.px[j], y = R.py[j], z = P.dim == 3 ? R.pz[j] : 0.f;
-        for (int32_t r = R.retire[j]; r < rec_end; ++r) {
+        for (int32_t r = max(R.retire[j], rec_lo); r < rec_end; ++r) {
             float *hp = P.hpos + (pid * P.L + r) * P.dim;
             hp[0] = x;
             hp[1] = y;
@@ -1168,9 +1184,12 @@ __global__ void fill_forward_kernel(const __grid_constant__ KParams P, StateView
                     for (int k = 0; k < P.nvol; ++k) P.hvol[((int64_t)k * P.n_total + pid) * P.Li + irec] = R.volc[k * R.stride + j];
                 for (int k = 0; k < P.nexpr; ++k) P.hcmp[((int64_t)k * P.n_total + pid) * P.Li + irec] = R.cmpc[k * R.stride + j];
             }
-            const int32_t cr = crec_of_rec[r];
-            if (P.curvature_mode == 3 && cr >= 0) P.hcurv[pid * P.Lc + cr] = R.curv[j];
         }
+        if (crec_of_rec && P.curvature_mode == 3)
+            for (int32_t r = R.retire[j]; r < rec_end; ++r) {
+                const int32_t cr = crec_of_rec[r];
+                if (cr >= 0) P.hcurv[pid * P.Lc + cr] = R.curv[j];
+            }
     }
 }
 
@@ -1387,6 +1406,110 @@ int launch_range(RunCtx &r, int64_t b, int64_t t) {
     return 0;
 }
 
+// ---------------------------------------------------------------- result streaming
+
+// Row bytes per particle below which a streamed copy waits for more records: pitched DMAs of
+// short rows run well below the link rate (about 38 GB/s at 240 B, 52 GB/s at 600 B on B200).
+constexpr int64_t kStreamRowBytes = 256;
+
+// Checks the destinations against this run's history and turns streaming on for it.
+int stream_begin(gr_engine *e, const RunPlan &R) {
+    e->dest_run = e->dest_during = false;
+    e->streamed = 0;
+    if (!e->dest_set || R.graph) return GR_OK;
+    const gr_result_destinations &d = e->dest;
+    const size_t n = (size_t)e->n;
+    if (d.positions) {
+        if (d.records_capacity < e->L)
+            return USER_ERR("Result destinations hold %lld records per particle; the run writes %lld. >",
+                            (long long)d.records_capacity, (long long)e->L);
+        if (!pinned_range(d.positions, n * (size_t)d.records_capacity * e->dim * sizeof(float)))
+            return USER_ERR("Result destinations must be page-locked host memory. >");
+    }
+    auto check_info = [&](const float *a) -> int {
+        if (!a || e->Li == 0) return GR_OK;
+        if (d.info_capacity < e->Li)
+            return USER_ERR("Result destinations hold %lld info records per particle; the run writes %lld. >",
+                            (long long)d.info_capacity, (long long)e->Li);
+        if (!pinned_range(a, n * (size_t)std::max<int64_t>(d.info_capacity, 1) * sizeof(float)))
+            return USER_ERR("Result destinations must be page-locked host memory. >");
+        return GR_OK;
+    };
+    for (int k = 0; k < (e->s.volume_mode != 0 ? e->nvol : 0); ++k) {
+        const int rc = check_info(d.volume_info[k]);
+        if (rc) return rc;
+    }
+    for (int k = 0; k < e->nexpr; ++k) {
+        const int rc = check_info(d.compute_info[k]);
+        if (rc) return rc;
+    }
+    if (!e->ds) CK(cudaStreamCreateWithFlags(&e->ds, cudaStreamNonBlocking));
+    if (!e->ds_ev) CK(cudaEventCreateWithFlags(&e->ds_ev, cudaEventDisableTiming));
+    e->dest_run = true;
+    e->dest_during = e->s.minimum_alive == 0;
+    return GR_OK;
+}
+
+// Copies records [e->streamed, r1) of every particle (and their volume / compute records) into
+// the destinations on the copy-out stream, behind everything already on the step stream.
+// Particles retired so far get those records filled first; particles still in the live set
+// wrote them in the step kernel.
+int stream_records(RunCtx &r, int32_t r1) {
+    gr_engine *e = r.e;
+    const int32_t r0 = e->streamed;
+    if (r1 <= r0 || e->n == 0) return GR_OK;
+    if (e->compacting) {
+        const StateView Rv = view_of(e->ret, e->n);
+        fill_forward_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(r.P, Rv, e->d_counts.p + 2, nullptr, r0, r1);
+        CK(cudaGetLastError());
+        e->stats.aux_launches++;
+    }
+    CK(cudaEventRecord(e->ds_ev, e->cs));
+    CK(cudaStreamWaitEvent(e->ds, e->ds_ev, 0));
+    const gr_result_destinations &d = e->dest;
+    const int64_t n = e->n;
+    // rows of `width` floats, one pitched DMA
+    auto copy_rows = [&](float *dst, int64_t dpitch, const float *src, int64_t spitch, int64_t width) -> int {
+        CK(cudaMemcpy2DAsync(dst, (size_t)dpitch * sizeof(float), src, (size_t)spitch * sizeof(float),
+                             (size_t)width * sizeof(float), (size_t)n, cudaMemcpyDeviceToHost, e->ds));
+        e->stats.d2h_bytes += width * n * (int64_t)sizeof(float);
+        return GR_OK;
+    };
+    if (d.positions) {
+        const int rc = copy_rows(d.positions + (size_t)r0 * e->dim, d.records_capacity * e->dim,
+                                 e->hpos.p + (size_t)r0 * e->dim, e->L * e->dim, (int64_t)(r1 - r0) * e->dim);
+        if (rc) return rc;
+    }
+    // info record i belongs to position record i + 1
+    const int32_t i0 = std::max(r0 - 1, 0), i1 = r1 - 1;
+    if (i1 > i0) {
+        auto copy_info = [&](float *dst, const float *src) -> int {
+            if (!dst) return GR_OK;
+            return copy_rows(dst + i0, d.info_capacity, src + i0, e->Li, i1 - i0);
+        };
+        for (int k = 0; k < (e->s.volume_mode != 0 ? e->nvol : 0); ++k) {
+            const int rc = copy_info(d.volume_info[k], e->hvol.p + (size_t)k * n * e->Li);
+            if (rc) return rc;
+        }
+        for (int k = 0; k < e->nexpr; ++k) {
+            const int rc = copy_info(d.compute_info[k], e->hcmp.p + (size_t)k * n * e->Li);
+            if (rc) return rc;
+        }
+    }
+    e->streamed = r1;
+    return GR_OK;
+}
+
+// During the run: streams the records complete after the steps enqueued so far once they fill
+// rows of kStreamRowBytes.
+int stream_progress(RunCtx &r) {
+    gr_engine *e = r.e;
+    if (!e->dest_during) return GR_OK;
+    const int32_t done = r.R->rec_before[(size_t)r.executed];
+    if ((int64_t)(done - e->streamed) * e->dim * (int64_t)sizeof(float) < kStreamRowBytes) return GR_OK;
+    return stream_records(r, done);
+}
+
 // Record counts after `executed` steps, including the SaveInterval == 0 final record.
 struct RecordCounts {
     int64_t rec = 1, crec = 0, irec = 0;
@@ -1437,7 +1560,7 @@ int run_tail(RunCtx &r, RecordCounts &c) {
         }
         const StateView Rv = view_of(e->ret, e->n);
         fill_forward_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, Rv, e->d_counts.p + 2, e->crec_of_rec.p,
-                                                                     (int32_t)c.rec);
+                                                                     e->streamed, (int32_t)c.rec);
         finalize_retired_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(Rv, e->d_counts.p + 2, s.abort_mode != 0,
                                                                          s.curvature_mode != 0, e->out_status.p,
                                                                          e->out_length.p, e->out_tc.p);
@@ -1517,6 +1640,8 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
     RunCtx r;
     rc = make_ctx(e, R, r);
     if (rc) return rc;
+    rc = stream_begin(e, R);
+    if (rc) return rc;
     CK(cudaEventRecord(run_a, e->cs));
     // the first windows read snapshots already uploaded
     for (int k = 0; k < e->K; ++k)
@@ -1551,6 +1676,8 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
             e->slot_used[k % e->K] = true;
         }
         const bool alive_abort = q == 1;
+        rc = stream_progress(r);
+        if (rc) return rc;
         if (exhausted) break;
         if (e->dyn_any) {
             int res = 0;
@@ -1568,8 +1695,28 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
     RecordCounts c;
     rc = run_tail(r, c);
     if (rc) return rc;
+    if (e->dest_run) {
+        // the rest of the records; the run ends when they are in host memory
+        rc = stream_records(r, (int32_t)c.rec);
+        if (rc) return rc;
+        CK(cudaEventRecord(e->ds_ev, e->ds));
+        CK(cudaStreamWaitEvent(e->cs, e->ds_ev, 0));
+    }
     CK(cudaEventRecord(run_b, e->cs));
     return run_collect(e, R, r.executed, windows_run, c, r.ev_used);
+}
+
+extern "C" int gr_set_result_destinations(gr_engine *e, const gr_result_destinations *dest) {
+    if (!e) return USER_ERR("null engine >");
+    if (!dest) {
+        e->dest = gr_result_destinations{};
+        e->dest_set = false;
+        return GR_OK;
+    }
+    if (dest->records_capacity < 0 || dest->info_capacity < 0) return USER_ERR("negative capacity >");
+    e->dest = *dest;
+    e->dest_set = true;
+    return GR_OK;
 }
 
 // ------------------------------------------------------------------ graph runs (batch.cu)

@@ -459,6 +459,9 @@ class TrajectoryIntegrator {
         return settings_.PinnedResults ? pinned_empty(shape) : py::array_t<float>(shape);
     }
 
+    // Results are fetched after the run.  Streaming them out during the run
+    // (gr_set_result_destinations) does not pay here: the run is bound by the snapshot uploads
+    // over the same link, and both directions together moved less than one after the other.
     std::unique_ptr<TrajectorySet> collect(bool comp) {
         gr_result_info info;
         check(gr_result_info_get(engine_, &info));

@@ -127,9 +127,10 @@ def _problem(n=3000, n_snap=6, seed=0):
     return settings, W.SnapshotSource(wind, volumes=vols, constants=cons, uplift=lift), seeds
 
 
-def _run(settings, loader, seeds, pinned_results):
+def _run(settings, loader, seeds, pinned_results, sort_interval=0):
     s = W.apply_settings(pg.IntegratorSettings(), settings, H.enums(pg))
     s.PinnedResults = pinned_results
+    s.SortInterval = sort_interval
     res = pg.TrajectoryIntegrator(s, loader, pg.TrajectorySet(seeds)).compute()
     return dict(trajectories=res.trajectories(), status=np.array([int(a) for a in res.abortReasons()], np.int32),
                 total_curvature=res.totalCurvatures(), curvatures=res.curvatures(),
@@ -146,6 +147,8 @@ def test_pinned_loads_and_results_match_the_oracle():
         "staged": _run(settings, W.make_loader(pg.DataLoader, src), seeds, False),
         "pinned source": _run(settings, W.make_loader(pg.DataLoader, _pinned_source(src)), seeds, True),
         "one reused buffer": _run(settings, _OneBufferLoader(src), seeds, True),
+        # results streamed while particles retire and the live set is re-sorted
+        "pinned, compacting": _run(settings, W.make_loader(pg.DataLoader, _pinned_source(src)), seeds, True, 1),
     }
     for name, eng in runs.items():
         H.assert_same(eng, ref, ("trajectories", "status", "total_curvature", "curvatures"))
@@ -177,3 +180,96 @@ def test_pinned_fetch_matches_staged_fetch_for_large_and_pitched_results():
     assert np.array_equal(staged["volume_info"][0], pinned["volume_info"][0])
     assert np.array_equal(staged["compute_info"][0], pinned["compute_info"][0])
     eng.close()
+
+
+def _stream_case(settings, src, seeds, **cs_extra):
+    """One capi run with result streaming into page-locked arrays sized by the plan; returns the
+    streamed arrays, the fetched results and the result info."""
+    cs = capi.settings_from_reference(settings, **cs_extra)
+    plan, _ = capi.plan(cs, with_steps=False)
+    eng = capi.Engine(cs)
+    n, dim = seeds.shape
+    pos = capi.pinned_empty((n, plan.records, dim))
+    nvol = len(src.volumes[0]) if settings.get("AdditionalVolumeMode", 0) else 0
+    nexpr = len(settings.get("AdditionalCompute", []))
+    vols = [capi.pinned_empty((n, plan.info_records)) for _ in range(nvol)]
+    cmps = [capi.pinned_empty((n, plan.info_records)) for _ in range(nexpr)]
+    eng.stream_results(pos, vols, cmps)
+    eng.set_seeds(seeds)
+    for k in (0, 1):
+        eng.load_windfield(k, src.wind[k])
+    names = list(src.volumes[0].keys()) if nvol else []
+    for j, name in enumerate(names):
+        eng.load_volume(0, j, src.volumes[0][name])
+    for e, code in enumerate(settings.get("AdditionalCompute", [])):
+        eng.compile_expression(e, code, names, [])
+    eng.run(lambda k: (eng.load_windfield(k, src.wind[k]), 1)[1] if k < len(src.wind) else 0)
+    ref = eng.results()
+    return eng, dict(pos=pos, vols=vols, cmps=cmps), ref, plan
+
+
+def _check_streamed(got, ref):
+    info = ref["info"]
+    R, I = info.records, info.info_records
+    assert np.array_equal(got["pos"][:, :R], ref["trajectories"])
+    for a, b in zip(got["vols"], ref["volume_info"]):
+        assert np.array_equal(a[:, :I], b)
+    for a, b in zip(got["cmps"], ref["compute_info"]):
+        assert np.array_equal(a[:, :I], b)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["3d-compacting", "3d-loader-runs-dry", "3d-minimum-alive", "3d-save0", "2d"])
+def test_streamed_records_equal_fetched_records(case):
+    if case == "2d":
+        settings, src, seeds = W.config1(n_particles=20_000, n_snapshots=16)
+        settings = dict(settings, MaximumSimulationTime=3.0)
+    else:
+        n_snap = 31 if case == "3d-loader-runs-dry" else 61
+        settings, src, seeds = W.config2(n_particles=50_000, n_snapshots=n_snap, grid=(16, 24, 24), steps=600)
+        settings = dict(settings, SaveInterval=3)
+        if case == "3d-minimum-alive":
+            settings["MinimumAliveParticles"] = 49_000
+        if case == "3d-save0":
+            settings["SaveInterval"] = 0
+    # compaction and re-sort after every launch, 5 steps per launch: retired particles are
+    # filled in before each streamed chunk
+    eng, got, ref, plan = _stream_case(settings, src, seeds, sort_interval=1, steps_per_launch=5)
+    info = ref["info"]
+    if case == "3d-loader-runs-dry":
+        assert info.records < plan.records
+    if case == "3d-minimum-alive":
+        assert info.steps < plan.steps
+    if case.startswith("3d") and case != "3d-minimum-alive":
+        assert (ref["status"] != 0).mean() > 0.05, "few particles retired: compaction untested"
+    _check_streamed(got, ref)
+    # a second run of the same engine streams again into the same arrays
+    for a in [got["pos"]] + got["vols"] + got["cmps"]:
+        a.fill(np.nan)
+    for k in (0, 1):
+        eng.load_windfield(k, src.wind[k])
+    eng.run(lambda k: (eng.load_windfield(k, src.wind[k]), 1)[1] if k < len(src.wind) else 0)
+    _check_streamed(got, eng.results())
+    eng.close()
+
+
+@pytest.mark.gpu
+def test_stream_destinations_are_checked_at_run():
+    settings, src, seeds = W.config2(n_particles=1000, n_snapshots=11, grid=(16, 24, 24), steps=100)
+    cs = capi.settings_from_reference(settings)
+    plan, _ = capi.plan(cs, with_steps=False)
+    for pos, msg in ((capi.pinned_empty((1000, plan.records - 1, 3)), "records per particle"),
+                     (np.empty((1000, plan.records, 3), np.float32), "page-locked")):
+        eng = capi.Engine(cs)
+        eng.stream_results(pos)
+        eng.set_seeds(seeds)
+        for k in (0, 1):
+            eng.load_windfield(k, src.wind[k])
+        eng.load_volume(0, 0, src.volumes[0]["T"])
+        eng.compile_expression(0, settings["AdditionalCompute"][0], ["T"], [])
+        with pytest.raises(capi.GraniteError, match=msg):
+            eng.run(lambda k: (eng.load_windfield(k, src.wind[k]), 1)[1] if k < len(src.wind) else 0)
+        eng.stream_results()   # off: the same engine runs
+        eng.run(lambda k: (eng.load_windfield(k, src.wind[k]), 1)[1] if k < len(src.wind) else 0)
+        assert eng.info().records == plan.records
+        eng.close()
