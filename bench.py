@@ -20,6 +20,7 @@ e2e   : the pygranite API, TrajectoryIntegrator(settings, loader, TrajectorySet(
         (float64, OpenMP on all host cores) runs bounded samples of the same workload.
 """
 import argparse
+import gc
 import json
 import os
 import subprocess
@@ -54,7 +55,7 @@ def parse():
     p.add_argument("--sort-interval", type=int, default=4,
                    help="launches between compaction / Morton re-sorts of the live particles (0 = off)")
     p.add_argument("--layout", type=int, default=0, help="0: window-pair wind layout, 1: ring slots")
-    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--e2e-steps", type=int, default=5)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-native", action="store_true", help="skip the native-loader run")
@@ -751,6 +752,7 @@ def main():
             s.PinnedResults = pinned_results
             e_ps, e_s, d2h, reps = 0, 0.0, 0, []
             for k in range(1 + args.e2e_steps):
+                gc.collect()   # the previous step's garbage, outside the timed region
                 torch.cuda.synchronize()
                 if pg_dist:
                     pg_dist.barrier()
