@@ -148,7 +148,12 @@ struct gr_engine {
     std::vector<int64_t> wind_holds, vol_holds, cons_holds, lift_holds;
     std::vector<cudaEvent_t> slot_free, slot_ready;
     std::vector<bool> slot_used;
-    DevBuf<float> raw;                 // device staging of one snapshot's planes
+    // device staging of a snapshot's planes, double-buffered: the upload of snapshot s + 1 (on
+    // the upload stream us) overlaps the pack of snapshot s, which waits for its ring slot
+    DevBuf<float> raw[2];
+    int raw_next = 0;
+    cudaEvent_t raw_free[2] = {nullptr, nullptr};   // the pack that read raw[j] is done
+    cudaStream_t us = nullptr;
     PinnedBuf pin[2];
     int pin_next = 0;
     cudaEvent_t upload_done = nullptr; // end of a DMA straight from a caller's page-locked buffer
@@ -218,6 +223,9 @@ struct gr_engine {
     ~gr_engine() {
         if (cs) cudaStreamSynchronize(cs);
         if (xs) cudaStreamSynchronize(xs);
+        if (us) cudaStreamSynchronize(us);
+        for (auto e : raw_free)
+            if (e) cudaEventDestroy(e);
         for (auto e : slot_free) cudaEventDestroy(e);
         for (auto e : slot_ready) cudaEventDestroy(e);
         for (auto e : ev_pool) cudaEventDestroy(e);
@@ -230,6 +238,7 @@ struct gr_engine {
         if (ds) cudaStreamDestroy(ds);
         if (cs) cudaStreamDestroy(cs);
         if (xs) cudaStreamDestroy(xs);
+        if (us) cudaStreamDestroy(us);
     }
 };
 
@@ -307,7 +316,7 @@ int setup_grid(gr_engine *e, int64_t nz, int64_t ny, int64_t nx) {
     const int bytes_node = e->s.storage == GR_STORE_F32 ? (e->dim == 3 ? 16 : 8) : (e->dim == 3 ? 8 : 4);
     e->wind_stride = ((e->nodes * bytes_node + 255) / 256) * 256;
     CK(e->wind.alloc((size_t)e->wind_stride * e->K));
-    CK(e->raw.alloc((size_t)e->nodes * e->dim));
+    for (auto &b : e->raw) CK(b.alloc((size_t)e->nodes * e->dim));
     e->grid_set = true;
     return GR_OK;
 }
@@ -366,32 +375,39 @@ int load_wind(gr_engine *e, int64_t snapshot, const float *const *comps, int32_t
     }
     const int slot = (int)(snapshot % e->K);
     const size_t plane = (size_t)e->nodes;
-    float *raw[3] = {e->raw.p, e->raw.p + plane, e->raw.p + 2 * plane};
-    // The planes go to the device staging `raw` first (free once the previous pack on this
-    // stream has run); only the pack into the ring slot waits for the slot to be released.
+    // Host planes go to a device staging buffer on the upload stream, which waits only for the
+    // pack that last read that buffer (two loads back); the pack into the ring slot, on the
+    // copy stream, waits for the upload and for the slot to be released.
+    const int j = e->raw_next;
+    float *raw[3] = {e->raw[j].p, e->raw[j].p + plane, e->raw[j].p + 2 * plane};
     bool pinned = !device_src;
     for (int c = 0; c < ncomp && pinned; ++c) pinned = pinned_range(comps[c], plane * sizeof(float));
     if (device_src) {
         for (int c = 0; c < ncomp; ++c) raw[c] = const_cast<float *>(comps[c]);
-    } else if (pinned) {
-        for (int c = 0; c < ncomp; ++c)
-            CK(cudaMemcpyAsync(raw[c], comps[c], plane * sizeof(float), cudaMemcpyHostToDevice, e->xs));
-        CK(cudaEventRecord(e->upload_done, e->xs));
-        e->stats.h2d_bytes += (int64_t)(plane * ncomp * sizeof(float));
     } else {
-        PinnedBuf *pb = nullptr;
-        rc = ensure_pinned(e, plane * ncomp * sizeof(float), pb);
-        if (rc) return rc;
-        for (int c = 0; c < ncomp; ++c)
-            parallel_memcpy(static_cast<float *>(pb->p) + c * plane, comps[c], plane * sizeof(float));
-        CK(cudaMemcpyAsync(e->raw.p, pb->p, plane * ncomp * sizeof(float), cudaMemcpyHostToDevice, e->xs));
-        CK(cudaEventRecord(pb->done, e->xs));
+        e->raw_next ^= 1;
+        CK(cudaStreamWaitEvent(e->us, e->raw_free[j], 0));
+        if (pinned) {
+            for (int c = 0; c < ncomp; ++c)
+                CK(cudaMemcpyAsync(raw[c], comps[c], plane * sizeof(float), cudaMemcpyHostToDevice, e->us));
+        } else {
+            PinnedBuf *pb = nullptr;
+            rc = ensure_pinned(e, plane * ncomp * sizeof(float), pb);
+            if (rc) return rc;
+            for (int c = 0; c < ncomp; ++c)
+                parallel_memcpy(static_cast<float *>(pb->p) + c * plane, comps[c], plane * sizeof(float));
+            CK(cudaMemcpyAsync(raw[0], pb->p, plane * ncomp * sizeof(float), cudaMemcpyHostToDevice, e->us));
+            CK(cudaEventRecord(pb->done, e->us));
+        }
+        CK(cudaEventRecord(e->upload_done, e->us));
+        CK(cudaStreamWaitEvent(e->xs, e->upload_done, 0));
         e->stats.h2d_bytes += (int64_t)(plane * ncomp * sizeof(float));
     }
     rc = wait_slot_free(e, slot);
     if (rc) return rc;
     rc = pack_launch(e, raw[0], raw[1], e->dim == 3 ? raw[2] : raw[1], slot);
     if (rc) return rc;
+    if (!device_src) CK(cudaEventRecord(e->raw_free[j], e->xs));
     CK(cudaEventRecord(e->slot_ready[slot], e->xs));
     if (device_src) CK(cudaStreamSynchronize(e->xs));
     if (pinned) CK(cudaEventSynchronize(e->upload_done));   // the caller may release its planes
@@ -458,6 +474,8 @@ int gr_create(const gr_settings *settings, gr_engine **out) {
         CK(cudaEventCreateWithFlags(&e->slot_ready[k], cudaEventDisableTiming));
     }
     CK(cudaEventCreateWithFlags(&e->upload_done, cudaEventDisableTiming));
+    CK(cudaStreamCreateWithFlags(&e->us, cudaStreamNonBlocking));
+    for (auto &ev : e->raw_free) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     e->wind_holds.assign(e->K, -1);
     e->vol_holds.assign(e->K, -1);
     e->cons_holds.assign(e->K, -1);
