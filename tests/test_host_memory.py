@@ -273,3 +273,39 @@ def test_stream_destinations_are_checked_at_run():
         eng.run(lambda k: (eng.load_windfield(k, src.wind[k]), 1)[1] if k < len(src.wind) else 0)
         assert eng.info().records == plan.records
         eng.close()
+
+
+@pytest.mark.gpu
+def test_loader_callback_overwriting_one_page_locked_buffer():
+    # The loader callback overwrites ONE page-locked buffer with each next snapshot: correct only
+    # if every wind load has finished reading the buffer before the loader runs again.
+    settings, src, seeds = W.config2(n_particles=20_000, n_snapshots=21, grid=(16, 24, 24), steps=200)
+
+    def run(one_buffer):
+        eng = capi.Engine(capi.settings_from_reference(settings, sort_interval=2))
+        eng.set_seeds(seeds)
+        for k in (0, 1):
+            eng.load_windfield(k, src.wind[k])
+        eng.load_volume(0, 0, src.volumes[0]["T"])
+        eng.compile_expression(0, settings["AdditionalCompute"][0], ["T"], [])
+        buf = capi.pinned_empty((3,) + src.wind[0][0].shape)
+
+        def cb(k):
+            if k >= len(src.wind):
+                return 0
+            if not one_buffer:
+                eng.load_windfield(k, src.wind[k])
+                return 1
+            for c in range(3):
+                buf[c] = src.wind[k][c]
+            eng.load_windfield(k, [buf[0], buf[1], buf[2]])
+            return 1
+        eng.run(cb)
+        out = eng.results()
+        eng.close()
+        return out
+
+    a, b = run(False), run(True)
+    for key in ("trajectories", "status", "total_curvature"):
+        assert np.array_equal(a[key], b[key]), key
+    assert np.array_equal(a["compute_info"][0], b["compute_info"][0])
