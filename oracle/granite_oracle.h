@@ -69,6 +69,8 @@ typedef struct {
     const float *seeds;            /* n*dim */
     int32_t threads;               /* OpenMP threads, 0 = runtime default */
     int64_t step_limit;            /* >= 0: stop after this many steps (bounded timing sample) */
+    int32_t filter_weights;        /* 0: exact filter fractions; 1 / 2: fractions rounded / truncated
+                                      to 1/256 like texture hardware (reference GPU comparisons) */
 } or_input;
 
 typedef struct {

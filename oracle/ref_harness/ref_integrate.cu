@@ -36,11 +36,16 @@ using my::math::Vec3;
 #define REF_ARGS_3P Vec3, Space::Space3D, Integrator::ClassicRungeKutta, BorderMode::Block, CurvatureMode::Off, \
     AbortMode::Time, UpLiftMode::Off, WindfieldMode::Dynamic, ConstantsMode::Off, AdditionalVolumeMode::Off,   \
     false, false, false, false, false
+// 3D Euler plain (one step of it samples the texture filter directly)
+#define REF_ARGS_3E Vec3, Space::Space3D, Integrator::ExplicitEuler, BorderMode::Block, CurvatureMode::Off,    \
+    AbortMode::Time, UpLiftMode::Off, WindfieldMode::Dynamic, ConstantsMode::Off, AdditionalVolumeMode::Off,   \
+    false, false, false, false, false
 
 extern "C" {
 
 typedef struct {
-    int32_t variant;          // 0: 2D Euler plain, 1: 3D RK4 curvature+volume+expression, 2: 3D RK4 plain
+    int32_t variant;          // 0: 2D Euler plain, 1: 3D RK4 curvature+volume+expression, 2: 3D RK4 plain,
+                              // 3: 3D Euler plain
     int32_t blocks_fixed;     // 0: launch shape as shipped; 1: BLOCKS = ceil(N / THREADS)
     float delta_t, data_time_distance, maximum_simulation_time;
     int64_t save_interval;
@@ -156,6 +161,7 @@ void launch<Vec2>(int, int blocks, int threads, const SimulationData<Vec2> &d) {
 template <>
 void launch<Vec3>(int variant, int blocks, int threads, const SimulationData<Vec3> &d) {
     if (variant == 1) integrate<REF_ARGS_3D><<<blocks, threads>>>(d);
+    else if (variant == 3) integrate<REF_ARGS_3E><<<blocks, threads>>>(d);
     else integrate<REF_ARGS_3P><<<blocks, threads>>>(d);
 }
 

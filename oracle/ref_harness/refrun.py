@@ -49,7 +49,7 @@ def available() -> bool:
 def run(settings: dict, wind, seeds, volume=None, blocks_fixed=False, step_limit=-1):
     """settings: reference IntegratorSettings fields (as in oracle.oracle.settings).  The
     variant is chosen from them: 2D Euler plain, 3D RK4 + TotalCurvature + one constant
-    volume + one expression, or 3D RK4 plain."""
+    volume + one expression, 3D RK4 plain, or 3D Euler plain."""
     lib = ctypes.CDLL(LIB_PATH)
     lib.ref_run.argtypes = [ctypes.POINTER(RefArgs)]
     lib.ref_run.restype = ctypes.c_int
@@ -59,6 +59,8 @@ def run(settings: dict, wind, seeds, volume=None, blocks_fixed=False, step_limit
         a.variant = 0
     elif settings.get("AdditionalCompute"):
         a.variant = 1
+    elif settings.get("Integrator", 1) == 0:
+        a.variant = 3
     else:
         a.variant = 2
     a.blocks_fixed = int(blocks_fixed)

@@ -9,6 +9,10 @@ counts, windows and record counts are matched exactly, except the border-creep s
 3D border addressing a particle creeping toward an upper face stalls (Wind) at a step that
 depends on the interpolation's rounding; those particles (within one cell of an upper face)
 are excluded.
+
+filter_reference.npz pins the texture filter itself: the oracle with weights rounded to the
+nearest 1/256 (filter_weights=1) reproduces the reference bit for bit in 2D and within one
+1/256 weight step in 3D.
 """
 import json
 import os
@@ -92,3 +96,51 @@ def test_engine_matches_reference_kernel():
     check_gyre(H.run_engine(s, src.wind, seeds), load("gyre_reference.npz"))
     s, src, seeds = MG.fourier_case()
     check_fourier(H.run_engine(s, src.wind, seeds, volumes=src.volumes), load("fourier_reference.npz"))
+
+
+# ------------------------------------------------------------ the texture filter itself
+# filter_reference.npz: one Euler step of the reference kernel through a field equal to its own
+# grid coordinates (make_golden.filter_case), so each new position encodes the weight the
+# texture unit used.  The oracle's filter_weights=1 mode (fractions rounded to the nearest
+# 1/256) is the model checked here.
+
+def _filter_run(dim, filter_weights):
+    s, src, seeds = MG.filter_case(dim)
+    return orc.run(orc.settings(**s), orc.Inputs(wind=src.wind, seeds=seeds), "f32",
+                   filter_weights=filter_weights)
+
+
+def test_texture_filter_2d_is_nearest_256th():
+    g = load("filter_reference.npz")
+    r = _filter_run(2, 1)
+    assert np.array_equal(r["status"], g["status2d"])
+    assert np.array_equal(r["trajectories"][:, 1], g["positions2d"])        # every particle, bit for bit
+    exact = _filter_run(2, 0)
+    assert not np.array_equal(exact["trajectories"][:, 1], g["positions2d"])
+
+
+def test_texture_filter_3d_within_one_256th():
+    # 3D (cudaArray, border addressing): the z weights are the nearest 1/256 for every sample;
+    # x and y weights differ from it by one 1/256 step for some samples (about 2% on the
+    # 16-node x axis, a third on the 12-node y axis), never by more.
+    g = load("filter_reference.npz")
+    r = _filter_run(3, 1)
+    assert np.array_equal(r["status"], g["status3d"])
+    got, ref = r["trajectories"][:, 1], g["positions3d"]
+    same = (got == ref).mean(0)
+    assert same[2] == 1.0 and same[0] > 0.95 and same[1] > 0.6, same
+    step = np.abs(got.astype(np.float64) - ref) * 16 * 256     # h = 1/16: weight difference in 1/256
+    assert step.max() <= 1.0 + 1e-6, step.max()
+
+
+def test_texture_weight_mode_tracks_the_gyre_fixture():
+    # with 1/256 weights the float32 oracle reproduces most of the reference's 2D run bit for bit
+    s, src, seeds = MG.gyre_case()
+    g = load("gyre_reference.npz")
+    tex = orc.run(orc.settings(**s), orc.Inputs(wind=src.wind, seeds=seeds), "f32", filter_weights=1)
+    ideal = orc.run(orc.settings(**s), orc.Inputs(wind=src.wind, seeds=seeds), "f32")
+    same = lambda r: np.all(r["trajectories"][:, 1] == g["trajectories"][:, 1], axis=1).mean()  # noqa: E731
+    assert same(tex) > 0.85 and same(ideal) < 0.2, (same(tex), same(ideal))
+    e_tex = cells(tex["trajectories"], g["trajectories"], [2 / 256, 1 / 128])
+    e_ideal = cells(ideal["trajectories"], g["trajectories"], [2 / 256, 1 / 128])
+    assert np.median(e_tex[:, 10]) < np.median(e_ideal[:, 10]) / 5
