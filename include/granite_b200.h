@@ -79,6 +79,11 @@ typedef struct gr_settings {
     int32_t grid_waves;            /* graph runs: resident waves of step-kernel blocks in the
                                       persistent grid (each thread walks live particles with a
                                       grid stride); 0 = 1 */
+    int32_t filter_weights;        /* 0: exact interpolation weights (float32 software filter);
+                                      1: fractions rounded to the nearest 1/256, the 8-bit weights
+                                      of the texture unit the reference filters with
+                                      (TrajectoryIntegrator.icc:22-50; cpp:444-583), which
+                                      reproduces its 2D results bit for bit */
 } gr_settings;
 
 /* Fills *s with the reference's IntegratorSettings defaults (IntegratorSettings.hpp:89-181). */

@@ -50,6 +50,7 @@ class Settings(ctypes.Structure):
         ("time_mode", ctypes.c_int32), ("compensated", ctypes.c_int32), ("ring_slots", ctypes.c_int32),
         ("steps_per_launch", ctypes.c_int32), ("sort_interval", ctypes.c_int32), ("block_size", ctypes.c_int32),
         ("device", ctypes.c_int32), ("layout", ctypes.c_int32), ("grid_waves", ctypes.c_int32),
+        ("filter_weights", ctypes.c_int32),
     ]
 
 

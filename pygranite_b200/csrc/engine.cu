@@ -455,6 +455,7 @@ int gr_create(const gr_settings *settings, gr_engine **out) {
     if (s.maximum_simulation_time / s.delta_t > 5.0e8f) return USER_ERR("Too many integration steps requested. >");
     if (s.save_interval < 0) return USER_ERR("SaveInterval must not be negative. >");
     if (s.storage < 0 || s.storage > 2) return USER_ERR("Invalid storage type. >");
+    if (s.filter_weights < 0 || s.filter_weights > 1) return USER_ERR("Invalid filter weights. >");
     auto e = std::make_unique<gr_engine>();
     e->s = s;
     e->dim = s.space == 0 ? 3 : 2;
@@ -723,6 +724,7 @@ int gr_update_settings(gr_engine *e, const gr_settings *s) {
     if (!std::isfinite(s->maximum_simulation_time)) return USER_ERR("MaximumSimulationTime must be finite. >");
     if (s->maximum_simulation_time / s->delta_t > 5.0e8f) return USER_ERR("Too many integration steps requested. >");
     if (s->save_interval < 0) return USER_ERR("SaveInterval must not be negative. >");
+    if (s->filter_weights < 0 || s->filter_weights > 1) return USER_ERR("Invalid filter weights. >");
     ++e->gen;
     const int32_t uplift = e->s.uplift_mode;
     e->s = *s;
@@ -1115,6 +1117,7 @@ KParams make_params(gr_engine *e) {
     P.sphere = e->dim == 2 && s.sphere_radius > 0.f;
     P.topography = e->has_topo ? 1 : 0;
     P.compensated = s.compensated ? 1 : 0;
+    P.filter_weights = s.filter_weights ? 1 : 0;
     P.nvol = P.volume_mode ? e->nvol : 0;
     P.ncon = P.constants_mode ? e->ncon : 0;
     P.nexpr = e->nexpr;

@@ -84,6 +84,7 @@ struct KParams {
     int32_t wind_dynamic, dyn_any, border_mode, curvature_mode, abort_mode, uplift_mode;
     int32_t constants_mode, volume_mode, reverse, sphere, topography, compensated;
     int32_t nvol, ncon, nexpr;
+    int32_t filter_weights;       // 1: interpolation fractions rounded to the nearest 1/256
     const Program *prog;          // [4]
     unsigned long long *counters; // [0] particle-steps, [1] alive at the end of the launch
     unsigned *alive_at;           // if set: [step - s0][32 shards] particles alive after each step
@@ -96,11 +97,14 @@ __device__ __forceinline__ float lerp_(float a, float b, float t) { return __fma
 // Texture coordinate -> cell index and fraction.  Coordinates are clamped to [-2, n+1]
 // first; every corner outside the grid is border (3D) or clamped (2D), so the clamp never
 // changes a value and keeps the integer conversion in range.
-__device__ __forceinline__ void cell(float a, int n, int &i, float &f) {
+// fw = 1 rounds the fraction to the nearest 1/256, the 8-bit weights of the texture unit the
+// reference filters with (CUDA Programming Guide, linear filtering); 0 keeps it exact.
+__device__ __forceinline__ void cell(float a, int n, int fw, int &i, float &f) {
     a = fminf(fmaxf(a, -2.0f), (float)(n + 1));
     const float fl = floorf(a);
     i = (int)fl;
     f = a - fl;
+    if (fw) f = floorf(f * 256.0f + 0.5f) * (1.0f / 256.0f);
 }
 
 template <typename W> struct Store;
@@ -205,9 +209,9 @@ struct Cell3 {
 __device__ __forceinline__ Cell3 make_cell3(const KParams &P, float ax, float ay, float az) {
     int ix, iy, iz;
     Cell3 c;
-    cell(ax, P.nx, ix, c.fx);
-    cell(ay, P.ny, iy, c.fy);
-    cell(az, P.nz, iz, c.fz);
+    cell(ax, P.nx, P.filter_weights, ix, c.fx);
+    cell(ay, P.ny, P.filter_weights, iy, c.fy);
+    cell(az, P.nz, P.filter_weights, iz, c.fz);
     const bool x0 = (unsigned)ix < (unsigned)P.nx, x1 = (unsigned)(ix + 1) < (unsigned)P.nx;
     const bool y0 = (unsigned)iy < (unsigned)P.ny, y1 = (unsigned)(iy + 1) < (unsigned)P.ny;
     const bool z0 = (unsigned)iz < (unsigned)P.nz, z1 = (unsigned)(iz + 1) < (unsigned)P.nz;
@@ -289,11 +293,11 @@ struct Cell2 {
     float fx, fy;
 };
 
-__device__ __forceinline__ Cell2 make_cell2(int nx, int ny, float ax, float ay) {
+__device__ __forceinline__ Cell2 make_cell2(int nx, int ny, int fw, float ax, float ay) {
     int ix, iy;
     Cell2 c;
-    cell(ax, nx, ix, c.fx);
-    cell(ay, ny, iy, c.fy);
+    cell(ax, nx, fw, ix, c.fx);
+    cell(ay, ny, fw, iy, c.fy);
     const int x0 = min(max(ix, 0), nx - 1), x1 = min(max(ix + 1, 0), nx - 1);
     const int y0 = min(max(iy, 0), ny - 1), y1 = min(max(iy + 1, 0), ny - 1);
     c.i00 = y0 * nx + x0;
@@ -359,7 +363,7 @@ __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, co
             tri3p<W>(wb, c, b, f);
             r.x = lerp_(b[0], f[0], t); r.y = lerp_(b[1], f[1], t); r.z = lerp_(b[2], f[2], t);
         } else {
-            const Cell2 c = make_cell2(P.nx, P.ny, ax, ay);
+            const Cell2 c = make_cell2(P.nx, P.ny, P.filter_weights, ax, ay);
             float b[2], f[2];
             bil2p<W>(wb, c, b, f);
             r.x = lerp_(b[0], f[0], t); r.y = lerp_(b[1], f[1], t);
@@ -379,7 +383,7 @@ __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, co
             r.x = bu; r.y = bv; r.z = bw;
         }
     } else {
-        const Cell2 c = make_cell2(P.nx, P.ny, ax, ay);
+        const Cell2 c = make_cell2(P.nx, P.ny, P.filter_weights, ax, ay);
         float bu, bv;
         bil2<W>(wb, c, bu, bv);
         if (P.wind_dynamic) {
@@ -481,7 +485,7 @@ __device__ __forceinline__ void eval_extras(const KParams &P, const StepEntry &E
                 }
             }
         } else {
-            const Cell2 c = make_cell2(P.nx, P.ny, ax, ay);
+            const Cell2 c = make_cell2(P.nx, P.ny, P.filter_weights, ax, ay);
 #pragma unroll
             for (int k = 0; k < GR_MAX_VOL; ++k) {
                 if (k < P.nvol) {
@@ -668,7 +672,7 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
                 if (bm == 0) {
                     bool topo = false;
                     if (DIM == 3 && P.topography) {
-                        const Cell2 c = make_cell2(P.nx, P.ny, np.x / P.scale[0], np.y / P.scale[1]);
+                        const Cell2 c = make_cell2(P.nx, P.ny, P.filter_weights, np.x / P.scale[0], np.y / P.scale[1]);
                         topo = bil1(P.topo, c) > np.z;
                     }
                     if (topo) abort = 3;

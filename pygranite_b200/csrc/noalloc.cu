@@ -237,6 +237,7 @@ extern "C" int gr_advance_noalloc(const gr_settings *s, int64_t nz, int64_t ny, 
     P.hh = 0.5f * h;
     P.sixth = 1.0f / 6;
     P.sphere_radius = s->sphere_radius;
+    P.filter_weights = s->filter_weights ? 1 : 0;
     P.wind_dynamic = 1;
     P.dyn_any = 1;
     P.border_mode = dim == 2 ? s->border_mode : 0;

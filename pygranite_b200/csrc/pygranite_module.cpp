@@ -79,6 +79,7 @@ struct IntegratorSettings {
     int32_t Device{0};
     int32_t WindLayout{0};
     bool PinnedResults{false};
+    bool ReferenceFilter{false};
 };
 
 // float32 array of `shape` in page-locked host memory (gr_host_alloc); the block returns to the
@@ -332,6 +333,7 @@ class TrajectoryIntegrator {
         s.block_size = S.BlockSize;
         s.device = S.Device;
         s.layout = S.WindLayout;
+        s.filter_weights = S.ReferenceFilter ? 1 : 0;
         check(gr_create(&s, &engine_));
         check(gr_set_seeds(engine_, seeds_.data(), static_cast<int64_t>(n_), dim_));
     }
@@ -602,7 +604,8 @@ PYBIND11_MODULE(_pygranite, m) {
         .def_readwrite("BlockSize", &IntegratorSettings::BlockSize)
         .def_readwrite("Device", &IntegratorSettings::Device)
         .def_readwrite("WindLayout", &IntegratorSettings::WindLayout)
-        .def_readwrite("PinnedResults", &IntegratorSettings::PinnedResults);
+        .def_readwrite("PinnedResults", &IntegratorSettings::PinnedResults)
+        .def_readwrite("ReferenceFilter", &IntegratorSettings::ReferenceFilter);
 
     m.def("pinned_empty", &pinned_empty, py::arg("shape"),
           "Uninitialised float32 array in page-locked host memory (engine extension).  Loader data "

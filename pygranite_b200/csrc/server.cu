@@ -402,6 +402,7 @@ KParams pool_params(gr_server *S, Pool &P) {
     K.border_mode = S->dim == 2 ? s.border_mode : 0;
     K.reverse = s.reverse ? 1 : 0;
     K.sphere = S->dim == 2 && s.sphere_radius > 0.f;
+    K.filter_weights = s.filter_weights ? 1 : 0;
     K.counters = S->counters.p;
     return K;
 }

@@ -30,7 +30,8 @@ def c_settings(s, **extra) -> capi.Settings:
     opts = dict(storage=int(s.WindStorage), time_mode=1 if s.Float64Time else 0,
                 compensated=1 if s.CompensatedPositions else 0, ring_slots=int(s.RingSlots),
                 steps_per_launch=int(s.StepsPerLaunch), sort_interval=int(s.SortInterval),
-                block_size=int(s.BlockSize), device=int(s.Device), layout=int(s.WindLayout))
+                block_size=int(s.BlockSize), device=int(s.Device), layout=int(s.WindLayout),
+                filter_weights=1 if s.ReferenceFilter else 0)
     opts.update(extra)
     return capi.settings_from_reference(d, **opts)
 

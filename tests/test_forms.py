@@ -18,7 +18,9 @@ def test_settings_conversion_keeps_every_field():
     s.GridScale, s.Offset = [2.0, 3.0], [-1.0, 5.0]
     s.CurvatureMode, s.MinimumAliveParticles, s.Reverse = pg.CurvatureMode.FastTotalCurvature, 17, True
     s.WindStorage, s.Float64Time, s.SortInterval, s.WindLayout = pg.WindStorage.Float16, True, 2, 1
+    s.ReferenceFilter = True
     c = forms.c_settings(s)
+    assert c.filter_weights == 1
     assert (c.space, c.integrator, c.border_mode, c.curvature_mode) == (1, 0, 3, 2)
     assert (c.delta_t, c.data_time_distance, c.maximum_simulation_time, c.save_interval) == (0.5, 4.0, 16.0, 3)
     assert list(c.grid_scale)[:2] == [2.0, 3.0] and c.grid_scale_len == 2 and list(c.offset)[:2] == [-1.0, 5.0]

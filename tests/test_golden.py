@@ -144,3 +144,32 @@ def test_texture_weight_mode_tracks_the_gyre_fixture():
     e_tex = cells(tex["trajectories"], g["trajectories"], [2 / 256, 1 / 128])
     e_ideal = cells(ideal["trajectories"], g["trajectories"], [2 / 256, 1 / 128])
     assert np.median(e_tex[:, 10]) < np.median(e_ideal[:, 10]) / 5
+
+
+@pytest.mark.gpu
+def test_engine_reference_filter_matches_the_reference_kernel():
+    # IntegratorSettings.ReferenceFilter: the engine rounds its interpolation weights like the
+    # reference's texture unit (nearest 1/256).  It equals the oracle's texture mode bit for bit,
+    # hence the reference's own 2D outputs bit for bit.
+    from tests import harness as H
+    g = load("filter_reference.npz")
+    for dim in (2, 3):
+        s, src, seeds = MG.filter_case(dim)
+        eng = H.run_engine(s, src.wind, seeds, ReferenceFilter=True)
+        ora = orc.run(orc.settings(**s), orc.Inputs(wind=src.wind, seeds=seeds), "f32", filter_weights=1)
+        assert np.array_equal(eng["trajectories"], ora["trajectories"]), dim
+        assert np.array_equal(eng["status"], ora["status"]), dim
+    s, src, seeds = MG.filter_case(2)
+    assert np.array_equal(H.run_engine(s, src.wind, seeds, ReferenceFilter=True)["trajectories"][:, 1],
+                          g["positions2d"])
+    s, src, seeds = MG.gyre_case()
+    gy = load("gyre_reference.npz")
+    eng = H.run_engine(s, src.wind, seeds, ReferenceFilter=True)
+    assert np.all(eng["trajectories"][:, 1] == gy["trajectories"][:, 1], axis=1).mean() > 0.85
+    s, src, seeds = MG.fourier_case()
+    eng = H.run_engine(s, src.wind, seeds, volumes=src.volumes, ReferenceFilter=True)
+    ora = orc.run(orc.settings(**s), orc.Inputs(wind=src.wind, seeds=seeds, volumes=src.volumes), "f32",
+                  filter_weights=1)
+    H.assert_same(eng, ora, ("trajectories", "status", "total_curvature"))
+    assert np.array_equal(eng["volume_info"]["T"], ora["volume_info"]["T"])
+    assert np.array_equal(eng["compute_info"][0], ora["compute_info"][0])
