@@ -3,6 +3,7 @@
 gr_plan restates the reference's host loop (TrajectoryIntegrator.tpp:778-995); its per-step
 windows, record flags and float32 time weights must equal the oracle's schedule exactly.
 """
+import ctypes
 import os
 import re
 import subprocess
@@ -52,6 +53,13 @@ def test_invalid_settings_are_rejected_without_gpu():
     for bad in (dict(delta_t=0.0), dict(data_time_distance=-1.0), dict(maximum_simulation_time=1e12, delta_t=1e-3)):
         with pytest.raises(capi.GraniteError, match="ERROR < USER INPUT"):
             capi.plan(capi.default_settings(**bad))
+    # engine options are checked before any CUDA call
+    L = capi.lib()
+    for bad, msg in ((dict(storage=3), b"storage"), (dict(filter_weights=2), b"filter weights"),
+                     (dict(filter_weights=-1), b"filter weights")):
+        h = ctypes.c_void_p()
+        assert L.gr_create(ctypes.byref(capi.default_settings(**bad)), ctypes.byref(h)) == -1
+        assert msg in L.gr_last_error() and not h.value
 
 
 PLANS = [
