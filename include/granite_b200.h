@@ -235,8 +235,8 @@ int gr_set_result_destinations(gr_engine *engine, const gr_result_destinations *
  * cudaHostRegister) is one DMA with no staging copy; a load from such memory returns once the
  * DMA has read it.  Other buffers go through the engine's pinned staging and a parallel host
  * copy.
- * gr_host_alloc rounds up to 2 MiB and hands out a cached block when one of the size (up to a
- * quarter larger) is free; gr_host_free returns a block to the cache while the cached total
+ * gr_host_alloc serves requests up to 4 KiB from 4 KiB slots of shared 2 MiB slabs; larger ones
+ * round up to 2 MiB and get a cached block when one of the size (up to a quarter larger) is free; gr_host_free returns a block to the cache while the cached total
  * stays within the limit (default: a quarter of physical memory; gr_host_cache_limit), and
  * frees it otherwise.  gr_host_free of a pointer not from gr_host_alloc is GR_ERR_USER.
  * gr_host_is_pinned returns 1 if `p` lies in page-locked memory known to CUDA, else 0. */

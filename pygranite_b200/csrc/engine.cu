@@ -229,8 +229,8 @@ struct gr_engine {
         for (auto e : slot_free) cudaEventDestroy(e);
         for (auto e : slot_ready) cudaEventDestroy(e);
         for (auto e : ev_pool) cudaEventDestroy(e);
-        if (h_counters) cudaFreeHost(h_counters);
-        if (h_live) cudaFreeHost(h_live);
+        if (h_counters) gr_host_free(h_counters);
+        if (h_live) gr_host_free(h_live);
         if (live_ready) cudaEventDestroy(live_ready);
         if (upload_done) cudaEventDestroy(upload_done);
         if (ds) cudaStreamSynchronize(ds);
@@ -254,9 +254,9 @@ int ensure_pinned(gr_engine *e, size_t bytes, PinnedBuf *&out) {
     e->pin_next ^= 1;
     if (b.done) CK(cudaEventSynchronize(b.done));
     if (b.bytes < bytes) {
-        if (b.p) CK(cudaFreeHost(b.p));
+        if (b.p) gr_host_free(b.p);
         b.p = nullptr;
-        CK(cudaMallocHost(&b.p, bytes));
+        if (gr_host_alloc((int64_t)bytes, &b.p) != GR_OK) return GR_ERR_RUNTIME;
         b.bytes = bytes;
     }
     if (!b.done) CK(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
@@ -482,7 +482,9 @@ int gr_create(const gr_settings *settings, gr_engine **out) {
     e->cons_holds.assign(e->K, -1);
     e->lift_holds.assign(e->K, -1);
     CK(e->counters.alloc(4));
-    CK(cudaMallocHost(&e->h_counters, 4 * sizeof(unsigned long long)));
+    // small page-locked words from the host cache: no page-locking per engine
+    if (gr_host_alloc(4 * sizeof(unsigned long long), reinterpret_cast<void **>(&e->h_counters)) != GR_OK)
+        return GR_ERR_RUNTIME;
     *out = e.release();
     return GR_OK;
 }
@@ -784,7 +786,8 @@ int alloc_state(gr_engine *e) {
     rc = alloc_set(e, e->ret, true);
     if (rc) return rc;
     CK(e->c_key.alloc(N));
-    if (!e->h_live) CK(cudaMallocHost(&e->h_live, sizeof(int32_t)));
+    if (!e->h_live && gr_host_alloc(sizeof(int32_t), reinterpret_cast<void **>(&e->h_live)) != GR_OK)
+        return GR_ERR_RUNTIME;
     if (!e->live_ready) CK(cudaEventCreateWithFlags(&e->live_ready, cudaEventDisableTiming));
     if (e->nbins == 0) {
         // Morton-ranked brick table (bricks of bx x by x bz nodes)
@@ -1857,7 +1860,7 @@ static int fetch_rows(gr_engine *e, void *out, int64_t capacity, const void *src
     // while the other fills
     for (auto &b : e->bounce) {
         if (!b.p) {
-            CK(cudaMallocHost(&b.p, kBounce));
+            if (gr_host_alloc((int64_t)kBounce, &b.p) != GR_OK) return GR_ERR_RUNTIME;
             b.bytes = kBounce;
         }
         if (!b.done) CK(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));

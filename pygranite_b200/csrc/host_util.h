@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "copy_pool.h"
+#include "../../include/granite_b200.h"
 
 #include <algorithm>
 #include <atomic>
@@ -52,12 +53,14 @@ struct DevBuf {
     }
 };
 
+// Page-locked staging from the library's host cache (gr_host_alloc): engines created one after
+// another reuse the same blocks instead of page-locking and unlocking memory each time.
 struct PinnedBuf {
     void *p = nullptr;
     size_t bytes = 0;
     cudaEvent_t done = nullptr;
     ~PinnedBuf() {
-        if (p) cudaFreeHost(p);
+        if (p) gr_host_free(p);
         if (done) cudaEventDestroy(done);
     }
 };

@@ -136,10 +136,14 @@ namespace {
 
 constexpr size_t kGranule = size_t(2) << 20;   // sizes round up to 2 MiB
 
+constexpr size_t kSlot = 4096;   // requests up to this size share slabs of one 2 MiB block
+
 struct HostCache {
     std::mutex mu;
     std::multimap<size_t, void *> free_blocks;   // cached blocks by size
     std::unordered_map<void *, size_t> live;      // blocks handed out, with their sizes
+    std::vector<void *> free_slots;               // small requests: 4 KiB slots of slab blocks
+    std::unordered_map<void *, char> live_slots;
     size_t cached = 0, live_bytes = 0, limit = 0;
     int64_t allocations = 0, reuses = 0;
     HostCache() {
@@ -186,8 +190,28 @@ int gr_host_alloc(int64_t bytes, void **out) {
     *out = nullptr;
     if (bytes < 0) return host_fail(GR_ERR_USER, "ERROR < USER INPUT | negative size >");
     if (bytes == 0) return GR_OK;
-    const size_t need = ((size_t)bytes + kGranule - 1) / kGranule * kGranule;
     HostCache &c = cache();
+    if ((size_t)bytes <= kSlot) {
+        // small words (counters, flags) share slabs: one page-locked block serves 512 of them
+        std::lock_guard<std::mutex> g(c.mu);
+        if (c.free_slots.empty()) {
+            void *slab = nullptr;
+            const cudaError_t err = cudaHostAlloc(&slab, kGranule, cudaHostAllocPortable);
+            if (err != cudaSuccess) {
+                cudaGetLastError();
+                return host_fail(GR_ERR_RUNTIME, std::string("ERROR < RUNTIME | CUDA error | ") +
+                                                     cudaGetErrorString(err) + " : page-locked slab >");
+            }
+            ++c.allocations;
+            for (size_t k = kGranule / kSlot; k-- > 0;) c.free_slots.push_back(static_cast<char *>(slab) + k * kSlot);
+        }
+        *out = c.free_slots.back();
+        c.free_slots.pop_back();
+        c.live_slots.emplace(*out, 0);
+        c.live_bytes += kSlot;
+        return GR_OK;
+    }
+    const size_t need = ((size_t)bytes + kGranule - 1) / kGranule * kGranule;
     {
         // smallest cached block that fits, unless it is more than a quarter larger
         std::lock_guard<std::mutex> g(c.mu);
@@ -230,6 +254,13 @@ int gr_host_free(void *p) {
     bool keep = false;
     {
         std::lock_guard<std::mutex> g(c.mu);
+        auto sl = c.live_slots.find(p);
+        if (sl != c.live_slots.end()) {
+            c.live_slots.erase(sl);
+            c.free_slots.push_back(p);
+            c.live_bytes -= kSlot;
+            return GR_OK;
+        }
         auto it = c.live.find(p);
         if (it == c.live.end())
             return host_fail(GR_ERR_USER, "ERROR < USER INPUT | gr_host_free: pointer not from gr_host_alloc >");
