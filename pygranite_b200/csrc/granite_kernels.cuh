@@ -256,6 +256,39 @@ __device__ __forceinline__ float tri_corners(const float (&c)[8], const Cell3 &c
     return lerp_(lerp_(a00, a10, cl.fy), lerp_(a01, a11, cl.fy), cl.fz);
 }
 
+// Raw 16-bit pair nodes of the last sampled cell (3D, 16-bit window-pair layouts): 32 registers.
+struct CornerCacheRaw {
+    int32_t base, sx, sy, sz;
+    unsigned valid;
+    uint4 q[8];
+};
+
+template <typename H>
+__device__ __forceinline__ void tri3p_cached16(const void *pairs, const Cell3 &c, CornerCacheRaw &cc, float (&ob)[3],
+                                               float (&of)[3]) {
+    if (c.base != cc.base || c.sx != cc.sx || c.sy != cc.sy || c.sz != cc.sz || c.valid != cc.valid) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
+            const int32_t idx = c.base + (dx ? c.sx : 0) + (dy ? c.sy : 0) + (dz ? c.sz : 0);
+            cc.q[k] = (c.valid & (1u << k)) ? __ldg(reinterpret_cast<const uint4 *>(pairs) + idx) : make_uint4(0, 0, 0, 0);
+        }
+        cc.base = c.base; cc.sx = c.sx; cc.sy = c.sy; cc.sz = c.sz; cc.valid = c.valid;
+    }
+    float u[8], v[8], w[8], uf[8], vf[8], wf[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const float2 b01 = Store<Pair<H>>::cvt(cc.q[k].x), b2 = Store<Pair<H>>::cvt(cc.q[k].y);
+        const float2 f01 = Store<Pair<H>>::cvt(cc.q[k].z), f2 = Store<Pair<H>>::cvt(cc.q[k].w);
+        u[k] = b01.x; v[k] = b01.y; w[k] = b2.x; uf[k] = f01.x; vf[k] = f01.y; wf[k] = f2.x;
+    }
+    ob[0] = tri_corners(u, c); ob[1] = tri_corners(v, c); ob[2] = tri_corners(w, c);
+    of[0] = tri_corners(uf, c); of[1] = tri_corners(vf, c); of[2] = tri_corners(wf, c);
+}
+
+template <typename W> struct PairElem { using type = void; };
+template <typename H> struct PairElem<Pair<H>> { using type = H; };
+
 // Back and front snapshot at once from a window-pair layout; same arithmetic as tri3 on each.
 template <typename W>
 __device__ __forceinline__ void tri3p(const void *pairs, const Cell3 &c, float (&ob)[3], float (&of)[3]) {
@@ -350,7 +383,8 @@ __device__ __forceinline__ float dot3(const V3 &a, const V3 &b, int dim) {
 
 // Wind at world position p, time weight t: interpolate() of TrajectoryIntegrator.icc:42-110.
 template <int DIM, typename W>
-__device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, const void *wb, const void *wf) {
+__device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, const void *wb, const void *wf,
+                                      CornerCacheRaw &cc) {
     V3 r{0.f, 0.f, 0.f};
     const float ax = (p.x - P.off[0]) * P.inv_scale[0];
     const float ay = (p.y - P.off[1]) * P.inv_scale[1];
@@ -360,7 +394,11 @@ __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, co
             const float az = (p.z - P.off[2]) * P.inv_scale[2];
             const Cell3 c = make_cell3(P, ax, ay, az);
             float b[3], f[3];
-            tri3p<W>(wb, c, b, f);
+            using H = typename PairElem<W>::type;
+            if constexpr (!std::is_same<H, float>::value && !std::is_same<H, void>::value)
+                tri3p_cached16<H>(wb, c, cc, b, f);
+            else
+                tri3p<W>(wb, c, b, f);
             r.x = lerp_(b[0], f[0], t); r.y = lerp_(b[1], f[1], t); r.z = lerp_(b[2], f[2], t);
         } else {
             const Cell2 c = make_cell2(P.nx, P.ny, P.filter_weights, ax, ay);
@@ -396,6 +434,13 @@ __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, co
     }
     return r;
     }
+}
+
+template <int DIM, typename W>
+__device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, const void *wb, const void *wf) {
+    CornerCacheRaw cc;
+    cc.base = -1; cc.sx = cc.sy = cc.sz = 0; cc.valid = 0;
+    return wind_at<DIM, W>(P, p, t, wb, wf, cc);
 }
 
 // sphere_coordinates (TrajectoryIntegrator.tpp:98-104).
@@ -574,6 +619,8 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
     bool dirty = false;   // volumes / expressions not yet evaluated for the last alive step
     const int sph = P.sphere && DIM == 2;
 
+    CornerCacheRaw cc;
+    cc.base = -1; cc.sx = cc.sy = cc.sz = 0; cc.valid = 0;
     for (int s = P.s0; s < P.s1; ++s) {
         const StepEntry E = P.sched[s];
         if (alive && s < life && s >= birth) {
@@ -587,16 +634,16 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
             V3 v, vc;
             if (RK4) {
                 const float t1 = E.t1, t2 = E.t2;
-                const V3 k1c = wind_at<DIM, W>(P, p, t0, wb, wf);
+                const V3 k1c = wind_at<DIM, W>(P, p, t0, wb, wf, cc);
                 const V3 k1 = sph ? sphere_(P, p.y, k1c) : k1c;
                 V3 a{__fmaf_rn(k1.x, P.hh, p.x), __fmaf_rn(k1.y, P.hh, p.y), DIM == 3 ? __fmaf_rn(k1.z, P.hh, p.z) : 0.f};
-                const V3 k2c = wind_at<DIM, W>(P, a, t1, wb, wf);
+                const V3 k2c = wind_at<DIM, W>(P, a, t1, wb, wf, cc);
                 const V3 k2 = sph ? sphere_(P, a.y, k2c) : k2c;
                 a = V3{__fmaf_rn(k2.x, P.hh, p.x), __fmaf_rn(k2.y, P.hh, p.y), DIM == 3 ? __fmaf_rn(k2.z, P.hh, p.z) : 0.f};
-                const V3 k3c = wind_at<DIM, W>(P, a, t1, wb, wf);
+                const V3 k3c = wind_at<DIM, W>(P, a, t1, wb, wf, cc);
                 const V3 k3 = sph ? sphere_(P, a.y, k3c) : k3c;
                 a = V3{__fmaf_rn(k3.x, P.h, p.x), __fmaf_rn(k3.y, P.h, p.y), DIM == 3 ? __fmaf_rn(k3.z, P.h, p.z) : 0.f};
-                const V3 k4c = wind_at<DIM, W>(P, a, t2, wb, wf);
+                const V3 k4c = wind_at<DIM, W>(P, a, t2, wb, wf, cc);
                 const V3 k4 = sph ? sphere_(P, a.y, k4c) : k4c;
                 v.x = (((k1.x + 2.f * k2.x) + 2.f * k3.x) + k4.x) * P.sixth;
                 v.y = (((k1.y + 2.f * k2.y) + 2.f * k3.y) + k4.y) * P.sixth;
@@ -609,7 +656,7 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
                     vc = v;
                 }
             } else {
-                vc = wind_at<DIM, W>(P, p, t0, wb, wf);
+                vc = wind_at<DIM, W>(P, p, t0, wb, wf, cc);
                 v = sph ? sphere_(P, p.y, vc) : vc;
             }
 
