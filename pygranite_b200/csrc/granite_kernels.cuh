@@ -256,15 +256,25 @@ __device__ __forceinline__ float tri_corners(const float (&c)[8], const Cell3 &c
     return lerp_(lerp_(a00, a10, cl.fy), lerp_(a01, a11, cl.fy), cl.fz);
 }
 
-// Raw 16-bit pair nodes of the last sampled cell (3D, 16-bit window-pair layouts): 32 registers.
-struct CornerCacheRaw {
+// Pair nodes of the last cell a particle sampled (window-pair layouts).  Consecutive samples of
+// one particle (its RK4 stages, its next step) mostly fall in the same cell, whose nodes then
+// need no new gathers; the values and the arithmetic are the same either way.  3D keeps the raw
+// 16-bit nodes (32 registers; float32 nodes would need 48 and spill at the kernel's register
+// bound, so the float32 3D path does not cache); 2D keeps the 4 corners as floats (16).
+struct SampleCache {
     int32_t base, sx, sy, sz;
     unsigned valid;
     uint4 q[8];
+    int32_t i00, i10, i01, i11;
+    float b2[4][2], f2[4][2];
+    __device__ __forceinline__ void reset() {
+        base = -1; sx = sy = sz = 0; valid = 0;
+        i00 = i10 = i01 = i11 = -1;
+    }
 };
 
 template <typename H>
-__device__ __forceinline__ void tri3p_cached16(const void *pairs, const Cell3 &c, CornerCacheRaw &cc, float (&ob)[3],
+__device__ __forceinline__ void tri3p_cached16(const void *pairs, const Cell3 &c, SampleCache &cc, float (&ob)[3],
                                                float (&of)[3]) {
     if (c.base != cc.base || c.sx != cc.sx || c.sy != cc.sy || c.sz != cc.sz || c.valid != cc.valid) {
 #pragma unroll
@@ -365,6 +375,25 @@ __device__ __forceinline__ void bil2p(const void *pairs, const Cell2 &c, float (
     }
 }
 
+// 2D: the 4 corners of the last cell, converted to float; bil2p's arithmetic.
+template <typename W>
+__device__ __forceinline__ void bil2p_cached(const void *pairs, const Cell2 &c, SampleCache &cc, float (&ob)[2],
+                                             float (&of)[2]) {
+    if (c.i00 != cc.i00 || c.i10 != cc.i10 || c.i01 != cc.i01 || c.i11 != cc.i11) {
+        Store<W>::load2p(pairs, c.i00, cc.b2[0], cc.f2[0]);
+        Store<W>::load2p(pairs, c.i10, cc.b2[1], cc.f2[1]);
+        Store<W>::load2p(pairs, c.i01, cc.b2[2], cc.f2[2]);
+        Store<W>::load2p(pairs, c.i11, cc.b2[3], cc.f2[3]);
+        cc.i00 = c.i00; cc.i10 = c.i10; cc.i01 = c.i01; cc.i11 = c.i11;
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        ob[k] = lerp_(lerp_(cc.b2[0][k], cc.b2[1][k], c.fx), lerp_(cc.b2[2][k], cc.b2[3][k], c.fx), c.fy);
+        of[k] = lerp_(lerp_(cc.f2[0][k], cc.f2[1][k], c.fx), lerp_(cc.f2[2][k], cc.f2[3][k], c.fx), c.fy);
+    }
+}
+
+
 __device__ __forceinline__ float bil1(const float *plane, const Cell2 &c) {
     return lerp_(lerp_(__ldg(plane + c.i00), __ldg(plane + c.i10), c.fx),
                  lerp_(__ldg(plane + c.i01), __ldg(plane + c.i11), c.fx), c.fy);
@@ -384,7 +413,7 @@ __device__ __forceinline__ float dot3(const V3 &a, const V3 &b, int dim) {
 // Wind at world position p, time weight t: interpolate() of TrajectoryIntegrator.icc:42-110.
 template <int DIM, typename W>
 __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, const void *wb, const void *wf,
-                                      CornerCacheRaw &cc) {
+                                      SampleCache &cc) {
     V3 r{0.f, 0.f, 0.f};
     const float ax = (p.x - P.off[0]) * P.inv_scale[0];
     const float ay = (p.y - P.off[1]) * P.inv_scale[1];
@@ -403,7 +432,7 @@ __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, co
         } else {
             const Cell2 c = make_cell2(P.nx, P.ny, P.filter_weights, ax, ay);
             float b[2], f[2];
-            bil2p<W>(wb, c, b, f);
+            bil2p_cached<W>(wb, c, cc, b, f);
             r.x = lerp_(b[0], f[0], t); r.y = lerp_(b[1], f[1], t);
         }
         return r;
@@ -438,8 +467,8 @@ __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, co
 
 template <int DIM, typename W>
 __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, const void *wb, const void *wf) {
-    CornerCacheRaw cc;
-    cc.base = -1; cc.sx = cc.sy = cc.sz = 0; cc.valid = 0;
+    SampleCache cc;
+    cc.reset();
     return wind_at<DIM, W>(P, p, t, wb, wf, cc);
 }
 
@@ -619,8 +648,8 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
     bool dirty = false;   // volumes / expressions not yet evaluated for the last alive step
     const int sph = P.sphere && DIM == 2;
 
-    CornerCacheRaw cc;
-    cc.base = -1; cc.sx = cc.sy = cc.sz = 0; cc.valid = 0;
+    SampleCache cc;
+    cc.reset();
     for (int s = P.s0; s < P.s1; ++s) {
         const StepEntry E = P.sched[s];
         if (alive && s < life && s >= birth) {
