@@ -1320,6 +1320,10 @@ int make_ctx(gr_engine *e, RunPlan &R, RunCtx &r) {
     r.P = make_params(e);
     r.fn = pick_kernel(e);
     r.threads = block_size_for(e);
+    // some step kernels are built for smaller blocks (their launch bounds)
+    cudaFuncAttributes fa{};
+    CK(cudaFuncGetAttributes(&fa, reinterpret_cast<const void *>(r.fn)));
+    r.threads = std::min(r.threads, fa.maxThreadsPerBlock);
     if (R.graph) {
         // one resident wave (times grid_waves) walks the live prefix with a grid-stride loop
         int per_sm = 0, sms = 0;

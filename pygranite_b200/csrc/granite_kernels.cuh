@@ -267,6 +267,7 @@ struct SampleCache {
     uint4 q[8];
     int32_t i00, i10, i01, i11;
     float b2[4][2], f2[4][2];
+    float c32[6][8];   // float32 3D: u, v, w back and front of the 8 corners
     __device__ __forceinline__ void reset() {
         base = -1; sx = sy = sz = 0; valid = 0;
         i00 = i10 = i01 = i11 = -1;
@@ -294,6 +295,25 @@ __device__ __forceinline__ void tri3p_cached16(const void *pairs, const Cell3 &c
     }
     ob[0] = tri_corners(u, c); ob[1] = tri_corners(v, c); ob[2] = tri_corners(w, c);
     of[0] = tri_corners(uf, c); of[1] = tri_corners(vf, c); of[2] = tri_corners(wf, c);
+}
+
+// float32 3D: the 8 corners as floats (48 registers; see AdvBounds for the launch shape).
+__device__ __forceinline__ void tri3p_cached32(const void *pairs, const Cell3 &c, SampleCache &cc, float (&ob)[3],
+                                               float (&of)[3]) {
+    if (c.base != cc.base || c.sx != cc.sx || c.sy != cc.sy || c.sz != cc.sz || c.valid != cc.valid) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
+            const int32_t idx = c.base + (dx ? c.sx : 0) + (dy ? c.sy : 0) + (dz ? c.sz : 0);
+            float b[3] = {0.f, 0.f, 0.f}, f[3] = {0.f, 0.f, 0.f};
+            if (c.valid & (1u << k)) Store<Pair<float>>::load3p(pairs, idx, b, f);
+            cc.c32[0][k] = b[0]; cc.c32[1][k] = b[1]; cc.c32[2][k] = b[2];
+            cc.c32[3][k] = f[0]; cc.c32[4][k] = f[1]; cc.c32[5][k] = f[2];
+        }
+        cc.base = c.base; cc.sx = c.sx; cc.sy = c.sy; cc.sz = c.sz; cc.valid = c.valid;
+    }
+    ob[0] = tri_corners(cc.c32[0], c); ob[1] = tri_corners(cc.c32[1], c); ob[2] = tri_corners(cc.c32[2], c);
+    of[0] = tri_corners(cc.c32[3], c); of[1] = tri_corners(cc.c32[4], c); of[2] = tri_corners(cc.c32[5], c);
 }
 
 template <typename W> struct PairElem { using type = void; };
@@ -426,6 +446,8 @@ __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, co
             using H = typename PairElem<W>::type;
             if constexpr (!std::is_same<H, float>::value && !std::is_same<H, void>::value)
                 tri3p_cached16<H>(wb, c, cc, b, f);
+            else if constexpr (std::is_same<H, float>::value)
+                tri3p_cached32(wb, c, cc, b, f);
             else
                 tri3p<W>(wb, c, b, f);
             r.x = lerp_(b[0], f[0], t); r.y = lerp_(b[1], f[1], t); r.z = lerp_(b[2], f[2], t);
@@ -890,8 +912,13 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
 // One thread per particle, or (P.grid_stride) a persistent grid striding over the live
 // prefix, whose size is read on the device: the launch shape then stays fixed while the live
 // count shrinks, as a captured CUDA graph needs.
+// Launch bounds: 256 threads, 2 blocks per SM (128 registers); the float32 3D pair kernel keeps
+// 48 cached floats and runs 128-thread blocks, 3 per SM (up to 170 registers).
+template <int DIM, typename W> struct AdvBounds { static constexpr int threads = 256, blocks = GR_ADV_MIN_BLOCKS; };
+template <> struct AdvBounds<3, Pair<float>> { static constexpr int threads = 128, blocks = 3; };
+
 template <int DIM, bool RK4, typename W>
-__global__ void __launch_bounds__(256, GR_ADV_MIN_BLOCKS) advance_kernel(const __grid_constant__ KParams P) {
+__global__ void __launch_bounds__(AdvBounds<DIM, W>::threads, AdvBounds<DIM, W>::blocks) advance_kernel(const __grid_constant__ KParams P) {
     const int64_t n_live = P.n_dev ? (int64_t)*P.n_dev : P.n;
     unsigned long long steps = 0;
     unsigned alive = 0;

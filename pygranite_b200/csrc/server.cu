@@ -356,6 +356,9 @@ int allocate(gr_server *S, int64_t budget) {
         const int st = S->s.storage;
         P.fn = st == GR_STORE_BF16 ? advance_bf16(S->dim, p == 1, true)
              : st == GR_STORE_F16 ? advance_f16(S->dim, p == 1, true) : advance_f32(S->dim, p == 1, true);
+        cudaFuncAttributes fa{};
+        SK(cudaFuncGetAttributes(&fa, reinterpret_cast<const void *>(P.fn)));
+        P.threads = std::min(P.threads, fa.maxThreadsPerBlock);   // the kernel's launch bounds
         int per_sm = 0, sms = 0;
         SK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, P.fn, P.threads, 0));
         SK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->s.device));
