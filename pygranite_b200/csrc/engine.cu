@@ -1855,21 +1855,27 @@ static int fetch_rows(gr_engine *e, void *out, int64_t capacity, const void *src
         CK(cudaStreamSynchronize(e->cs));
         return GR_OK;
     }
-    constexpr size_t kBounce = size_t(64) << 20;
-    if (total < 2 * kBounce || row_bytes > kBounce) {
+    // up to 64 MB per bounce buffer; results from 8 MB on go through them, so the host copies
+    // (and the first-touch page faults of a fresh destination) run on the copy threads
+    constexpr size_t kBounce = size_t(64) << 20, kBounceFrom = size_t(8) << 20;
+    if (total < kBounceFrom || row_bytes > kBounce) {
         CK(cudaMemcpy2D(out, row_bytes, src, row_stride * elem, row_bytes, rows, cudaMemcpyDeviceToHost));
         return GR_OK;
     }
     // large results: DMA into two pinned bounce buffers, each emptied by a parallel host copy
     // while the other fills
+    const size_t chunk = std::min(kBounce, total);
     for (auto &b : e->bounce) {
-        if (!b.p) {
-            if (gr_host_alloc((int64_t)kBounce, &b.p) != GR_OK) return GR_ERR_RUNTIME;
-            b.bytes = kBounce;
+        if (b.bytes < chunk) {
+            if (b.p) gr_host_free(b.p);
+            b.p = nullptr;
+            b.bytes = 0;
+            if (gr_host_alloc((int64_t)chunk, &b.p) != GR_OK) return GR_ERR_RUNTIME;
+            b.bytes = chunk;
         }
         if (!b.done) CK(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
     }
-    const int64_t rows_per = (int64_t)(kBounce / row_bytes);
+    const int64_t rows_per = (int64_t)(std::min(e->bounce[0].bytes, e->bounce[1].bytes) / row_bytes);
     const char *s8 = static_cast<const char *>(src);
     char *d8 = static_cast<char *>(out);
     int64_t prev_rows = 0, prev_row0 = 0;
