@@ -258,9 +258,10 @@ __device__ __forceinline__ float tri_corners(const float (&c)[8], const Cell3 &c
 
 // Pair nodes of the last cell a particle sampled (window-pair layouts).  Consecutive samples of
 // one particle (its RK4 stages, its next step) mostly fall in the same cell, whose nodes then
-// need no new gathers; the values and the arithmetic are the same either way.  3D keeps the raw
-// 16-bit nodes (32 registers; float32 nodes would need 48 and spill at the kernel's register
-// bound, so the float32 3D path does not cache); 2D keeps the 4 corners as floats (16).
+// need no new gathers; the values and the arithmetic are the same either way.  3D 16-bit kernels
+// keep the raw nodes (32 registers, within their 128-register bound); the float32 3D kernel
+// keeps the 48 floats and is built for 128-thread blocks, 3 per SM (AdvBounds); 2D keeps the 4
+// corners as floats (16 registers).
 struct SampleCache {
     int32_t base, sx, sy, sz;
     unsigned valid;
