@@ -50,6 +50,21 @@ def test_pinned_arrays_are_page_locked_and_reused():
     assert capi.pinned_empty(0).size == 0
 
 
+@pytest.mark.gpu
+def test_small_page_locked_requests_share_slabs():
+    # requests up to 4 KiB (counters, flags) take 4 KiB slots of shared 2 MiB slabs
+    s0 = capi.host_cache_stats()
+    arrs = [capi.pinned_empty(16) for _ in range(600)]
+    s1 = capi.host_cache_stats()
+    assert s1.allocations - s0.allocations <= 2
+    assert all(capi.is_pinned(a) for a in arrs) and len({a.ctypes.data for a in arrs}) == 600
+    assert s1.live_bytes == s0.live_bytes + 600 * 4096
+    for arr in arrs:
+        arr[...] = 1.0
+    del arrs, arr
+    assert capi.host_cache_stats().live_bytes == s0.live_bytes
+
+
 def _pinned_source(src):
     """The same snapshots, each array copied into page-locked memory."""
     def pin(a):
