@@ -142,6 +142,10 @@ struct gr_engine {
     bool use_pair = false;             // window-pair layout for the step kernel
     DevBuf<char> pairbuf[2];
     int64_t pair_window[2] = {-1, -1};
+    // the next window's pair is packed on ps while the current window's launches run
+    cudaStream_t ps = nullptr;
+    cudaEvent_t pair_ready[2] = {nullptr, nullptr}, pair_go = nullptr;
+    bool pair_pending[2] = {false, false};
     DevBuf<float> vol, cons, lift, topo;
     int nvol = 0, ncon = 0;
     bool has_topo = false, has_uplift = false;
@@ -224,6 +228,10 @@ struct gr_engine {
         if (cs) cudaStreamSynchronize(cs);
         if (xs) cudaStreamSynchronize(xs);
         if (us) cudaStreamSynchronize(us);
+        if (ps) cudaStreamSynchronize(ps);
+        for (auto ev : pair_ready)
+            if (ev) cudaEventDestroy(ev);
+        if (pair_go) cudaEventDestroy(pair_go);
         for (auto e : raw_free)
             if (e) cudaEventDestroy(e);
         for (auto e : slot_free) cudaEventDestroy(e);
@@ -239,6 +247,7 @@ struct gr_engine {
         if (cs) cudaStreamDestroy(cs);
         if (xs) cudaStreamDestroy(xs);
         if (us) cudaStreamDestroy(us);
+        if (ps) cudaStreamDestroy(ps);
     }
 };
 
@@ -476,6 +485,9 @@ int gr_create(const gr_settings *settings, gr_engine **out) {
     }
     CK(cudaEventCreateWithFlags(&e->upload_done, cudaEventDisableTiming));
     CK(cudaStreamCreateWithFlags(&e->us, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&e->ps, cudaStreamNonBlocking));
+    for (auto &ev : e->pair_ready) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&e->pair_go, cudaEventDisableTiming));
     for (auto &ev : e->raw_free) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     e->wind_holds.assign(e->K, -1);
     e->vol_holds.assign(e->K, -1);
@@ -932,6 +944,7 @@ std::vector<int32_t> crec_table(const gr_engine *e, const RunPlan &R, int64_t ex
 }
 
 int ensure_pair(gr_engine *e, int64_t w);
+int settle_pairs(gr_engine *e);
 
 int pair_elem(const gr_engine *e) {
     return e->s.storage == GR_STORE_F32 ? (e->dim == 3 ? 16 : 8) : (e->dim == 3 ? 8 : 4);
@@ -1053,6 +1066,10 @@ int run_prepare(gr_engine *e, RunPlan &R, bool graph) {
     // window-pair layout: one load per corner returns both snapshots; launches never cross a
     // window boundary then
     e->use_pair = e->wind_dynamic && s.layout == 0;
+    {
+        const int rc = settle_pairs(e);
+        if (rc) return rc;
+    }
     e->pair_window[0] = e->pair_window[1] = -1;
     if (graph) {
         if (e->use_pair)
@@ -1279,23 +1296,65 @@ cudaEvent_t pool_event(gr_engine *e, size_t k) {
 }
 
 // Builds the window-pair buffer of window w from its two ring slots (on the compute stream).
-int ensure_pair(gr_engine *e, int64_t w) {
+// Packs window w's pair (ring slots w and w + 1, interleaved) into pairbuf[w & 1] on `stream`.
+int pack_pair(gr_engine *e, int64_t w, cudaStream_t stream) {
     const int b = (int)(w & 1);
-    if (e->pair_window[b] == w) return GR_OK;
     const int elem = pair_elem(e);
     CK(e->pairbuf[b].alloc((size_t)e->nodes * 2 * elem));
     const char *back = e->wind.p + (int64_t)(w % e->K) * e->wind_stride;
     const char *front = e->wind.p + (int64_t)((w + 1) % e->K) * e->wind_stride;
     const int threads = 256, blocks = grid_for(e->nodes, threads);
     if (elem == 16)
-        pair_pack_kernel<uint4><<<blocks, threads, 0, e->cs>>>((const uint4 *)back, (const uint4 *)front, (uint4 *)e->pairbuf[b].p, e->nodes);
+        pair_pack_kernel<uint4><<<blocks, threads, 0, stream>>>((const uint4 *)back, (const uint4 *)front, (uint4 *)e->pairbuf[b].p, e->nodes);
     else if (elem == 8)
-        pair_pack_kernel<uint2><<<blocks, threads, 0, e->cs>>>((const uint2 *)back, (const uint2 *)front, (uint2 *)e->pairbuf[b].p, e->nodes);
+        pair_pack_kernel<uint2><<<blocks, threads, 0, stream>>>((const uint2 *)back, (const uint2 *)front, (uint2 *)e->pairbuf[b].p, e->nodes);
     else
-        pair_pack_kernel<unsigned><<<blocks, threads, 0, e->cs>>>((const unsigned *)back, (const unsigned *)front, (unsigned *)e->pairbuf[b].p, e->nodes);
+        pair_pack_kernel<unsigned><<<blocks, threads, 0, stream>>>((const unsigned *)back, (const unsigned *)front, (unsigned *)e->pairbuf[b].p, e->nodes);
     CK(cudaGetLastError());
     e->pair_window[b] = w;
     e->stats.aux_launches++;
+    return GR_OK;
+}
+
+// Orders every pair packed ahead on ps before later work on cs (the end of a run, a failed run,
+// the next run's first upload into a ring slot that the pack reads).
+int settle_pairs(gr_engine *e) {
+    for (int b = 0; b < 2; ++b)
+        if (e->pair_pending[b]) {
+            CK(cudaStreamWaitEvent(e->cs, e->pair_ready[b], 0));
+            e->pair_pending[b] = false;
+        }
+    return GR_OK;
+}
+
+int ensure_pair(gr_engine *e, int64_t w) {
+    const int b = (int)(w & 1);
+    if (e->pair_window[b] == w) {
+        if (e->pair_pending[b]) {   // packed ahead on ps
+            CK(cudaStreamWaitEvent(e->cs, e->pair_ready[b], 0));
+            e->pair_pending[b] = false;
+        }
+        return GR_OK;
+    }
+    return pack_pair(e, w, e->cs);
+}
+
+// Before window w's first launch: the pair of window w + 1 goes to the other buffer on ps, once
+// the launches of window w - 1 (the last readers of that buffer) are done and both of its
+// snapshots are in the ring, so the pack overlaps window w's launches.
+int prefetch_pair(gr_engine *e, int64_t w, int64_t nwin) {
+    const int64_t w1 = w + 1;
+    const int b1 = (int)(w1 & 1);
+    if (w1 >= nwin || e->pair_window[b1] == w1) return GR_OK;
+    if (e->wind_holds[w1 % e->K] != w1 || e->wind_holds[(w1 + 1) % e->K] != w1 + 1) return GR_OK;
+    CK(cudaEventRecord(e->pair_go, e->cs));
+    CK(cudaStreamWaitEvent(e->ps, e->pair_go, 0));
+    CK(cudaStreamWaitEvent(e->ps, e->slot_ready[w1 % e->K], 0));
+    CK(cudaStreamWaitEvent(e->ps, e->slot_ready[(w1 + 1) % e->K], 0));
+    const int rc = pack_pair(e, w1, e->ps);
+    if (rc) return rc;
+    CK(cudaEventRecord(e->pair_ready[b1], e->ps));
+    e->pair_pending[b1] = true;
     return GR_OK;
 }
 
@@ -1343,9 +1402,13 @@ int launch_steps(RunCtx &r, int64_t s0, int64_t s1, int64_t window) {
     P.s0 = (int32_t)s0;
     P.s1 = (int32_t)s1;
     if (e->use_pair) {
-        const int rc = ensure_pair(e, window);
+        int rc = ensure_pair(e, window);
         if (rc) return rc;
         P.pair = e->pairbuf[window & 1].p;
+        if (!r.R->graph && e->s.minimum_alive == 0) {
+            rc = prefetch_pair(e, window, r.R->nwin);
+            if (rc) return rc;
+        }
     }
     if (r.R->graph) {
         r.fn<<<(unsigned)r.grid, r.threads, 0, e->cs>>>(P);
@@ -1745,6 +1808,8 @@ extern "C" int gr_run(gr_engine *e, gr_loader_fn loader, void *user) {
 
     RecordCounts c;
     rc = run_tail(r, c);
+    if (rc) return rc;
+    rc = settle_pairs(e);   // a pair packed ahead for a window that did not run
     if (rc) return rc;
     if (e->dest_run) {
         // the rest of the records; the run ends when they are in host memory
