@@ -5,8 +5,10 @@
 // (source/granite/DataLoader.hpp:26-81, TrajectoryIntegrator.cpp:146-360).  For synthetic
 // fields this evaluates each snapshot on the GPU instead and hands the planes to the engine's
 // device-pointer load, so a run needs no host snapshot memory and no Python in its loop.
-// Arithmetic is float64 (no contraction: the library builds with --fmad=false), rounded to
-// float32 at the end, in the operation order of the host generators of the benchmark inputs.
+// Arithmetic is float64 (no contraction besides the explicit fma of the Fourier sums), rounded
+// to float32 at the end.  The double gyre follows the host generator's operation order; the
+// Fourier field is, like the host generator, a separable product of per-axis plane-wave factors
+// (association order differs, so the two agree to float64 rounding, not bit for bit).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -33,6 +35,8 @@ struct gr_field {
     int modes = 0;
     double spacing[3]{};               // per axis, grid order (z, y, x) / (y, x)
     DevBuf<double> k, amp, phase, om, scale;
+    DevBuf<double2> fac_x, fac_y, fac_z;   // exp(i k_a x_i) per (component, mode) and node index
+    DevBuf<double2> coef;              // amp e^{i (phase - omega t)} of the current snapshot
     DevBuf<float> planes;              // dim planes of the current snapshot
     int64_t holds = -1;                // snapshot in `planes`
     cudaStream_t stream = nullptr;
@@ -78,24 +82,81 @@ __global__ void double_gyre_kernel(double A, double eps, double omega, double t,
     }
 }
 
-// component c = scale_c * sum_m amp_cm cos(phase_cm - omega_cm t + k_cm . position)
-__global__ void fourier_kernel(const double *__restrict__ k, const double *__restrict__ amp,
-                               const double *__restrict__ phase, const double *__restrict__ om,
-                               const double *__restrict__ scale, int dim, int modes, int64_t nz, int64_t ny,
-                               int64_t nx, double dz, double dy, double dx, double t, float *__restrict__ out) {
-    const int64_t nodes = nz * ny * nx;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t ix = i % nx, iy = (i / nx) % ny, iz = i / (nx * ny);
-        const double px = (double)ix * dx, py = (double)iy * dy, pz = (double)iz * dz;
+// Per-axis plane-wave factors, time-independent: fac[cm][i] = exp(i k_cm,a x_i), x_i = i * spacing
+// along grid axis a (k holds each mode's wave vector in grid order, z y x / y x).
+__global__ void fourier_factors_kernel(const double *__restrict__ k, int dim, int axis, int64_t cms, int64_t n,
+                                       double spacing, double2 *__restrict__ fac) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < cms * n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t cm = j / n, i = j % n;
+        double sn, cs;
+        sincos(k[cm * dim + axis] * ((double)i * spacing), &sn, &cs);
+        fac[j] = make_double2(cs, sn);
+    }
+}
+
+// The snapshot's mode coefficients: coef[cm] = amp_cm exp(i (phase_cm - omega_cm t)).
+__global__ void fourier_coef_kernel(const double *__restrict__ amp, const double *__restrict__ phase,
+                                    const double *__restrict__ om, int64_t cms, double t, double2 *__restrict__ coef) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < cms; j += (int64_t)gridDim.x * blockDim.x) {
+        double sn, cs;
+        sincos(phase[j] - om[j] * t, &sn, &cs);
+        coef[j] = make_double2(amp[j] * cs, amp[j] * sn);
+    }
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+constexpr int kFieldThreads = 128;   // x positions per block
+constexpr int kFieldRows = 8;        // grid rows (consecutive (z, y) pairs) per block
+constexpr int kModeChunk = 64;       // modes whose row coefficients are staged at once
+
+// component c = scale_c Re sum_m (coef_cm fz_cm[iz] fy_cm[iy]) fx_cm[ix]: the plane waves as a
+// rank-`modes` separable product, so a node costs two multiply-adds per mode instead of a
+// cosine.  The row coefficients (everything but fx) of a chunk of modes are staged in shared
+// memory for the block's kFieldRows rows; each thread keeps one x position's sums for all of them.
+__global__ void __launch_bounds__(kFieldThreads) fourier_rows_kernel(
+        const double2 *__restrict__ fx, const double2 *__restrict__ fy, const double2 *__restrict__ fz,
+        const double2 *__restrict__ coef, const double *__restrict__ scale, int dim, int modes, int64_t nz,
+        int64_t ny, int64_t nx, float *__restrict__ out) {
+    __shared__ double2 w[kModeChunk][kFieldRows];
+    const int64_t rows = nz * ny, nodes = rows * nx;
+    const int64_t ix = (int64_t)blockIdx.x * kFieldThreads + threadIdx.x;
+    const bool in_x = ix < nx;
+    for (int64_t row0 = (int64_t)blockIdx.y * kFieldRows; row0 < rows; row0 += (int64_t)gridDim.y * kFieldRows) {
         for (int c = 0; c < dim; ++c) {
-            double sum = 0.0;
-            for (int m = 0; m < modes; ++m) {
-                const int64_t cm = (int64_t)c * modes + m;
-                const double *kv = k + cm * dim;
-                const double kdx = dim == 3 ? (kv[0] * pz + kv[1] * py) + kv[2] * px : kv[0] * py + kv[1] * px;
-                sum += amp[cm] * cos((phase[cm] - om[cm] * t) + kdx);
+            double acc[kFieldRows];
+#pragma unroll
+            for (int r = 0; r < kFieldRows; ++r) acc[r] = 0.0;
+            for (int m0 = 0; m0 < modes; m0 += kModeChunk) {
+                const int mc = min(kModeChunk, modes - m0);
+                __syncthreads();   // the previous chunk's coefficients are no longer read
+                for (int j = threadIdx.x; j < mc * kFieldRows; j += kFieldThreads) {
+                    const int mm = j / kFieldRows, r = j % kFieldRows;
+                    const int64_t row = row0 + r, cm = (int64_t)c * modes + m0 + mm;
+                    double2 v = make_double2(0.0, 0.0);
+                    if (row < rows) {
+                        v = coef[cm];
+                        if (dim == 3) v = cmul(v, fz[cm * nz + row / ny]);
+                        v = cmul(v, fy[cm * ny + row % ny]);
+                    }
+                    w[mm][r] = v;
+                }
+                __syncthreads();
+                if (in_x) {
+                    for (int mm = 0; mm < mc; ++mm) {
+                        const double2 e = fx[((int64_t)c * modes + m0 + mm) * nx + ix];
+#pragma unroll
+                        for (int r = 0; r < kFieldRows; ++r) acc[r] = fma(-w[mm][r].y, e.y, fma(w[mm][r].x, e.x, acc[r]));
+                    }
+                }
             }
-            out[(int64_t)c * nodes + i] = (float)(sum * scale[c]);
+            if (in_x) {
+#pragma unroll
+                for (int r = 0; r < kFieldRows; ++r)
+                    if (row0 + r < rows) out[(int64_t)c * nodes + (row0 + r) * nx + ix] = (float)(acc[r] * scale[c]);
+            }
         }
     }
 }
@@ -111,10 +172,14 @@ int generate(gr_field *f, int64_t snapshot) {
                                                               f->lx / (double)f->nx, f->ly / (double)f->ny,
                                                               f->planes.p, f->planes.p + f->nodes);
     } else {
-        const double dz = f->dim == 3 ? f->spacing[0] : 0.0;
-        const double dy = f->spacing[f->dim - 2], dx = f->spacing[f->dim - 1];
-        fourier_kernel<<<blocks, threads, 0, f->stream>>>(f->k.p, f->amp.p, f->phase.p, f->om.p, f->scale.p, f->dim,
-                                                          f->modes, f->nz, f->ny, f->nx, dz, dy, dx, t, f->planes.p);
+        const int64_t cms = (int64_t)f->dim * f->modes;
+        fourier_coef_kernel<<<grid_for(cms, 256), 256, 0, f->stream>>>(f->amp.p, f->phase.p, f->om.p, cms, t, f->coef.p);
+        FK(cudaGetLastError());
+        const int64_t groups = (f->nz * f->ny + kFieldRows - 1) / kFieldRows;
+        const dim3 grid((unsigned)((f->nx + kFieldThreads - 1) / kFieldThreads), (unsigned)std::min<int64_t>(groups, 65535));
+        fourier_rows_kernel<<<grid, kFieldThreads, 0, f->stream>>>(f->fac_x.p, f->fac_y.p, f->fac_z.p, f->coef.p,
+                                                                   f->scale.p, f->dim, f->modes, f->nz, f->ny, f->nx,
+                                                                   f->planes.p);
     }
     FK(cudaGetLastError());
     FK(cudaStreamSynchronize(f->stream));
@@ -189,6 +254,21 @@ int gr_field_fourier(int32_t dim, const int64_t *shape, const double *spacing, i
     FK(cudaMemcpy(f->phase.p, phase, cm * sizeof(double), cudaMemcpyHostToDevice));
     FK(cudaMemcpy(f->om.p, omega, cm * sizeof(double), cudaMemcpyHostToDevice));
     FK(cudaMemcpy(f->scale.p, scale, (size_t)dim * sizeof(double), cudaMemcpyHostToDevice));
+    // the per-axis factors of every mode (time-independent)
+    FK(f->coef.alloc(cm));
+    FK(f->fac_x.alloc(cm * (size_t)f->nx));
+    FK(f->fac_y.alloc(cm * (size_t)f->ny));
+    if (dim == 3) FK(f->fac_z.alloc(cm * (size_t)f->nz));
+    struct Axis { DevBuf<double2> *fac; int axis; int64_t n; };
+    const Axis axes[3] = {{&f->fac_x, dim - 1, f->nx}, {&f->fac_y, dim - 2, f->ny}, {&f->fac_z, 0, f->nz}};
+    for (int a = 0; a < dim; ++a) {
+        const int64_t total = (int64_t)cm * axes[a].n;
+        fourier_factors_kernel<<<grid_for(total, 256), 256, 0, f->stream>>>(f->k.p, dim, axes[a].axis, (int64_t)cm,
+                                                                             axes[a].n, f->spacing[axes[a].axis],
+                                                                             axes[a].fac->p);
+        FK(cudaGetLastError());
+    }
+    FK(cudaStreamSynchronize(f->stream));
     *out = f.release();
     return GR_OK;
 }
