@@ -42,10 +42,17 @@ def test_double_gyre_snapshots_match_host_generator():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape,spacing", [((16, 24, 32), (250.0, 1000.0, 1000.0)), ((48, 64), (1000.0, 1000.0))])
-def test_fourier_snapshots_match_host_generator(shape, spacing):
+@pytest.mark.parametrize("shape,spacing,modes", [
+    ((16, 24, 32), (250.0, 1000.0, 1000.0), 32),
+    ((48, 64), (1000.0, 1000.0), 32),
+    # several x blocks (the last one partial), a row count that is no multiple of the rows per
+    # block, and mode chunks with a partial last chunk
+    ((5, 7, 150), (250.0, 1000.0, 1000.0), 100),
+    ((13, 300), (1000.0, 1000.0), 65),
+])
+def test_fourier_snapshots_match_host_generator(shape, spacing, modes):
     kw = {} if len(shape) == 3 else dict(rms=(7.0710678, 7.0710678))
-    field = W.FourierField(shape, spacing, n_modes=32, seed=4, **kw)
+    field = W.FourierField(shape, spacing, n_modes=modes, seed=4, **kw)
     f = capi.Field.fourier(field, 600.0, 8)
     for k in (0, 5):
         ref = field.snapshot(600.0 * k)
