@@ -15,7 +15,7 @@
 namespace granite_b200 {
 
 // Host copies into and out of pinned staging, split into 1 MB chunks over a persistent pool of
-// worker threads (at most 8, created on first use) and the calling thread.  One core copies a
+// worker threads (at most 16, created on first use) and the calling thread.  One core copies a
 // few GB/s, which would otherwise set the pace of a run fed from host memory.
 class CopyPool {
   public:
@@ -71,7 +71,7 @@ class CopyPool {
 
     CopyPool() {
         const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-        const unsigned n = std::min(7u, hw > 1 ? hw - 1 : 0u);   // plus the caller: at most 8
+        const unsigned n = std::min(15u, hw > 1 ? hw - 1 : 0u);   // plus the caller: at most 16
         for (unsigned k = 0; k < n; ++k) workers_.emplace_back([this] { loop(); });
     }
 
