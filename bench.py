@@ -59,8 +59,12 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-native", action="store_true", help="skip the native-loader run")
-    p.add_argument("--cpu-particles", type=int, default=20000)
-    p.add_argument("--cpu-steps", type=int, default=100)
+    p.add_argument("--cpu-particles", type=int, default=1_000_000)
+    p.add_argument("--cpu-steps", type=int, default=200)
+    p.add_argument("--ref-steps", type=int, default=20, help="reference arm: steps of the workload's prefix")
+    p.add_argument("--parity-sample", type=int, default=2000,
+                   help="particles of the timed run checked against the float32 / float64 oracle (0 = off)")
+    p.add_argument("--no-forms", action="store_true", help="plain workload: skip the batch / serve / precision forms")
     p.add_argument("--workload", default="plain", choices=["plain", "batch", "serve", "precision"],
                    help="plain: the 3D RK4 configuration; batch: 512 seed sets of uneven size and lifetime; "
                         "serve: a Poisson stream of requests on the request server")
@@ -77,6 +81,7 @@ def parse():
     p.add_argument("--no-plain", action="store_true", help="batch: skip the one-run-per-set baseline")
     p.add_argument("--no-acc", action="store_true", help="batch: skip the float64 accuracy sample")
     p.add_argument("--serve-budget-gb", type=float, default=0.0, help="serve: HBM budget (0 = 1/4 of free)")
+    p.add_argument("--serve-acc", type=int, default=2, help="serve: requests checked against the float64 oracle")
     p.add_argument("--acc-life", type=int, default=500,
                    help="accuracy sample: sets with at most this lifetime are checked against the float64 oracle")
     return p.parse_args()
@@ -170,9 +175,11 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic_per_particle_step(storage):
-    """DRAM bytes per particle-step from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "advance_kernel_traffic.json")
+def load_kernel_profile(storage):
+    """Per-particle-step figures of the step kernel from the committed ncu summary
+    (profiles/advance_kernel_counters.json): DRAM bytes and warp instructions per
+    particle-step, with the capture they come from."""
+    path = os.path.join(ROOT, "profiles", "advance_kernel_counters.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
@@ -192,24 +199,124 @@ def cpu_baseline(args, settings, src, seeds, threads=None):
                 sample=f"{n} particles x {r['steps']} RK4 steps of the same workload (float64 oracle)")
 
 
+CELL_3D = np.array([1000.0, 1000.0, 250.0])
+
+
+def sample_ids(n, m):
+    """m particle ids spread evenly over the seed array."""
+    return np.unique(np.linspace(0, n - 1, min(m, n)).round().astype(np.int64))
+
+
+def plain_oracle(settings, src, seeds, ids):
+    """float32 and float64 oracle runs of the sampled particles on the same snapshots (the
+    checker; particles are independent, so a subset runs exactly as inside the full set)."""
+    from oracle import oracle as orc
+    data = orc.Inputs(wind=src.wind, seeds=seeds[ids], volumes=src.volumes)
+    th = os.cpu_count() or 1
+    return (orc.run(orc.settings(**settings), data, precision="f32", threads=th),
+            orc.run(orc.settings(**settings), data, precision="f64", threads=th))
+
+
+def check_plain(got, ref32, ref64):
+    """got: the sampled rows of a run (trajectories, status, total_curvature, T samples,
+    expression values).  Bit-for-bit comparison with the float32 oracle, and the position
+    error in grid cells against the float64 oracle after 100 steps (record 10) and at the end,
+    over particles not yet aborted in either run at that record."""
+    traj, status = got["trajectories"], got["status"]
+    checks = {
+        "positions": bool(np.array_equal(traj, ref32["trajectories"])),
+        "status": bool(np.array_equal(status, ref32["status"])),
+        "total_curvature": bool(np.array_equal(got["total_curvature"], ref32["total_curvature"])),
+        "volume_T": bool(np.array_equal(got["volume"], ref32["volume_info"]["T"])),
+        "expression": bool(np.array_equal(got["expression"], ref32["compute_info"][0])),
+    }
+    bad = np.any(traj != ref32["trajectories"], axis=(1, 2)) | (status != ref32["status"])
+    L = traj.shape[1]
+    f64 = {}
+    for rec in sorted({min(10, L - 1), L - 1}):
+        k = 10 * rec
+        live = ((ref64["step_of_abort"] < 0) | (ref64["step_of_abort"] >= k)) & \
+               ((ref32["step_of_abort"] < 0) | (ref32["step_of_abort"] >= k))
+        d = (np.abs(traj[live, rec].astype(np.float64) - ref64["trajectories"][live, rec]) / CELL_3D).max(axis=1)
+        f64[f"after_{k}_steps"] = {"particles": int(d.size),
+                                   "cell_rms": float(np.sqrt(np.mean(d ** 2))) if d.size else None,
+                                   "cell_p50": float(np.median(d)) if d.size else None,
+                                   "cell_p99": float(np.percentile(d, 99)) if d.size else None,
+                                   "cell_max": float(d.max()) if d.size else None}
+    return {"f32_bitexact": all(checks.values()), "checks": checks, "sample": int(traj.shape[0]), "records": int(L),
+            "mismatched_particles": int(bad.sum()), "status_vs_f64_differ": int(np.sum(status != ref64["status"])),
+            "f64": f64}
+
+
+def plain_config(args, world):
+    """The `config` object of the plain workload, the same in both arms."""
+    n_snap = args.sim_steps // 10 + 1
+    return {"workload": WORKLOAD, "particles_per_gpu": args.particles, "sim_steps": args.sim_steps,
+            "snapshots": n_snap, "grid": [192, 192, 64], "storage": args.storage,
+            "parallelism": f"replicas{world}", "l2": f"inputs larger than L2 ({n_snap} snapshots, 7.6 GB ring)",
+            "records_every": 10, "sort_interval": args.sort_interval, "steps_per_launch": args.steps_per_launch,
+            "wind_layout": ["window-pair", "ring"][args.layout]}
+
+
+def reference_gpu_available():
+    from oracle.ref_harness import refrun
+    return refrun.available()
+
+
 def run_reference(args):
+    """The reference's own implementation of the path: its `integrate` kernel, instantiated
+    unmodified from its sources (oracle/_ref, built by oracle/ref_harness), run by a host loop
+    that restates its computeLoop_ (one launch, one synchronisation and the record copies per
+    step, snapshots uploaded between windows) on a bounded prefix of the same workload.  Headline:
+    the launch shape as shipped (TrajectoryIntegrator.tpp:790-796 swaps the arguments of sdiv, so
+    one 512-thread block does all the work); beside it the same with BLOCKS = ceil(N / THREADS).
+    The float64 CPU oracle (OpenMP) is reported as cpu_baseline.  Without the built kernel the
+    CPU oracle is the value."""
     world, rank, _ = dist_env()
     if rank != 0:
         return 0
-    settings, src, seeds = workload(args, 0)
-    vals = []
-    for k in range(args.warmup + args.steps):
-        cb = cpu_baseline(args, settings, src, seeds)
-        if k >= args.warmup:
-            vals.append(cb["value"])
-    value = float(np.mean(vals))
-    cb["value"] = value
-    line = {"impl": "reference", "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+    from pygranite_b200 import workloads as W
+    prefix = args.ref_steps
+    n_snap = max(prefix, args.cpu_steps) // 10 + 3
+    settings, src, seeds = W.config2(n_particles=args.particles, n_snapshots=n_snap, steps=args.sim_steps, seed=0)
+    cb = cpu_baseline(args, settings, src, seeds)
+    line = {"impl": "reference", "metric": "particle-steps/s", "unit": "particle-steps/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Fourier-mode field)",
-            "config": {"workload": WORKLOAD, "particles": args.particles, "sim_steps": args.sim_steps},
-            "cpu_baseline": cb,
-            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Fourier-mode field)",
+            "config": plain_config(args, 1), "cpu_baseline": cb}
+    if not reference_gpu_available():
+        line.update(value=cb["value"], dtype="f64", ms_per_step=None,
+                    reference_gpu={"unavailable": "oracle/_ref/libref_integrate.so not built (needs the reference's "
+                                                  "sources: make -C oracle/ref_harness REF=<checkout>)"},
+                    e2e={"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0})
+        print(json.dumps(line), flush=True)
+        return 0
+    from oracle.ref_harness import refrun
+    vol = src.volumes[0]["T"]
+    out = {}
+    for fixed in (False, True):
+        ms = ps = h2d = d2h = 0.0
+        for k in range(args.warmup + args.steps):
+            r = refrun.run(settings, src.wind, seeds, volume=vol, blocks_fixed=fixed, step_limit=prefix,
+                           count_steps=True)
+            if k >= args.warmup:
+                ms += r["loop_ms"]
+                ps += r["particle_steps"]
+                h2d += r["h2d_bytes"]
+                d2h += r["d2h_bytes"]
+        out["blocks_fixed" if fixed else "as_shipped"] = {
+            "value": ps / (ms / 1e3), "unit": "particle-steps/s", "ms_per_step": ms / args.steps,
+            "launch": f"{r['blocks']} x {r['threads']} threads", "steps": int(r["steps"]),
+            "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps)}
+    ship = out["as_shipped"]
+    line.update(value=ship["value"], ms_per_step=ship["ms_per_step"],
+                reference_gpu=dict(out, sample=f"{args.particles} particles x the first {prefix} RK4 steps of the "
+                                               "workload; wall clock of the step loop (launch, synchronise, record "
+                                               "copies every 10 steps, snapshot uploads between windows)"),
+                e2e={"value": ship["value"], "unit": "particle-steps/s",
+                     "h2d_bytes_per_step": ship["h2d_bytes_per_step"],
+                     "d2h_bytes_per_step": ship["d2h_bytes_per_step"]})
     print(json.dumps(line), flush=True)
     return 0
 
@@ -283,108 +390,129 @@ def batch_accuracy(w, storage, sample, batch_final, plain_final, horizon):
     return out
 
 
-def run_batch(args, world, rank, local, pg_dist):
-    """512 seed sets, BF16 batched in one graph vs one plain FP32 run per set."""
+def run_batch(args, world, rank, local, pg_dist, storages=None):
+    """512 seed sets batched in one graph per wind storage (16-bit by default) vs one plain
+    FP32 run per set.  storages: the batched storages to measure (default: --batch-storage);
+    the first one is the headline."""
     import torch
     from pygranite_b200 import capi
     from pygranite_b200 import workloads as W
 
+    storages = list(storages or [args.batch_storage])
     w = W.BatchWorkload(n_sets=args.batch_sets, life_max=args.batch_life_max, seed=rank)
     n_snap = w.n_snapshots
-    bst = args.batch_storage
     code = {"f32": 0, "bf16": 1, "f16": 2}
-    groups, eng_b, eng_p, spans = {}, {}, {}, {}
+    groups, eng_b, eng_p, spans = {}, {bst: {} for bst in storages}, {}, {}
     for dim in (3, 2):
         seeds, lifes, sp = w.group(dim)
         if not sp:
             continue
         groups[dim] = (seeds, lifes)
         spans[dim] = sp
-        eng_b[dim] = capi.Engine(capi.settings_from_reference(w.settings(dim), ring_slots=n_snap, storage=code[bst],
-                                                              device=local, sort_interval=args.sort_interval))
-        eng_b[dim].set_seeds(seeds)
-        eng_b[dim].set_lifetimes(lifes)
+        for bst in storages:
+            e = capi.Engine(capi.settings_from_reference(w.settings(dim), ring_slots=n_snap, storage=code[bst],
+                                                         device=local, sort_interval=args.sort_interval))
+            e.set_seeds(seeds)
+            e.set_lifetimes(lifes)
+            eng_b[bst][dim] = e
         if not args.no_plain:
             eng_p[dim] = capi.Engine(capi.settings_from_reference(w.settings(dim), ring_slots=n_snap, storage=0,
                                                                   device=local, sort_interval=args.sort_interval))
     t0 = time.perf_counter()
     for k in range(n_snap):
-        for dim in eng_b:
+        for dim in groups:
             snap = w.snapshot(dim, k)
-            eng_b[dim].load_windfield(k, snap)
+            for bst in storages:
+                eng_b[bst][dim].load_windfield(k, snap)
             if dim in eng_p:
                 eng_p[dim].load_windfield(k, snap)
     load_s = time.perf_counter() - t0
     resident = lambda s: 1 if s < n_snap else 0  # noqa: E731
-
-    # ---- autotuner, then one graph over both field groups
-    tuned = {}
-    for dim, e in eng_b.items():
-        if args.tune_steps > 0:
-            r = e.tune(trial_steps=args.tune_steps)
-            tuned[f"{dim}d"] = {"layout": ["window-pair", "ring"][r.layout], "block_size": r.block_size,
-                                "sort_interval": r.sort_interval, "grid_waves": r.grid_waves,
-                                "trials": r.trials, "trial_rate": r.particle_steps_per_s}
-    batch = capi.Batch([eng_b[d] for d in sorted(eng_b)])
-    for _ in range(max(1, args.warmup)):
-        batch.run()
-    torch.cuda.synchronize()
-    if pg_dist:
-        pg_dist.barrier()
-    sampler = ClockSampler(local)
-    sampler.start()
-    time.sleep(0.3)
-    g_ms, g_ps, ps_dim = 0.0, 0, {d: 0 for d in eng_b}
-    for _ in range(args.steps):
-        batch.run()
-        st = batch.stats()
-        g_ms += st.graph_ms
-        g_ps += st.particle_steps
-        for d, e in eng_b.items():
-            ps_dim[d] += e.stats().particle_steps
-    sampler.stop()
-    clocks = sampler.summary()
-    bst_stats = batch.stats()
-    t_max, ps_all = combine_ranks(pg_dist, g_ms, g_ps, "cuda")
-    value = ps_all / (t_max / 1e3)
-
-    # ---- end to end: new host seeds every step (same counts: the graph replays), final
-    # positions and abort codes back to the host
-    e2e_s, e2e_ps, h2d, d2h = 0.0, 0, 0, 0
-    for k in range(0 if args.no_e2e else 1 + max(1, args.e2e_steps)):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for d in sorted(eng_b):
-            eng_b[d].set_seeds(groups[d][0])
-        batch.run()
-        outs = [(eng_b[d].final_positions(), eng_b[d].status()) for d in sorted(eng_b)]
-        dt = time.perf_counter() - t0
-        if k >= 1:
-            e2e_s += dt
-            e2e_ps += batch.stats().particle_steps
-            h2d = sum(groups[d][0].nbytes for d in eng_b)
-            d2h = sum(p.nbytes + s_.nbytes for p, s_ in outs)
-    assert batch.stats().captures == bst_stats.captures, "new seeds of the same counts must not capture again"
-    e_t, e_ps = combine_ranks(pg_dist, e2e_s * 1e3, e2e_ps, "cuda")
-    e2e = None if args.no_e2e else {"value": e_ps / (e_t / 1e3), "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
-           "d2h_bytes_per_step": int(d2h), "steps": max(1, args.e2e_steps),
-           "path": "capi.Engine.set_seeds (host) + capi.Batch.run + final positions / status to host"}
-
-    # ---- accuracy sample: a few sets per field, the first particles of each
+    loc = {j: (d, off, cnt) for d in spans for j, off, cnt in spans[d]}
     per_set, horizon = 64, 100
     sample = {d: [(j, min(per_set, cnt)) for j, off, cnt in spans[d] if w.sets[j]["life"] <= args.acc_life][:6]
               for d in spans}
-    batch_final, plain_final = {}, {}
-    for d in spans:
-        pos, st = eng_b[d].final_positions(), eng_b[d].status()
-        batch_final[(d, "lifetime")] = {j: (pos[off:off + cnt], st[off:off + cnt])
-                                        for j, off, cnt in spans[d] if any(j == q for q, _ in sample[d])}
-    plain_final = {(d, "lifetime"): {} for d in spans}
     sampled = {j for d in sample for j, _ in sample[d]}
 
+    results = {}
+    for bst in storages:
+        eb = eng_b[bst]
+        # ---- autotuner, then one graph over both field groups
+        tuned = {}
+        for dim, e in eb.items():
+            if args.tune_steps > 0:
+                r = e.tune(trial_steps=args.tune_steps)
+                tuned[f"{dim}d"] = {"layout": ["window-pair", "ring"][r.layout], "block_size": r.block_size,
+                                    "sort_interval": r.sort_interval, "grid_waves": r.grid_waves,
+                                    "trials": r.trials, "trial_rate": r.particle_steps_per_s}
+        batch = capi.Batch([eb[d] for d in sorted(eb)])
+        for _ in range(max(1, args.warmup)):
+            batch.run()
+        torch.cuda.synchronize()
+        if pg_dist:
+            pg_dist.barrier()
+        sampler = ClockSampler(local)
+        sampler.start()
+        time.sleep(0.3)
+        g_ms, g_ps, ps_dim = 0.0, 0, {d: 0 for d in eb}
+        for _ in range(args.steps):
+            batch.run()
+            st = batch.stats()
+            g_ms += st.graph_ms
+            g_ps += st.particle_steps
+            for d, e in eb.items():
+                ps_dim[d] += e.stats().particle_steps
+        sampler.stop()
+        clocks = sampler.summary()
+        bst_stats = batch.stats()
+        t_max, ps_all = combine_ranks(pg_dist, g_ms, g_ps, "cuda")
+        value = ps_all / (t_max / 1e3)
+
+        # ---- end to end: new host seeds every step (same counts: the graph replays), final
+        # positions and abort codes back to the host
+        e2e_s, e2e_ps, h2d, d2h = 0.0, 0, 0, 0
+        for k in range(0 if args.no_e2e else 1 + max(1, args.e2e_steps)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for d in sorted(eb):
+                eb[d].set_seeds(groups[d][0])
+            batch.run()
+            outs = [(eb[d].final_positions(), eb[d].status()) for d in sorted(eb)]
+            dt = time.perf_counter() - t0
+            if k >= 1:
+                e2e_s += dt
+                e2e_ps += batch.stats().particle_steps
+                h2d = sum(groups[d][0].nbytes for d in eb)
+                d2h = sum(p.nbytes + s_.nbytes for p, s_ in outs)
+        assert batch.stats().captures == bst_stats.captures, "new seeds of the same counts must not capture again"
+        e_t, e_ps = combine_ranks(pg_dist, e2e_s * 1e3, e2e_ps, "cuda")
+        e2e = None if args.no_e2e else {
+            "value": e_ps / (e_t / 1e3), "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "steps": max(1, args.e2e_steps),
+            "path": "capi.Engine.set_seeds (host) + capi.Batch.run + final positions / status to host"}
+        final = {}
+        for d in spans:
+            pos, st = eb[d].final_positions(), eb[d].status()
+            final[(d, "lifetime")] = {j: (pos[off:off + cnt], st[off:off + cnt])
+                                      for j, off, cnt in spans[d] if j in sampled}
+        # fixed horizon: the batch again with every lifetime capped
+        if rank == 0 and not args.no_acc and not args.no_plain:
+            for d in spans:
+                eb[d].set_lifetimes(np.minimum(groups[d][1], horizon))
+            batch.run()
+            for d in spans:
+                pos, st = eb[d].final_positions(), eb[d].status()
+                final[(d, "fixed")] = {j: (pos[off:off + cnt], st[off:off + cnt])
+                                       for j, off, cnt in spans[d] if j in sampled}
+        batch.close()
+        for e in eb.values():
+            e.close()
+        results[bst] = dict(value=value, t_max=t_max, ps_dim=ps_dim, g_ms=g_ms, clocks=clocks, stats=bst_stats,
+                            tuned=tuned, e2e=e2e, final=final)
+
     # ---- plain FP32: one run per set, sequentially, every snapshot resident
+    plain_final = {(d, h): {} for d in spans for h in ("lifetime", "fixed")}
     plain_ms, plain_ps = 0.0, 0
-    loc = {j: (d, off, cnt) for d in spans for j, off, cnt in spans[d]}
     torch.cuda.synchronize()
     wall0 = time.perf_counter()
     for j, s in enumerate([] if args.no_plain else w.sets):
@@ -404,27 +532,18 @@ def run_batch(args, world, rank, local, pg_dist):
     plain_value_wall = p_ps / (p_t / 1e3) if p_ps else None
     pd_t, _ = combine_ranks(pg_dist, plain_ms, plain_ps, "cuda")
     plain_value_dev = p_ps / (pd_t / 1e3) if p_ps else None
-
-    # fixed horizon: the batch again with every lifetime capped, and the sampled sets alone
-    acc = None
+    acc = {}
     if rank == 0 and not args.no_acc and not args.no_plain:
         for d in spans:
-            eng_b[d].set_lifetimes(np.minimum(groups[d][1], horizon))
-        batch.run()
-        for d in spans:
-            pos, st = eng_b[d].final_positions(), eng_b[d].status()
-            batch_final[(d, "fixed")] = {j: (pos[off:off + cnt], st[off:off + cnt])
-                                         for j, off, cnt in spans[d] if j in sampled}
-            plain_final[(d, "fixed")] = {}
             for j, m in sample[d]:
                 _, off, cnt = loc[j]
                 eng_p[d].set_seeds(groups[d][0][off:off + cnt])
                 eng_p[d].update_settings(maximum_simulation_time=60.0 * horizon)
                 eng_p[d].run(resident)
                 plain_final[(d, "fixed")][j] = (eng_p[d].final_positions(), eng_p[d].status())
-        acc = batch_accuracy(w, bst, sample, batch_final, plain_final, horizon)
-    batch.close()
-    for e in list(eng_b.values()) + list(eng_p.values()):
+        for bst in storages:
+            acc[bst] = batch_accuracy(w, bst, sample, results[bst]["final"], plain_final, horizon)
+    for e in eng_p.values():
         e.close()
     if pg_dist:
         pg_dist.barrier()
@@ -432,31 +551,40 @@ def run_batch(args, world, rank, local, pg_dist):
         return None
 
     peak, peak_src = load_peaks()
-    alg = sum(ps_dim[d] * RK4_FINAL_BYTES[(d, bst)] for d in ps_dim)
-    achieved = alg / (g_ms / 1e3) / 1e9 if g_ms > 0 else None
+    plain = None if args.no_plain else {
+        "storage": "f32", "value_device": plain_value_dev, "value_wall": plain_value_wall,
+        "seconds_wall": p_t / 1e3, "particle_steps": int(p_ps),
+        "path": "one capi.Engine.run per set (set_seeds, MaximumSimulationTime = lifetime * 60 s)"}
+    per = {}
+    for bst in storages:
+        r = results[bst]
+        alg = sum(r["ps_dim"][d] * RK4_FINAL_BYTES[(d, bst)] for d in r["ps_dim"])
+        achieved = alg / (r["g_ms"] / 1e3) / 1e9 if r["g_ms"] > 0 else None
+        per[bst] = {
+            "value": r["value"], "ms_per_step": r["t_max"] / args.steps,
+            "speedup_vs_plain_f32": r["value"] / plain_value_wall if plain_value_wall else None,
+            "speedup_vs_plain_f32_device": r["value"] / plain_value_dev if plain_value_dev else None,
+            "accuracy": acc.get(bst), "e2e": r["e2e"], "tuned": r["tuned"], "graph_nodes": r["stats"].nodes,
+            "clocks": r["clocks"],
+            "gpu_launches": int((r["stats"].kernel_launches + r["stats"].aux_launches) * args.steps),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": None, "peak_source": peak_src,
+                         "bytes_per_particle_step": {f"{d}d": RK4_FINAL_BYTES[(d, bst)] for d in r["ps_dim"]},
+                         "kernel": "advance_kernel (graph replay, whole run)"}}
+    head = per[storages[0]]
     return {
-        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": t_max / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": bst,
+        "metric": "particle-steps/s", "value": head["value"], "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(1, args.warmup), "ms_per_step": head["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": storages[0],
         "data": "synthetic (seeded Fourier-mode fields, 3D 192x192x64 and 2D 1024x512)",
         "config": {"workload": BATCH_WORKLOAD, "sets": len(w.sets),
                    "particles_per_gpu": int(sum(s["n"] for s in w.sets)),
                    "sets_3d": int(sum(s["dim"] == 3 for s in w.sets)), "snapshots": n_snap,
-                   "lifetimes": [100, args.batch_life_max], "storage": bst, "parallelism": f"replicas{world}",
-                   "l2": f"inputs larger than L2 ({n_snap} snapshots per field resident)", "tuned": tuned,
-                   "graph_nodes": bst_stats.nodes},
-        "plain": None if args.no_plain else {
-            "storage": "f32", "value_device": plain_value_dev, "value_wall": plain_value_wall,
-            "seconds_wall": p_t / 1e3, "particle_steps": int(p_ps),
-            "path": "one capi.Engine.run per set (set_seeds, MaximumSimulationTime = lifetime * 60 s)"},
-        "speedup_vs_plain_f32": value / plain_value_wall if plain_value_wall else None,
-        "speedup_vs_plain_f32_device": value / plain_value_dev if plain_value_dev else None,
-        "accuracy": acc, "e2e": e2e,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None, "peak_source": peak_src,
-                     "bytes_per_particle_step": {f"{d}d": RK4_FINAL_BYTES[(d, bst)] for d in ps_dim},
-                     "kernel": "advance_kernel (graph replay, whole run)"},
-        "clocks": clocks, "gpu_launches": int((bst_stats.kernel_launches + bst_stats.aux_launches) * args.steps),
+                   "lifetimes": [100, args.batch_life_max], "storages": storages, "parallelism": f"replicas{world}",
+                   "l2": f"inputs larger than L2 ({n_snap} snapshots per field resident)"},
+        "plain": plain, "per_storage": per,
+        "speedup_vs_plain_f32": head["speedup_vs_plain_f32"], "accuracy": head["accuracy"], "e2e": head["e2e"],
+        "roofline": head["roofline"], "clocks": head["clocks"], "gpu_launches": head["gpu_launches"],
         "load_s": load_s,
     }
 
@@ -480,7 +608,7 @@ def run_precision(args, world, rank, local, pg_dist):
     field = W.FourierField((64, 192, 192), (250.0, 1000.0, 1000.0), n_modes=32, seed=rank)
     fld = capi.Field.fourier(field, 600.0, n_snap, device=local)
     # record r >= 1 holds the state after 100 (r - 1) + 1 steps (records after every 100th step)
-    checks = [r for r in (2, 11, 50) if 100 * (r - 1) + 1 <= steps]
+    checks = [r for r in (2, 5, 11, 50) if 100 * (r - 1) + 1 <= steps]
     forms = {"f32": dict(storage=0), "bf16": dict(storage=1, compensated=1, time_mode=1),
              "f16": dict(storage=2, compensated=1, time_mode=1)}
     out, hist = {}, {}
@@ -555,6 +683,49 @@ def run_precision(args, world, rank, local, pg_dist):
 SERVE_WORKLOAD = "serve-poisson-3d-512x512x96"
 
 
+def serve_sample(w, count):
+    """Requests checked against the float64 oracle: the shortest ones of each integrator that
+    end inside the field; returns their indices and the snapshots they read."""
+    clock = int(round(600.0 * (w.n_snapshots - 1) / 60.0))
+    picks = []
+    for integ in (1, 0):
+        cand = [j for j in range(len(w.arrivals)) if w.integrators[j] == integ
+                and int(np.floor(w.starts[j] / 60.0 + 1e-9)) + int(w.steps[j]) <= clock]
+        cand.sort(key=lambda j: (int(w.steps[j]), int(w.counts[j])))
+        picks += cand[:max(1, count // 2)]
+    keep = set()
+    for j in picks:
+        k0 = int(np.floor(w.starts[j] / 60.0 + 1e-9))
+        first, last = k0 // 10, (k0 + int(w.steps[j])) // 10 + 1
+        keep.update(range(first, min(last, w.n_snapshots - 1) + 1))
+    return picks, keep
+
+
+def serve_accuracy(w, results, host_snaps, storage, m=256):
+    """Final-position error in grid cells of sampled served requests against the float64
+    oracle on the same float32 snapshots (the oracle's clock starts every particle at the
+    request's start step, as the server's does)."""
+    from oracle import oracle as orc
+    cell = CELL_3D
+    any_snap = next(iter(host_snaps.values()))
+    wind = [host_snaps.get(k, any_snap) for k in range(w.n_snapshots)]   # unread windows: placeholders
+    out = []
+    for j, (pos, status, k0, steps) in sorted(results.items()):
+        seeds = w.seeds(j)[:m]
+        st = orc.settings(**dict(w.settings(), Integrator=int(w.integrators[j])))
+        ref = orc.run(st, orc.Inputs(wind=wind, seeds=seeds), precision="f64", start_step=int(k0),
+                      step_limit=int(k0 + steps), threads=os.cpu_count() or 1)
+        both = (ref["status"] == 0) & (status[:m] == 0)
+        d = (np.abs(pos[:m].astype(np.float64) - ref["trajectories"][:, -1]) / cell).max(axis=1)[both]
+        out.append({"request": int(j), "integrator": ["euler", "rk4"][int(w.integrators[j])], "start_step": int(k0),
+                    "steps": int(steps), "particles": int(d.size),
+                    "cell_rms": float(np.sqrt(np.mean(d ** 2))) if d.size else None,
+                    "cell_max": float(d.max()) if d.size else None,
+                    "status_mismatch": int(np.sum(ref["status"] != status[:m]))})
+    return {"vs_f64": out, "storage": storage,
+            "note": "served result (" + storage + " wind) against the float64 oracle on the float32 snapshots"}
+
+
 def run_serve(args, world, rank, local, pg_dist):
     """Requests arrive as a Poisson stream; latency = submit -> results on the host."""
     import torch
@@ -567,11 +738,17 @@ def run_serve(args, world, rank, local, pg_dist):
     t0 = time.perf_counter()
     srv = capi.Server(capi.settings_from_reference(w.settings(), storage=code, device=local), w.n_snapshots, w.grid,
                       hbm_budget=int(args.serve_budget_gb * (1 << 30)))
+    # accuracy sample: the shortest RK4 and Euler requests that end inside the field; the
+    # float32 snapshots they read are kept on the host for the float64 oracle
+    acc_req, keep = serve_sample(w, args.serve_acc) if rank == 0 else ([], set())
+    host_snaps = {}
     dev = W.DeviceFourierField(w.field, device=f"cuda:{local}")
     for k in range(w.n_snapshots):
         planes = dev.snapshot(600.0 * k)
         torch.cuda.synchronize()
         srv.set_snapshot_device(k, [p.data_ptr() for p in planes])
+        if k in keep:
+            host_snaps[k] = [p.cpu().numpy() for p in planes]
     del dev
     torch.cuda.empty_cache()
     setup_s = time.perf_counter() - t0
@@ -596,8 +773,8 @@ def run_serve(args, world, rank, local, pg_dist):
             time.sleep(delay)
         ids.append(srv.submit(sd, float(w.starts[j]), int(w.steps[j]), int(w.integrators[j])))
     submit_end = time.perf_counter() - start
-    lat, queue, nparts, steps_run = [], [], 0, 0
-    for rid in ids:
+    lat, queue, nparts, steps_run, acc_out = [], [], 0, 0, {}
+    for j, rid in enumerate(ids):
         st = srv.wait(rid, 600.0)
         info = srv.info(rid)
         if st == capi.GR_REQ_DONE:
@@ -605,6 +782,9 @@ def run_serve(args, world, rank, local, pg_dist):
             queue.append(info.admit_s - info.submit_s)
             nparts += info.n
             steps_run += info.steps
+            if j in acc_req:
+                pos, status = srv.result(rid)[:2]
+                acc_out[j] = (pos, status, info.start_step, info.steps)
         srv.release(rid)
     wall = time.perf_counter() - start
     sampler.stop()
@@ -620,6 +800,7 @@ def run_serve(args, world, rank, local, pg_dist):
         return None
     lat, queue = np.array(lat), np.array(queue)
     pct = lambda a, q: float(np.percentile(a, q)) if a.size else None  # noqa: E731
+    accuracy = serve_accuracy(w, acc_out, host_snaps, args.serve_storage) if acc_out else None
     return {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
         "steps": 1, "warmup": 3, "ms_per_step": t_max, "higher_is_better": True, "scaling": "weak",
@@ -632,7 +813,7 @@ def run_serve(args, world, rank, local, pg_dist):
                    "l2": "window pair 403 MB > L2: streamed from HBM"},
         "latency_s": {"p50": pct(lat, 50), "p90": pct(lat, 90), "p99": pct(lat, 99), "max": pct(lat, 100),
                       "mean": float(lat.mean()) if lat.size else None},
-        "queue_s": {"p50": pct(queue, 50), "p99": pct(queue, 99)},
+        "queue_s": {"p50": pct(queue, 50), "p99": pct(queue, 99)}, "accuracy": accuracy,
         "server": {"windows": s1.windows, "sweeps": s1.sweeps, "jumps": s1.jumps, "deferred": s1.deferred,
                    "peak_particles": s1.peak_particles, "capacity_particles": s1.capacity_particles,
                    "steps_requested_mean": float(np.mean(w.steps)), "steps_run_mean": steps_run / max(1, lat.size),
@@ -642,6 +823,32 @@ def run_serve(args, world, rank, local, pg_dist):
                 "path": "capi.Server.submit (host seeds) -> results on the host; wall clock over the stream"},
         "roofline": None, "clocks": clocks, "gpu_launches": None,
     }
+
+
+def run_forms(args, world, rank, local):
+    """The three forms beside the plain kernel, on one GPU, each its own phase after the plain
+    measurement: batching (BF16 and FP16 graphs against one plain FP32 run per set), serving
+    (the Poisson request stream) and precision (the 4e6-particle, 5,000-step configuration per
+    storage).  A form that fails reports its error instead of a figure."""
+    import copy
+    import traceback
+    import torch
+    forms = {}
+    for name, fn, kw in (("precision", run_precision, {}), ("batch", run_batch, {"storages": ["bf16", "f16"]}),
+                         ("serve", run_serve, {})):
+        a = copy.copy(args)
+        a.steps, a.warmup = min(args.steps, 5), min(args.warmup, 2)
+        t0 = time.perf_counter()
+        try:
+            forms[name] = fn(a, world, rank, local, None, **kw)
+        except Exception as exc:  # reported in the line; the plain figures stand
+            forms[name] = {"error": f"{type(exc).__name__}: {exc}", "trace": traceback.format_exc()[-2000:]}
+        if isinstance(forms[name], dict):
+            forms[name]["phase_s"] = time.perf_counter() - t0
+        gc.collect()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return forms
 
 
 def main():
@@ -727,6 +934,21 @@ def main():
     # max over ranks of the device time, sum of the particle-steps
     t_max, ps_all = combine_ranks(pg_dist, tot_ms, ps, "cuda")
     value = ps_all / (t_max / 1e3)
+
+    # ---------------- the timed run's own output against the oracle (after the timed region):
+    # a fixed sample of particle ids spread over the seed array, every record
+    parity, ids, refs = None, None, None
+    if args.parity_sample > 0 and rank == 0 and storage == 0:
+        res = eng.results(pinned=True)
+        ids = sample_ids(seeds.shape[0], args.parity_sample)
+        got = {"trajectories": np.array(res["trajectories"][ids]), "status": res["status"][ids],
+               "total_curvature": res["total_curvature"][ids], "volume": np.array(res["volume_info"][0][ids]),
+               "expression": np.array(res["compute_info"][0][ids])}
+        del res
+        gc.collect()
+        refs = plain_oracle(settings, src, seeds, ids)
+        parity = check_plain(got, *refs)
+        parity["run"] = "the last timed run (device-resident engine)"
     eng.close()
 
     # ---------------- end to end through the pygranite API (host snapshots, 3-slot ring)
@@ -742,7 +964,7 @@ def main():
                      CurvatureMode=pg.CurvatureMode)
         h2d = seeds.nbytes + sum(p.nbytes for snap in src.wind for p in snap) + src.volumes[0]["T"].nbytes
 
-        def e2e_run(source, pinned_results):
+        def e2e_run(source, pinned_results, check):
             s = W.apply_settings(pg.IntegratorSettings(), settings, enums)
             s.WindStorage = [pg.WindStorage.Float32, pg.WindStorage.BFloat16, pg.WindStorage.Float16][storage]
             s.Device = local
@@ -750,7 +972,7 @@ def main():
             s.StepsPerLaunch = args.steps_per_launch
             s.WindLayout = args.layout
             s.PinnedResults = pinned_results
-            e_ps, e_s, d2h, reps = 0, 0.0, 0, []
+            e_ps, e_s, d2h, reps, par = 0, 0.0, 0, [], None
             for k in range(1 + args.e2e_steps):
                 gc.collect()   # the previous step's garbage, outside the timed region
                 torch.cuda.synchronize()
@@ -772,14 +994,25 @@ def main():
                              "total_ms": round(1e3 * dt, 1)})
                 if k >= 1:
                     e_s += dt
-                    e_ps += info.particle_steps
+                    e_ps += res.particleSteps()   # counted by this run's own engine
                     d2h = res.trajectories().nbytes + res.computeInfo(0).nbytes + res.volumeInfo("T").nbytes + \
                         res.totalCurvatures().nbytes + 4 * seeds.shape[0]
+                if check and k == args.e2e_steps and refs is not None:
+                    # the last timed step's TrajectorySet, through the reference's accessors
+                    got = {"trajectories": res.trajectories()[ids],
+                           "status": np.array([int(r) for r in res.abortReasons()], np.int32)[ids],
+                           "total_curvature": np.asarray(res.totalCurvatures())[ids],
+                           "volume": res.volumeInfo("T")[ids], "expression": res.computeInfo(0)[ids]}
+                    par = check_plain(got, *refs)
+                    par["run"] = "the last timed pygranite-API run (TrajectorySet accessors)"
                 del res
             e_t, e_psa = combine_ranks(pg_dist, e_s, e_ps, "cuda")
-            return {"value": e_psa / e_t, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "steps": args.e2e_steps,
-                    "ms_per_step": 1e3 * e_t / max(1, args.e2e_steps), "reps": reps}
+            out = {"value": e_psa / e_t, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
+                   "d2h_bytes_per_step": int(d2h), "steps": args.e2e_steps,
+                   "ms_per_step": 1e3 * e_t / max(1, args.e2e_steps), "particle_steps": int(e_psa), "reps": reps}
+            if par is not None:
+                out["parity"] = par
+            return out
 
         # the same snapshots and volume, copied once into page-locked memory (data preparation,
         # outside the timed region)
@@ -792,10 +1025,10 @@ def main():
         pinned_T[...] = src.volumes[0]["T"]
         psrc = W.SnapshotSource([[pinned_wind[k, c] for c in range(3)] for k in range(n_snap)],
                                 volumes=[{"T": pinned_T}])
-        e2e = e2e_run(psrc, True)
+        e2e = e2e_run(psrc, True, True)
         e2e["host_buffers"] = "page-locked: loader arrays from pinned_empty, IntegratorSettings.PinnedResults = True"
         if world == 1:
-            e2e["pageable"] = e2e_run(src, False)
+            e2e["pageable"] = e2e_run(src, False, False)
             e2e["pageable"]["host_buffers"] = "pageable numpy loader arrays, results in fresh numpy arrays (the defaults)"
         else:
             # N processes share one host: the pageable variant's extra 4 GB per rank is left out
@@ -845,30 +1078,45 @@ def main():
 
     peak, peak_src = load_peaks()
     bpps = BYTES_PER_PARTICLE_STEP[args.storage]
+    avg_launch_ms = kern_ms / max(launches, 1)
+    ps_launch = ps / max(launches, 1)
     achieved = ps * bpps / (kern_ms / 1e3) / 1e9 if kern_ms > 0 else None
-    tpps = load_traffic_per_particle_step(args.storage)
+    prof = load_kernel_profile(args.storage)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None,
-                "traffic": (tpps * ps / max(launches, 1)) if tpps else None,
+                "traffic": (prof["dram_bytes_per_particle_step"] * ps_launch) if prof else None,
                 "peak_source": peak_src, "bytes_per_particle_step": bpps,
-                "kernel": "advance_kernel<3,RK4>", "avg_launch_ms": kern_ms / max(launches, 1),
-                "particle_steps_per_launch": ps / max(launches, 1)}
+                "bytes_note": "gather-equivalent: every corner of every stage counted as if fetched from HBM; the "
+                              "window pair is L2-resident, so this fraction can exceed 1",
+                "kernel": "advance_kernel<3,RK4,Pair<float>>", "avg_launch_ms": avg_launch_ms,
+                "particle_steps_per_launch": ps_launch}
+    if prof:
+        rate = ps / (kern_ms / 1e3)                 # particle-steps per second of step-kernel time
+        dram_gbs = prof["dram_bytes_per_particle_step"] * rate / 1e9
+        sm_mhz = clocks.get("sm_mhz") or 1965.0
+        issue_peak = 148 * 4 * sm_mhz * 1e6         # warp instructions per second, 4 schedulers per SM
+        issue = prof["warp_inst_per_particle_step"] * rate
+        roofline.update(dram_gbs=dram_gbs, dram_frac=dram_gbs / peak, issue_frac=issue / issue_peak,
+                        active_bound="issue (instruction throughput)" if issue / issue_peak > dram_gbs / peak
+                        else "hbm", profile=prof.get("source"))
     cpu = None
     if not args.no_cpu and world == 1:
         cpu = cpu_baseline(args, settings, src, seeds)
+    del src
+    gc.collect()
+    forms = None
+    if world == 1 and not args.no_forms:
+        forms = run_forms(args, world, rank, local)
+    cfg = plain_config(args, world)
     line = {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": args.storage, "data": "synthetic (seeded Fourier-mode field)",
-        "config": {"workload": WORKLOAD, "particles_per_gpu": args.particles, "sim_steps": args.sim_steps,
-                   "snapshots": n_snap, "grid": [192, 192, 64], "storage": args.storage,
-                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (201 snapshots, 7.6 GB ring)",
-                   "records": int(info.records), "steps_run": int(info.steps),
-                   "sort_interval": args.sort_interval, "steps_per_launch": args.steps_per_launch,
-                   "wind_layout": ["window-pair", "ring"][args.layout]},
-        "e2e": e2e, "native_loader": native, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-        "gpu_launches": int(launches + aux), "wall_s": wall,
+        "dtype": args.storage, "data": "synthetic (seeded Fourier-mode field)", "config": cfg,
+        "run": {"records": int(info.records), "steps_run": int(info.steps),
+                "particle_steps_per_run": int(ps / max(1, args.steps))},
+        "parity": parity, "e2e": e2e, "native_loader": native, "roofline": roofline, "cpu_baseline": cpu,
+        "clocks": clocks, "gpu_launches": int(launches + aux), "wall_s": wall, "forms": forms,
     }
     print(json.dumps(line), flush=True)
     if pg_dist:

@@ -414,25 +414,31 @@ int gr_field_snapshot(gr_field *field, int64_t snapshot, float *out, int64_t cap
 void gr_field_destroy(gr_field *field);
 
 /* Allocation-free advance of particles between two snapshots.  No counterpart in the
- * reference: it exists for callers that cannot call cudaMalloc — code running while a CUDA
- * graph is being captured, hosts whose device memory belongs to their own pool allocator,
- * real-time loops that forbid allocation after start-up.  It allocates no device memory and
- * calls no allocating routine; the caller owns every input and output buffer:
+ * reference.  It exists for callers that cannot call cudaMalloc: plug-in hosts whose device
+ * memory belongs to their own pool allocator (an allocation behind its back escapes the host's
+ * accounting and limits), and real-time loops that forbid allocation after start-up (an
+ * allocation may synchronise the device or take an unbounded time).  It allocates no device
+ * memory and calls no allocating routine; the caller owns every input and output buffer:
  *   wind_back / wind_front: the two snapshots, node-major (z, y, x), float4 {u, v, w, 0}
  *     per node in 3D or float2 {u, v} in 2D, on the device;
  *   px, py, pz, status: particle positions and abort codes (0 = alive), device arrays of n,
  *     updated in place; pz unused in 2D.
- * It runs `steps` integrator steps starting at time_start inside the window
- * [time_back, time_front], with the reference's float32 time arithmetic, and writes the
- * particle-steps done to *particle_steps (if non-null; this synchronises `stream`).  Only the
- * plain integrator: Euler / RK4, Reverse, border modes, sphere coordinates; no curvature,
- * volumes, constants, uplift, topography or length abort, float32 storage (GR_ERR_USER
- * otherwise).
+ * It runs `steps` integrator steps starting at time_start, which must lie in
+ * [time_back, time_front), with the reference's float32 time arithmetic (T = T + DeltaT; a
+ * step that ends past time_front extrapolates the weights, as the reference's last step of a
+ * window does), and writes the particle-steps done to *particle_steps (if non-null; this
+ * synchronises `stream`).  Only the plain integrator: Euler / RK4 with dynamic wind, Reverse,
+ * border modes, sphere coordinates, ReferenceFilter; no curvature, volumes, constants, uplift,
+ * topography, length abort, MinimumAliveParticles, constant wind, 16-bit storage, Kahan
+ * positions or float64 time weights (GR_ERR_USER otherwise).
  * Its scratch (the per-step time weights and two counters, GR_NOALLOC_SCRATCH_BYTES) is one
  * file-scope device array that every GPU loading the library holds until the process exits;
  * steps beyond GR_NOALLOC_MAX_STEPS are rejected.  The first call on a device looks up that
- * array's device address, so make it before any stream capture.  All calls share the array:
- * calls whose work overlaps on the GPU (different streams, no ordering) race. */
+ * array's device address (cudaGetSymbolAddress) and keeps it for the life of the process, so
+ * make that first call before any stream capture; a cudaDeviceReset between calls is not
+ * supported.  Each call rebuilds the weights and clears the counters on `stream` before its
+ * step kernel.  All calls share the array: calls whose work overlaps on the GPU (different
+ * streams, no ordering between them) race. */
 #define GR_NOALLOC_MAX_STEPS 4096
 #define GR_NOALLOC_SCRATCH_BYTES (GR_NOALLOC_MAX_STEPS * 48 + 16)
 int gr_advance_noalloc(const gr_settings *settings, int64_t nz, int64_t ny, int64_t nx,

@@ -71,6 +71,8 @@ typedef struct {
     int64_t step_limit;            /* >= 0: stop after this many steps (bounded timing sample) */
     int32_t filter_weights;        /* 0: exact filter fractions; 1 / 2: fractions rounded / truncated
                                       to 1/256 like texture hardware (reference GPU comparisons) */
+    int64_t start_step;            /* particles integrate from this step of the clock on (a request
+                                      joining mid-run); earlier steps leave them where they are */
 } or_input;
 
 typedef struct {

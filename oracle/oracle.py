@@ -58,6 +58,7 @@ class OrInput(ctypes.Structure):
         ("expr", ctypes.POINTER(ctypes.POINTER(_Node))), ("expr_len", ctypes.POINTER(ctypes.c_int32)),
         ("n", ctypes.c_int64), ("seeds", _FP), ("threads", ctypes.c_int32),
         ("step_limit", ctypes.c_int64), ("filter_weights", ctypes.c_int32),
+        ("start_step", ctypes.c_int64),
     ]
 
 
@@ -162,7 +163,8 @@ def _ptr(a):
     return a.ctypes.data_as(_FP)
 
 
-def _build_input(s: dict, data: Inputs, time_mode=0, threads=0, step_limit=-1, compensated=False, filter_weights=0):
+def _build_input(s: dict, data: Inputs, time_mode=0, threads=0, step_limit=-1, compensated=False, filter_weights=0,
+                 start_step=0):
     keep = []
     dim = 3 if s["Space"] == 0 else 2
     seeds = np.ascontiguousarray(data.seeds, dtype=np.float32)
@@ -256,6 +258,7 @@ def _build_input(s: dict, data: Inputs, time_mode=0, threads=0, step_limit=-1, c
     inp.threads = threads
     inp.step_limit = step_limit
     inp.filter_weights = filter_weights
+    inp.start_step = start_step
     meta = dict(dim=dim, n=n, vol_names=vol_names, n_expr=len(exprs), grid=(nx, ny, nz),
                 scale=scale, offset=offset, domain=domain)
     return inp, keep, meta
@@ -275,10 +278,13 @@ def schedule(s: dict, data: Inputs, time_mode=0):
 
 
 def run(s: dict, data: Inputs, precision="f64", time_mode=0, threads=0, step_limit=-1, compensated=False,
-        filter_weights=0) -> dict:
+        filter_weights=0, start_step=0) -> dict:
     """Runs the oracle; returns outputs in the reference's accessor shapes.  filter_weights: 0 exact
-    filter fractions, 1 / 2 fractions rounded / truncated to 1/256 (texture-hardware readings)."""
-    inp, keep, meta = _build_input(s, data, time_mode, threads, step_limit, compensated, filter_weights)
+    filter fractions, 1 / 2 fractions rounded / truncated to 1/256 (texture-hardware readings).
+    start_step > 0: the particles stay put until that step of the clock, then integrate (a request
+    that joins a running clock; the reference has no such form)."""
+    inp, keep, meta = _build_input(s, data, time_mode, threads, step_limit, compensated, filter_weights,
+                                   start_step)
     n, dim = meta["n"], meta["dim"]
     windows = ctypes.c_int64(0)
     k = lib().oracle_schedule(ctypes.byref(inp), None, 0, ctypes.byref(windows))

@@ -70,6 +70,9 @@ typedef struct {
     double loop_ms;               // wall time of the step loop
     int32_t threads, blocks;
     char message[256];
+    int32_t count_steps;          // 1: count the particle-steps (alive particles at each launch)
+    int64_t particle_steps;       // counted when count_steps
+    int64_t h2d_bytes, d2h_bytes; // copies made inside the step loop
 } ref_args;
 
 }  // extern "C"
@@ -84,6 +87,16 @@ namespace {
             return 1;                                                                               \
         }                                                                                           \
     } while (0)
+
+// Particles alive (status Time) before a launch, summed into *out: the particle-steps of that
+// launch.  The harness's own bookkeeping, not part of the reference.
+__global__ void count_alive_kernel(const AbortReason *status, int64_t n, unsigned long long *out) {
+    unsigned c = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        c += status[i] == AbortReason::Time ? 1u : 0u;
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, (unsigned long long)c);
+}
 
 struct Tex {
     cudaTextureObject_t obj = 0;
@@ -173,11 +186,15 @@ int run(ref_args *a) {
     Tex wind[3][3];   // [slot][component]
     Tex vol;
     int back = 0, front = 1, cache = 2;
+    a->h2d_bytes = a->d2h_bytes = 0;
+    a->particle_steps = 0;
+    const int64_t plane_bytes = a->nx * a->ny * (DIM == 3 ? a->nz : 1) * (int64_t)sizeof(float);
     auto load_snapshot = [&](int slot, int s) -> int {
         for (int c = 0; c < DIM; ++c) {
             const float *h = a->wind[(int64_t)s * DIM + c];
             if ((DIM == 3 ? load3(a, wind[slot][c], h) : load2(a, wind[slot][c], h))) return 1;
         }
+        a->h2d_bytes += DIM * plane_bytes;
         return 0;
     };
     // initializeData (cpp:146-259): snapshot 0, the constant volume, then one loader step
@@ -247,12 +264,14 @@ int run(ref_args *a) {
         VEC_T *f = buf[swap_index];
         if (a->records < a->max_records) {
             RCK(cudaMemcpy(a->positions + a->records * n * DIM, f, n * sizeof(VEC_T), cudaMemcpyDeviceToHost));
+            a->d2h_bytes += n * sizeof(VEC_T);
         }
         a->records++;
         if (extras) {
             if (a->info_records < a->max_records) {
                 RCK(cudaMemcpy(a->compute_info + a->info_records * n, cinfo, n * sizeof(float), cudaMemcpyDeviceToHost));
                 RCK(cudaMemcpy(a->volume_info + a->info_records * n, vinfo, n * sizeof(float), cudaMemcpyDeviceToHost));
+                a->d2h_bytes += 2 * n * sizeof(float);
             }
             a->info_records++;
         }
@@ -261,6 +280,13 @@ int run(ref_args *a) {
     // record 0 = the seeds
     if (a->max_records > 0) memcpy(a->positions, a->seeds, n * sizeof(VEC_T));
     a->records = 1;
+
+    unsigned long long *steps_dev = nullptr;
+    if (a->count_steps) {
+        RCK(cudaMalloc(&steps_dev, sizeof(unsigned long long)));
+        RCK(cudaMemset(steps_dev, 0, sizeof(unsigned long long)));
+    }
+    a->h2d_bytes = 0;   // copies before the loop are set-up, not counted
 
     // computeLoop_ / computeLoopGPU_ (tpp:778-995)
     float time = 0.f, max_wt = a->data_time_distance;
@@ -281,6 +307,7 @@ int run(ref_args *a) {
             swap_index = (swap_index + 1) % 2;
             d.FrontParticles = buf[swap_index];
             d.BackParticles = buf[(swap_index + 1) % 2];
+            if (steps_dev) count_alive_kernel<<<148 * 4, 256>>>(status, (int64_t)n, steps_dev);
             launch<VEC_T>(a->variant, blocks, threads, d);
             RCK(cudaDeviceSynchronize());
             RCK(cudaGetLastError());
@@ -309,6 +336,12 @@ int run(ref_args *a) {
         if (save(d.Time > 0)) return 1;
     a->loop_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
     a->steps = (int64_t)sim;
+    if (steps_dev) {
+        unsigned long long c = 0;
+        RCK(cudaMemcpy(&c, steps_dev, sizeof c, cudaMemcpyDeviceToHost));
+        a->particle_steps = (int64_t)c;
+        cudaFree(steps_dev);
+    }
     RCK(cudaMemcpy(a->status, status, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
     if (extras && a->total_curvature) RCK(cudaMemcpy(a->total_curvature, tc, n * sizeof(float), cudaMemcpyDeviceToHost));
 

@@ -39,6 +39,8 @@ class RefArgs(ctypes.Structure):
         ("records", ctypes.c_int64), ("info_records", ctypes.c_int64), ("steps", ctypes.c_int64),
         ("windows", ctypes.c_int64), ("loop_ms", ctypes.c_double), ("threads", ctypes.c_int32),
         ("blocks", ctypes.c_int32), ("message", ctypes.c_char * 256),
+        ("count_steps", ctypes.c_int32), ("particle_steps", ctypes.c_int64),
+        ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
     ]
 
 
@@ -46,7 +48,7 @@ def available() -> bool:
     return os.path.exists(LIB_PATH)
 
 
-def run(settings: dict, wind, seeds, volume=None, blocks_fixed=False, step_limit=-1):
+def run(settings: dict, wind, seeds, volume=None, blocks_fixed=False, step_limit=-1, count_steps=False):
     """settings: reference IntegratorSettings fields (as in oracle.oracle.settings).  The
     variant is chosen from them: 2D Euler plain, 3D RK4 + TotalCurvature + one constant
     volume + one expression, 3D RK4 plain, or 3D Euler plain."""
@@ -64,6 +66,7 @@ def run(settings: dict, wind, seeds, volume=None, blocks_fixed=False, step_limit
     else:
         a.variant = 2
     a.blocks_fixed = int(blocks_fixed)
+    a.count_steps = int(count_steps)
     a.delta_t = settings["DeltaT"]
     a.data_time_distance = settings["DataTimeDistance"]
     a.maximum_simulation_time = settings["MaximumSimulationTime"]
@@ -122,4 +125,5 @@ def run(settings: dict, wind, seeds, volume=None, blocks_fixed=False, step_limit
     return dict(trajectories=np.ascontiguousarray(pos[:L].transpose(1, 0, 2)), status=st,
                 total_curvature=tc, volume_info=np.ascontiguousarray(vi[:Li].T),
                 compute_info=np.ascontiguousarray(ci[:Li].T), steps=a.steps, windows=a.windows,
-                loop_ms=a.loop_ms, threads=a.threads, blocks=a.blocks)
+                loop_ms=a.loop_ms, threads=a.threads, blocks=a.blocks, particle_steps=a.particle_steps,
+                h2d_bytes=a.h2d_bytes, d2h_bytes=a.d2h_bytes)

@@ -1,8 +1,9 @@
 // noalloc.cu — gr_advance_noalloc: advancing particles without allocating device memory.
 //
-// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is being captured,
-// plug-in hosts whose device memory belongs to their own pool allocator, real-time loops that
-// forbid allocation after start-up.  This entry point gives them the plain integrator (Euler
+// Some callers cannot call cudaMalloc: plug-in hosts whose device memory belongs to their own
+// pool allocator (a cudaMalloc there would go around the host's accounting and limits), and
+// real-time loops that forbid allocation after start-up (an allocation may synchronise the
+// device or take an unbounded time).  This entry point gives them the plain integrator (Euler
 // or RK4 between two snapshots, the border checks and abort codes) on buffers they own.  Its
 // only scratch, the per-step time weights and two counters, is the file-scope array below:
 // every GPU that loads the library keeps these GR_NOALLOC_SCRATCH_BYTES until the process
@@ -37,11 +38,38 @@ static __device__ __align__(256) NoAllocScratch g_scratch;
 constexpr int MAX_DEVICES = 64;
 std::mutex g_mutex;
 NoAllocScratch *g_scratch_ptr[MAX_DEVICES] = {};   // device address of g_scratch, per device
-StepEntry g_host_sched[GR_NOALLOC_MAX_STEPS];       // host staging of the weights (under g_mutex)
 
 int err(int code, const char *msg) {
     set_last_error(msg);   // reported by gr_last_error()
     return code;
+}
+
+// Time weights of `steps` steps from time_start, with the float32 arithmetic of
+// TrajectoryIntegrator.tpp:126-144 (the file is built with --fmad=false, so nothing is
+// contracted).  The time accumulator T = T + h is a dependent chain: thread 0 walks it and
+// parks each step's start time in t0; then the block turns the start times into the weights.
+__global__ void __launch_bounds__(256) noalloc_schedule_kernel(NoAllocScratch *S, float time_back, float time_front,
+                                                               float time_start, float h, int32_t steps) {
+    if (threadIdx.x == 0) {
+        float T = time_start;
+        for (int k = 0; k < steps; ++k) {
+            S->sched[k].t0 = T;
+            T = T + h;
+        }
+        S->counters[0] = 0ull;   // the counters keep the previous call's values: clear them
+        S->counters[1] = 0ull;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < steps; k += blockDim.x) {
+        StepEntry E{};
+        const float T = S->sched[k].t0;
+        E.t0 = (T - time_back) / (time_front - time_back);
+        E.t1 = ((T + 0.5f * h) - time_back) / (time_front - time_back);
+        E.t2 = ((T + h) - time_back) / (time_front - time_back);
+        E.slot_back = 0;
+        E.slot_front = 1;
+        S->sched[k] = E;
+    }
 }
 
 // The plain step loop of advance_kernel (granite_kernels.cuh) with the same arithmetic:
@@ -167,11 +195,15 @@ extern "C" int gr_advance_noalloc(const gr_settings *s, int64_t nz, int64_t ny, 
         return err(GR_ERR_USER, "ERROR < USER INPUT | steps must be between 0 and GR_NOALLOC_MAX_STEPS (4096) >");
     if (n < 0 || n > 0x7fffffffLL) return err(GR_ERR_USER, "ERROR < USER INPUT | invalid particle count >");
     if (s->curvature_mode != 0 || s->volume_mode != 0 || s->constants_mode != 0 || (dim == 3 && s->uplift_mode != 0) ||
-        s->abort_mode != 0 || s->storage != GR_STORE_F32 || s->compensated)
+        s->abort_mode != 0 || s->storage != GR_STORE_F32 || s->compensated || s->windfield_mode != 1 ||
+        s->time_mode != 0 || s->minimum_alive > 0)
         return err(GR_ERR_USER, "ERROR < USER INPUT | the allocation-free entry point runs the plain integrator only "
-                                "(no curvature, volumes, constants, uplift, length abort; float32 storage) >");
+                                "(dynamic wind, float32 storage and time weights; no curvature, volumes, constants, "
+                                "uplift, length abort or MinimumAliveParticles) >");
     if (!(s->delta_t > 0.f) || !(time_front > time_back))
         return err(GR_ERR_USER, "ERROR < USER INPUT | DeltaT must be positive and time_front > time_back >");
+    if (!(time_start >= time_back) || !(time_start < time_front))
+        return err(GR_ERR_USER, "ERROR < USER INPUT | time_start must lie in [time_back, time_front) >");
     if (nx < 1 || ny < 1 || (dim == 3 && nz < 1) || nx * ny * (dim == 3 ? nz : 1) > 0x7fffffffLL)
         return err(GR_ERR_USER, "ERROR < USER INPUT | invalid grid >");
     if (s->device < 0 || s->device >= MAX_DEVICES) return err(GR_ERR_USER, "ERROR < USER INPUT | invalid device >");
@@ -188,24 +220,10 @@ extern "C" int gr_advance_noalloc(const gr_settings *s, int64_t nz, int64_t ny, 
     NoAllocScratch *S = g_scratch_ptr[s->device];
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
-    // time weights of the window, the float32 arithmetic of TrajectoryIntegrator.tpp:126-144
+    // the step schedule and cleared counters, built on the device in stream order
+    noalloc_schedule_kernel<<<1, 256, 0, st>>>(S, time_back, time_front, time_start, s->delta_t, steps);
+    if (cudaGetLastError() != cudaSuccess) return err(GR_ERR_RUNTIME, "ERROR < RUNTIME | schedule launch failed >");
     const float h = s->delta_t;
-    float T = time_start;
-    for (int k = 0; k < steps; ++k) {
-        StepEntry E{};
-        E.t0 = (T - time_back) / (time_front - time_back);
-        E.t1 = ((T + 0.5f * h) - time_back) / (time_front - time_back);
-        E.t2 = ((T + h) - time_back) / (time_front - time_back);
-        E.slot_back = 0;
-        E.slot_front = 1;
-        g_host_sched[k] = E;
-        T = T + h;
-    }
-    if (steps > 0 && cudaMemcpyAsync(S->sched, g_host_sched, sizeof(StepEntry) * steps, cudaMemcpyHostToDevice, st) != cudaSuccess)
-        return err(GR_ERR_RUNTIME, "ERROR < RUNTIME | schedule upload failed >");
-    // the counters keep the previous call's values: clear them
-    if (cudaMemsetAsync(S->counters, 0, sizeof S->counters, st) != cudaSuccess)
-        return err(GR_ERR_RUNTIME, "ERROR < RUNTIME | counter reset failed >");
 
     KParams P;
     std::memset(&P, 0, sizeof P);

@@ -149,6 +149,7 @@ class TrajectorySet {
     std::vector<std::pair<std::string, py::array_t<float>>> volume_data;
     std::vector<py::array_t<float>> compute_data;
     size_t num_compute{0};
+    int64_t particle_steps{0};            // of the run that produced this set (0 for seeds)
 
     TrajectorySet() = default;
 
@@ -471,6 +472,7 @@ class TrajectoryIntegrator {
         set->space = space_;
         set->n = n_;
         set->dim = static_cast<size_t>(dim_);
+        set->particle_steps = info.particle_steps;
         const auto N = static_cast<py::ssize_t>(n_);
         set->traj = result_array({N, static_cast<py::ssize_t>(info.records), static_cast<py::ssize_t>(dim_)});
         check(gr_fetch_positions(engine_, set->traj.mutable_data(), static_cast<int64_t>(set->traj.size())));
@@ -635,5 +637,8 @@ PYBIND11_MODULE(_pygranite, m) {
         .def("computeInfo", &TrajectorySet::computeInfo)
         .def("lengthTrajectories", &TrajectorySet::lengthTrajectories)
         .def("abortReasons", &TrajectorySet::abortReasons)
-        .def("numberTrajectories", &TrajectorySet::numberTrajectories);
+        .def("numberTrajectories", &TrajectorySet::numberTrajectories)
+        // not in the reference: alive particles advanced by the run that produced this set,
+        // summed over its steps (0 for a set made from seeds)
+        .def("particleSteps", [](const TrajectorySet &t) { return t.particle_steps; });
 }

@@ -147,3 +147,31 @@ def test_lifetimes_in_a_plain_run_and_records_after_the_lifetime():
         # ... and every later record repeats the state after its lifetime
         for r in range(lp, info.records):
             assert np.array_equal(traj[:, r], ref_pos), (j, r)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", [0, 1])
+def test_batched_sets_match_the_float32_oracle(storage):
+    """Each set of the batch against the float32 oracle run of that set alone
+    (MaximumSimulationTime = lifetime * DeltaT, TrajectoryIntegrator.tpp:778-995), on the
+    field as the ring stores it (BF16: the float32 snapshots rounded to nearest even)."""
+    from oracle import oracle as orc
+    w = W.BatchWorkload(**SMALL)
+    name = {0: "f32", 1: "bf16"}[storage]
+    engines = {d: group_engine(w, d, storage) for d in (3, 2)}
+    batch = capi.Batch([engines[3][0], engines[2][0]])
+    batch.run()
+    checked = {3: set(), 2: set()}
+    for dim, (eng, spans) in engines.items():
+        pos, status = finals(eng)
+        for j, off, cnt in spans:
+            life = w.sets[j]["life"]
+            snaps = [[W.round_storage(p, name) for p in w.snapshot(dim, k)] for k in range(life // 10 + 2)]
+            st = orc.settings(**dict(w.settings(dim), MaximumSimulationTime=60.0 * life))
+            ref = orc.run(st, orc.Inputs(wind=snaps, seeds=w.seeds(j)), precision="f32")
+            assert np.array_equal(status[off:off + cnt], ref["status"]), (dim, j)
+            assert np.array_equal(pos[off:off + cnt], ref["trajectories"][:, -1]), (dim, j)
+            checked[dim].add(life)
+    batch.close()
+    # sets of different lifetimes on each field
+    assert len(checked[3]) >= 4 and len(checked[2]) >= 3, checked

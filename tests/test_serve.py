@@ -186,3 +186,35 @@ def test_two_dimensional_field_alone_and_in_the_mix():
             pos, status, _ = srv.result(rid)
             assert np.array_equal(status, alone[j][1]) and np.array_equal(pos, alone[j][0]), j
     srv.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", [0, 1])
+def test_mid_window_requests_match_the_float32_oracle(storage):
+    """Requests that start inside a window (start times off the step grid too, rounded down to
+    it), Euler and RK4, submitted together: each result against the float32 oracle run whose
+    particles join the field's clock at the request's start step (the time and window driver of
+    TrajectoryIntegrator.tpp:778-995, entered mid-run), on the field as the ring stores it."""
+    from oracle import oracle as orc
+    snaps = field()
+    name = {0: "f32", 1: "bf16"}[storage]
+    stored = [[W.round_storage(p, name) for p in s] for s in snaps]
+    reqs = [dict(seeds=seeds(300 + 50 * j, 500 + j), start=60.0 * k0 + off, steps=steps, integrator=integ)
+            for j, (k0, off, steps, integ) in enumerate([(3, 0.0, 41, 1), (17, 12.5, 60, 1), (26, 59.0, 33, 0),
+                                                         (44, 30.0, 70, 0), (58, 1.0, 55, 1), (71, 45.0, 49, 0)])]
+    srv = make_server(snaps, storage)
+    ids = [srv.submit(r["seeds"], r["start"], r["steps"], r["integrator"]) for r in reqs]
+    for j, (rid, r) in enumerate(zip(ids, reqs)):
+        assert srv.wait(rid, 120.0) == capi.GR_REQ_DONE, j
+        pos, st, info = srv.result(rid)
+        k0 = int(np.floor(r["start"] / 60.0))
+        assert info.start_step == k0 and info.steps == r["steps"]
+        assert k0 % 10 != 0, "the start must fall inside a window"
+        base = dict(Space=0, Integrator=r["integrator"], WindfieldMode=1, DeltaT=60.0, DataTimeDistance=600.0,
+                    GridScale=[1000.0, 1000.0, 250.0], Offset=[0.0, 0.0, 0.0], SaveInterval=0, BorderMode=0,
+                    CurvatureMode=0, MaximumSimulationTime=60.0 * 10 * (N_SNAP - 1))
+        ref = orc.run(orc.settings(**base), orc.Inputs(wind=stored, seeds=r["seeds"]), precision="f32",
+                      start_step=k0, step_limit=k0 + r["steps"])
+        assert np.array_equal(st, ref["status"]), j
+        assert np.array_equal(pos, ref["trajectories"][:, -1]), j
+    srv.close()

@@ -1,10 +1,10 @@
 """The allocation-free entry point gr_advance_noalloc (GPU).
 
-It exists for callers that cannot call cudaMalloc (graph capture, pool-owned device memory,
-real-time loops).  Its results must equal what gr_run computes for the same particles and
-snapshots: compared bit for bit (the tolerance of the parity tests for this path), on two
-calls in a row, since every call reuses the same device scratch array.  This file is named so
-that pytest collects it last.
+It exists for callers that cannot call cudaMalloc: plug-in hosts whose device memory belongs
+to their own pool allocator, and real-time loops that forbid allocation after start-up.  Its
+results must equal what gr_run computes for the same particles and snapshots: compared bit for
+bit (the tolerance of the parity tests for this path), on two calls in a row, since every call
+reuses the same device scratch array.  This file is named so that pytest collects it last.
 """
 import numpy as np
 import pytest
@@ -84,6 +84,13 @@ def test_noalloc_rejects_oversized_and_unsupported_requests():
     dummy = 1 << 20   # never dereferenced: the arguments are rejected first
     with pytest.raises(capi.GraniteError, match="GR_NOALLOC_MAX_STEPS"):
         capi.advance_noalloc(s, (4, 4, 4), dummy, dummy, 0.0, 1.0, 0.0, 4097, dummy, dummy, dummy, dummy, 10)
-    s = capi.default_settings(space=0, delta_t=0.5, curvature_mode=1)
-    with pytest.raises(capi.GraniteError, match="plain integrator only"):
-        capi.advance_noalloc(s, (4, 4, 4), dummy, dummy, 0.0, 1.0, 0.0, 4, dummy, dummy, dummy, dummy, 10)
+    unsupported = [dict(curvature_mode=1), dict(windfield_mode=0), dict(time_mode=1), dict(minimum_alive=5),
+                   dict(volume_mode=1), dict(abort_mode=1), dict(storage=1), dict(compensated=1)]
+    for kw in unsupported:
+        s = capi.default_settings(space=0, delta_t=0.5, **kw)
+        with pytest.raises(capi.GraniteError, match="plain integrator only"):
+            capi.advance_noalloc(s, (4, 4, 4), dummy, dummy, 0.0, 1.0, 0.0, 4, dummy, dummy, dummy, dummy, 10)
+    s = capi.default_settings(space=0, delta_t=0.5)
+    for start in (-0.5, 1.0, 2.0):   # the first step must start inside [time_back, time_front)
+        with pytest.raises(capi.GraniteError, match="time_start"):
+            capi.advance_noalloc(s, (4, 4, 4), dummy, dummy, 0.0, 1.0, start, 4, dummy, dummy, dummy, dummy, 10)
