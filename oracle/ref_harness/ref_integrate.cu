@@ -106,7 +106,8 @@ struct Tex {
 };
 
 // loadTexture3D (cpp:444-514)
-int load3(ref_args *a, Tex &t, const float *host) {
+template <typename A>
+int load3(A *a, Tex &t, const float *host) {
     const cudaExtent ext = make_cudaExtent(a->nx, a->ny, a->nz);
     cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
     if (!t.arr) RCK(cudaMalloc3DArray(&t.arr, &cd, ext));
@@ -134,7 +135,8 @@ int load3(ref_args *a, Tex &t, const float *host) {
 }
 
 // loadTexture2D (cpp:516-583)
-int load2(ref_args *a, Tex &t, const float *host) {
+template <typename A>
+int load2(A *a, Tex &t, const float *host) {
     if (!t.lin) RCK(cudaMallocPitch(&t.lin, &t.pitch, sizeof(float) * a->nx, a->ny));
     RCK(cudaMemcpy2D(t.lin, t.pitch, host, sizeof(float) * a->nx, sizeof(float) * a->nx, a->ny,
                      cudaMemcpyHostToDevice));
@@ -359,6 +361,352 @@ int run(ref_args *a) {
 }
 
 }  // namespace
+
+// ------------------------------------------------------------------------------------------
+// The option matrix: further instantiations of the reference's kernel, each with the data its
+// options read (textures, per-particle arrays) set up as compute_ / computeLoop_ /
+// computeLoopGPU_ / initializeData / updateData do (tpp:467-995, cpp:146-360, 635-660).
+// Harness-side deviations, where the reference's host code is defective: dynamic constants are
+// stored by their constant index (updateData indexes them from Reference_F0, cpp:319-320, past
+// the end of its arrays).  Dynamic volumes are not instantiated: the kernel samples the wind's
+// u component for them (icc:52-68).
+
+#define OPT_VARIANTS(X)                                                                                                \
+    X(10, Vec2, Space2D, ExplicitEuler, LoopX, Off, Time, Off, Dynamic, Off, Off, false, false, false, false)           \
+    X(11, Vec2, Space2D, ClassicRungeKutta, LoopY, Off, Time, Off, Dynamic, Off, Off, false, false, false, false)       \
+    X(12, Vec2, Space2D, ClassicRungeKutta, LoopXY, Off, Time, Off, Dynamic, Off, Off, false, false, false, false)      \
+    X(13, Vec2, Space2D, ClassicRungeKutta, LoopXY, Off, Time, Off, Dynamic, Off, Off, false, false, true, false)       \
+    X(14, Vec2, Space2D, ExplicitEuler, LoopY, Off, Time, Off, Dynamic, Off, Off, false, false, true, false)            \
+    X(15, Vec2, Space2D, ClassicRungeKutta, Block, FastTotalCurvature, Time, Off, Dynamic, Off, Off, false, true, false, \
+      false)                                                                                                            \
+    X(16, Vec2, Space2D, ClassicRungeKutta, Block, Off, Time, Off, Constant, Off, Off, false, false, false, false)      \
+    X(17, Vec2, Space2D, ClassicRungeKutta, LoopX, FastTotalCurvature, Time, Off, Dynamic, Off, Off, false, false, true,\
+      false)                                                                                                            \
+    X(20, Vec3, Space3D, ClassicRungeKutta, Block, IndividualAndTotalCurvature, Length, Off, Dynamic, Off, Off, false,  \
+      false, false, false)                                                                                              \
+    X(21, Vec3, Space3D, ExplicitEuler, Block, Off, FitLength, Constant, Dynamic, Off, Off, false, false, false, false) \
+    X(22, Vec3, Space3D, ClassicRungeKutta, Block, Off, Time, Dynamic, Dynamic, Off, Off, true, false, false, false)    \
+    X(23, Vec3, Space3D, ClassicRungeKutta, Block, TotalCurvature, Time, Off, Dynamic, Constant, Constant, false, false,\
+      false, true)                                                                                                      \
+    X(24, Vec3, Space3D, ClassicRungeKutta, Block, Off, Time, Off, Dynamic, Dynamic, Off, false, true, false, true)     \
+    X(25, Vec3, Space3D, ExplicitEuler, Block, TotalCurvature, Length, Off, Constant, Off, Off, false, true, false, false)
+
+extern "C" {
+
+typedef struct {
+    // the variant: enum values of the reference's IntegratorSettings (IntegratorSettings.hpp:16-74)
+    int32_t dim, integrator, border_mode, curvature_mode, abort_mode, uplift_mode, windfield_mode, constants_mode,
+        volume_mode, use_topography, reverse, use_sphere, comp_additional;
+    int32_t blocks_fixed;
+    float delta_t, data_time_distance, maximum_simulation_time, maximum_length, sphere_radius;
+    int64_t save_interval;
+    float scale[3], offset[3];
+    int64_t nx, ny, nz;
+    int32_t n_snapshots;
+    const float *const *wind;        // [snapshot * dim] planes
+    int32_t n_volumes;               // 0 or 1 (constant volume)
+    const float *const *volumes;     // [n_volumes] planes
+    int32_t n_constants;             // 0..4
+    const float *const *constants;   // [snapshot * n_constants] arrays of n (snapshot 0 only if constant)
+    const float *const *uplift;      // [snapshot] arrays of n * dim (snapshot 0 only if constant)
+    const float *topography;         // (ny, nx) or null
+    const ASTANode *ast;             // one flat expression (comp_additional)
+    int32_t ast_len;
+    int64_t n;
+    const float *seeds;
+    // outputs
+    int64_t max_records;
+    float *positions;                // [max_records][n][dim]
+    int32_t *status;
+    float *total_curvature, *lengths;
+    float *curvature;                // [max_records][n]
+    float *volume_info;              // [max_records][n]
+    float *compute_info;             // [max_records][n]
+    int64_t records, curvature_records, info_records, steps, windows;
+    char message[256];
+} ref_opt_args;
+
+}  // extern "C"
+
+namespace {
+
+template <typename VEC_T>
+using OptLaunch = void (*)(int blocks, int threads, const SimulationData<VEC_T> &d);
+
+struct OptEntry {
+    int id, dim, integrator, border, curvature, abort_mode, uplift, windfield, constants, volume, topo, reverse, sphere,
+        comp;
+    void *fn;
+};
+
+#define OPT_KERNEL(ID, VT, SP, IN, BM, CM, AM, UM, WM, KM, VM, TOPO, REV, SPH, COMP)                                   \
+    void opt_launch_##ID(int blocks, int threads, const SimulationData<VT> &d) {                                       \
+        integrate<VT, Space::SP, Integrator::IN, BorderMode::BM, CurvatureMode::CM, AbortMode::AM, UpLiftMode::UM,      \
+                  WindfieldMode::WM, ConstantsMode::KM, AdditionalVolumeMode::VM, TOPO, REV, SPH, COMP,                 \
+                  AdditionalVolumeMode::VM != AdditionalVolumeMode::Off><<<blocks, threads>>>(d);                       \
+    }
+OPT_VARIANTS(OPT_KERNEL)
+#undef OPT_KERNEL
+
+#define OPT_ENTRY(ID, VT, SP, IN, BM, CM, AM, UM, WM, KM, VM, TOPO, REV, SPH, COMP)                                    \
+    {ID, (int)sizeof(VT) / (int)sizeof(float), (int)Integrator::IN, (int)BorderMode::BM, (int)CurvatureMode::CM,        \
+     (int)AbortMode::AM, (int)UpLiftMode::UM, (int)WindfieldMode::WM, (int)ConstantsMode::KM,                           \
+     (int)AdditionalVolumeMode::VM, TOPO, REV, SPH, COMP, (void *)&opt_launch_##ID},
+const OptEntry kOpt[] = {OPT_VARIANTS(OPT_ENTRY)};
+#undef OPT_ENTRY
+
+template <typename VEC_T>
+int run_opt(ref_opt_args *a, OptLaunch<VEC_T> fn) {
+    constexpr int DIM = sizeof(VEC_T) / sizeof(float);
+    const int64_t n = a->n;
+    const bool dyn_wind = a->windfield_mode == 1;
+    const bool dyn_any = dyn_wind || a->uplift_mode == 2 || a->volume_mode == 2 || a->constants_mode == 2;
+    Tex wind[3][3], vol, topo;
+    float *cons[3][4] = {};
+    VEC_T *lift[3] = {};
+    int back = 0, front = 1, cache = 2;
+    // updateData(index) of the snapshot s (cpp:262-360), and its first call in initializeData
+    auto load_snapshot = [&](int slot, int s, bool first) -> int {
+        if (first || dyn_wind)
+            for (int c = 0; c < DIM; ++c) {
+                const float *h = a->wind[(int64_t)s * DIM + c];
+                if ((DIM == 3 ? load3(a, wind[slot][c], h) : load2(a, wind[slot][c], h))) return 1;
+            }
+        if (a->constants_mode != 0 && (first || a->constants_mode == 2))
+            for (int k = 0; k < a->n_constants; ++k) {
+                if (!cons[slot][k]) RCK(cudaMalloc(&cons[slot][k], n * sizeof(float)));
+                RCK(cudaMemcpy(cons[slot][k], a->constants[(int64_t)s * a->n_constants + k], n * sizeof(float),
+                               cudaMemcpyHostToDevice));
+            }
+        if (a->uplift_mode != 0 && (first || a->uplift_mode == 2)) {
+            if (!lift[slot]) RCK(cudaMalloc(&lift[slot], n * sizeof(VEC_T)));
+            RCK(cudaMemcpy(lift[slot], a->uplift[s], n * sizeof(VEC_T), cudaMemcpyHostToDevice));
+        }
+        return 0;
+    };
+    // initializeData (cpp:146-259)
+    if (load_snapshot(0, 0, true)) return 1;
+    if (a->volume_mode == 1 && a->n_volumes > 0)
+        if ((DIM == 3 ? load3(a, vol, a->volumes[0]) : load2(a, vol, a->volumes[0]))) return 1;
+    int loaded = 1;
+    if (dyn_any) {
+        if (a->n_snapshots < 2) {
+            snprintf(a->message, sizeof a->message, "Cannot increment loader.");
+            return 1;
+        }
+        if (load_snapshot(1, 1, false)) return 1;
+        loaded = 2;
+    }
+    // initializeTopography (cpp:635-660): a 2D pitch texture of the (ny, nx) plane
+    if (a->use_topography) {
+        ref_opt_args t2 = *a;
+        t2.nz = 1;
+        if (load2(&t2, topo, a->topography)) {
+            memcpy(a->message, t2.message, sizeof a->message);
+            return 1;
+        }
+    }
+
+    // compute_ (tpp:467-712)
+    VEC_T *buf[2] = {nullptr, nullptr};
+    RCK(cudaMalloc(&buf[0], n * sizeof(VEC_T)));
+    RCK(cudaMalloc(&buf[1], n * sizeof(VEC_T)));
+    RCK(cudaMemcpy(buf[0], a->seeds, n * sizeof(VEC_T), cudaMemcpyHostToDevice));
+    int swap_index = 0;
+    AbortReason *status = nullptr;
+    RCK(cudaMalloc(&status, n * sizeof(AbortReason)));
+    RCK(cudaMemset(status, 0, n * sizeof(AbortReason)));
+    SimulationData<VEC_T> d;
+    d.Status = status;
+    d.NumParticles = n;
+    d.Radius = a->sphere_radius;
+    d.GridScale.X = a->scale[0]; d.GridScale.Y = a->scale[1]; d.GridScale.Z = a->scale[2];
+    d.Domain.X = a->nx * a->scale[0]; d.Domain.Y = a->ny * a->scale[1]; d.Domain.Z = a->nz * a->scale[2];
+    d.Offset.X = a->offset[0]; d.Offset.Y = a->offset[1]; d.Offset.Z = a->offset[2];
+    float *len = nullptr, *curv = nullptr, *tc = nullptr, *vinfo = nullptr, *cinfo = nullptr;
+    VEC_T *lastdir = nullptr;
+    ASTANode *ast = nullptr;
+    if (a->abort_mode != 0) {
+        RCK(cudaMalloc(&len, n * sizeof(float)));
+        RCK(cudaMemset(len, 0, n * sizeof(float)));
+        d.MaximumLength = a->maximum_length;
+        d.CurrentLength = len;
+    }
+    if (a->curvature_mode != 0) {
+        if (a->curvature_mode == 3) {
+            RCK(cudaMalloc(&curv, n * sizeof(float)));
+            RCK(cudaMemset(curv, 0, n * sizeof(float)));
+            d.Curvature = curv;
+        }
+        if (a->curvature_mode == 2) RCK(cudaMalloc(&lastdir, n * sizeof(VEC_T)));
+        RCK(cudaMalloc(&tc, n * sizeof(float)));
+        RCK(cudaMemset(tc, 0, n * sizeof(float)));
+        d.TotalCurvature = tc;
+        d.LastDirections = lastdir;
+    }
+    d.NumAdditionalVolumes = 0;
+    if (a->volume_mode != 0) {
+        d.NumAdditionalVolumes = a->n_volumes;
+        if (a->n_volumes > 0) {
+            RCK(cudaMalloc(&vinfo, n * sizeof(float)));
+            RCK(cudaMemset(vinfo, 0, n * sizeof(float)));   // the reference leaves it uninitialised
+            d.ParticleVolumeInfo[0] = vinfo;
+        }
+    }
+    d.NumAdditionalCompute = 0;
+    if (a->comp_additional) {
+        d.NumAdditionalCompute = 1;
+        RCK(cudaMalloc(&ast, sizeof(ASTANode) * a->ast_len));
+        RCK(cudaMemcpy(ast, a->ast, sizeof(ASTANode) * a->ast_len, cudaMemcpyHostToDevice));
+        d.ASTNodes[0] = ast;
+        d.ASTSizes[0] = a->ast_len;
+        RCK(cudaMalloc(&cinfo, n * sizeof(float)));
+        RCK(cudaMemset(cinfo, 0, n * sizeof(float)));
+        d.ParticleComputeInfo[0] = cinfo;
+    }
+
+    // computeLoop_ (tpp:764-918)
+    cudaDeviceProp prop;
+    RCK(cudaGetDeviceProperties(&prop, 0));
+    const unsigned threads = (unsigned)(std::min((size_t)prop.maxThreadsPerBlock, (size_t)n)) / 2;
+    unsigned blocks = (unsigned)std::min<size_t>((threads + n - 1) / n, (size_t)prop.maxThreadsDim[0]);
+    if (a->blocks_fixed) blocks = (unsigned)((n + threads - 1) / threads);
+    if (!dyn_wind)
+        for (int c = 0; c < DIM; ++c) d.WindfieldBack[c] = wind[0][c].obj;
+    if (a->volume_mode == 1 && a->n_volumes > 0) d.AdditionalVolumesBack[0] = vol.obj;
+    if (a->uplift_mode == 1) d.LiftBack = lift[0];
+    d.NumAdditionalConstants = a->n_constants;
+    if (a->constants_mode == 1)
+        for (int k = 0; k < a->n_constants; ++k) {
+            d.ComputeDataBack[k] = cons[0][k];
+            d.ComputeDataFront[k] = cons[0][k];
+        }
+    d.DeltaT = a->delta_t;
+
+    std::vector<float> host_f(n);
+    a->records = a->curvature_records = a->info_records = 0;
+    // copyParticleInfo (tpp:997-1049)
+    auto save = [&]() -> int {
+        VEC_T *f = buf[swap_index];
+        if (a->records < a->max_records)
+            RCK(cudaMemcpy(a->positions + a->records * n * DIM, f, n * sizeof(VEC_T), cudaMemcpyDeviceToHost));
+        a->records++;
+        if (a->curvature_mode == 3 && d.Time > 0) {
+            if (a->curvature_records < a->max_records)
+                RCK(cudaMemcpy(a->curvature + a->curvature_records * n, curv, n * sizeof(float), cudaMemcpyDeviceToHost));
+            a->curvature_records++;
+        }
+        if (cinfo || vinfo) {
+            if (a->info_records < a->max_records) {
+                if (cinfo)
+                    RCK(cudaMemcpy(a->compute_info + a->info_records * n, cinfo, n * sizeof(float), cudaMemcpyDeviceToHost));
+                if (vinfo)
+                    RCK(cudaMemcpy(a->volume_info + a->info_records * n, vinfo, n * sizeof(float), cudaMemcpyDeviceToHost));
+            }
+            a->info_records++;
+        }
+        return 0;
+    };
+    if (a->max_records > 0) memcpy(a->positions, a->seeds, n * sizeof(VEC_T));
+    a->records = 1;
+
+    size_t counter = 0, sim = 0;
+    float max_wt = a->data_time_distance;
+    const float limit = a->maximum_simulation_time / a->delta_t;
+    d.Time = 0.f;
+    a->windows = 0;
+    do {
+        // computeLoopGPU_ (tpp:920-995)
+        a->windows++;
+        const float window_end = dyn_any ? max_wt : a->maximum_simulation_time;
+        if (a->use_topography) d.Topography = topo.obj;
+        d.TimeBack = counter * a->data_time_distance;
+        d.TimeFront = (counter + 1) * a->data_time_distance;
+        if (dyn_wind)
+            for (int c = 0; c < DIM; ++c) {
+                d.WindfieldBack[c] = wind[back][c].obj;
+                d.WindfieldFront[c] = wind[front][c].obj;
+            }
+        if (a->uplift_mode == 2) {
+            d.LiftBack = lift[back];
+            d.LiftFront = lift[front];
+        }
+        if (a->constants_mode == 2)
+            for (int k = 0; k < a->n_constants; ++k) {
+                d.ComputeDataBack[k] = cons[back][k];
+                d.ComputeDataFront[k] = cons[front][k];
+            }
+        while ((float)sim < limit) {
+            swap_index = (swap_index + 1) % 2;
+            d.FrontParticles = buf[swap_index];
+            d.BackParticles = buf[(swap_index + 1) % 2];
+            fn(blocks, threads, d);
+            RCK(cudaDeviceSynchronize());
+            RCK(cudaGetLastError());
+            if (a->save_interval != 0 && sim % a->save_interval == 0)
+                if (save()) return 1;
+            d.Time += d.DeltaT;
+            ++sim;
+            if (d.Time >= window_end) break;
+        }
+        if (dyn_any) {
+            if (loaded < a->n_snapshots) {   // _loader.step() returned true
+                if (load_snapshot(cache, loaded, false)) return 1;
+                ++loaded;
+                max_wt += a->data_time_distance;
+                const int tmp = back;
+                back = front;
+                front = cache;
+                cache = tmp;
+                ++counter;
+            } else {
+                break;
+            }
+        }
+    } while (dyn_wind && (float)sim < limit);
+    if (a->save_interval == 0)
+        if (save()) return 1;
+    a->steps = (int64_t)sim;
+    RCK(cudaMemcpy(a->status, status, n * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (tc && a->total_curvature) RCK(cudaMemcpy(a->total_curvature, tc, n * sizeof(float), cudaMemcpyDeviceToHost));
+    if (len && a->lengths) RCK(cudaMemcpy(a->lengths, len, n * sizeof(float), cudaMemcpyDeviceToHost));
+
+    cudaFree(buf[0]); cudaFree(buf[1]); cudaFree(status);
+    for (float *p : {len, curv, tc, vinfo, cinfo}) if (p) cudaFree(p);
+    if (lastdir) cudaFree(lastdir);
+    if (ast) cudaFree(ast);
+    for (auto &sl : cons) for (float *p : sl) if (p) cudaFree(p);
+    for (VEC_T *p : lift) if (p) cudaFree(p);
+    for (auto &sl : wind) for (auto &t : sl) free_tex(t);
+    free_tex(vol);
+    free_tex(topo);
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int ref_run_opt(ref_opt_args *a) {
+    a->message[0] = 0;
+    if (a->n < 2) {
+        snprintf(a->message, sizeof a->message, "the reference's launch shape needs at least 2 particles");
+        return 1;
+    }
+    if (a->n_volumes > 1 || a->n_constants > 4) {
+        snprintf(a->message, sizeof a->message, "at most one volume and four constants");
+        return 1;
+    }
+    for (const OptEntry &v : kOpt) {
+        if (v.dim == a->dim && v.integrator == a->integrator && v.border == a->border_mode &&
+            v.curvature == a->curvature_mode && v.abort_mode == a->abort_mode && v.uplift == a->uplift_mode &&
+            v.windfield == a->windfield_mode && v.constants == a->constants_mode && v.volume == a->volume_mode &&
+            v.topo == a->use_topography && v.reverse == a->reverse && v.sphere == a->use_sphere &&
+            v.comp == a->comp_additional)
+            return a->dim == 2 ? run_opt<Vec2>(a, reinterpret_cast<OptLaunch<Vec2>>(v.fn))
+                               : run_opt<Vec3>(a, reinterpret_cast<OptLaunch<Vec3>>(v.fn));
+    }
+    snprintf(a->message, sizeof a->message, "no instantiated reference variant for these settings");
+    return 2;
+}
 
 extern "C" int ref_run(ref_args *a) {
     a->message[0] = 0;

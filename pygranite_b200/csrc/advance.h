@@ -8,9 +8,20 @@ namespace granite_b200 {
 
 using AdvanceFn = void (*)(const KParams);
 
-// Step kernel for a dimension, integrator and wind layout (pair = window-pair buffer).
-AdvanceFn advance_f32(int dim, bool rk4, bool pair);
-AdvanceFn advance_bf16(int dim, bool rk4, bool pair);
-AdvanceFn advance_f16(int dim, bool rk4, bool pair);
+// The feature set (FT_* in granite_kernels.cuh) a launch with parameters P may use: a lean
+// variant when every option it leaves out is off in P (window-pair layouts only), else generic.
+inline int kernel_features(const KParams &P, bool pair) {
+    if (!pair || P.compensated || P.uplift_mode != 0 || P.abort_mode != 0 || P.topography || P.sphere ||
+        P.border_mode != 0 || P.alive_at != nullptr || (P.curvature_mode != 0 && P.curvature_mode != 1))
+        return FT_GENERIC;
+    const bool extras = (P.volume_mode != 0 && P.nvol > 0) || P.nexpr > 0;
+    return FT_LEAN | (P.curvature_mode == 1 ? FT_CURV : 0) | (extras ? FT_EXTRAS : 0);
+}
+
+// Step kernel for a dimension, integrator, wind layout (pair = window-pair buffer) and feature
+// set (kernel_features).
+AdvanceFn advance_f32(int dim, bool rk4, bool pair, int ft);
+AdvanceFn advance_bf16(int dim, bool rk4, bool pair, int ft);
+AdvanceFn advance_f16(int dim, bool rk4, bool pair, int ft);
 
 }  // namespace granite_b200

@@ -306,6 +306,9 @@ int setup_grid(gr_engine *e, int64_t nz, int64_t ny, int64_t nx) {
         return USER_ERR("Invalid dataset was provided. Grid too large. >");
     e->nx = nx; e->ny = ny; e->nz = e->dim == 3 ? nz : 1;
     e->nodes = e->nx * e->ny * e->nz;
+    // the step kernel indexes nodes (and the padded 3D window pair) with 32-bit integers
+    if ((e->dim == 3 ? padded_pair_nodes(e->nx, e->ny, e->nz) : e->nodes) > (int64_t(1) << 31) - 1)
+        return USER_ERR("Invalid dataset was provided. Grid too large. >");
     const gr_settings &s = e->s;
     // GridScale / Offset / Domain (TrajectoryIntegrator.tpp:521-574)
     const float *gs = s.grid_scale, *of = s.offset;
@@ -950,6 +953,12 @@ int pair_elem(const gr_engine *e) {
     return e->s.storage == GR_STORE_F32 ? (e->dim == 3 ? 16 : 8) : (e->dim == 3 ? 8 : 4);
 }
 
+// Bytes of one window-pair buffer: 3D pairs carry a zero border (pair_pack_padded_kernel).
+size_t pair_bytes(const gr_engine *e) {
+    const int64_t nodes = e->dim == 3 ? padded_pair_nodes(e->nx, e->ny, e->nz) : e->nodes;
+    return (size_t)nodes * 2 * pair_elem(e);
+}
+
 // Validation, schedule, device schedule and programs, state and history buffers.
 int run_prepare(gr_engine *e, RunPlan &R, bool graph) {
     if (!e) return USER_ERR("null engine >");
@@ -1073,7 +1082,7 @@ int run_prepare(gr_engine *e, RunPlan &R, bool graph) {
     e->pair_window[0] = e->pair_window[1] = -1;
     if (graph) {
         if (e->use_pair)
-            for (int b = 0; b < 2; ++b) CK(e->pairbuf[b].alloc((size_t)e->nodes * 2 * pair_elem(e)));
+            for (int b = 0; b < 2; ++b) CK(e->pairbuf[b].alloc(pair_bytes(e)));
         // the fill-forward table of the full run, uploaded before the capture
         const std::vector<int32_t> t = crec_table(e, R, R.nsteps);
         CK(e->crec_of_rec.alloc(t.size()));
@@ -1104,6 +1113,7 @@ KParams make_params(gr_engine *e) {
         P.scale[d] = e->scale[d];
     }
     P.nx = (int32_t)e->nx; P.ny = (int32_t)e->ny; P.nz = (int32_t)e->nz; P.dim = e->dim;
+    P.pnx = (int32_t)(e->nx + 3); P.pnxy = (int32_t)((e->nx + 3) * (e->ny + 3));
     P.wind = e->wind.p; P.wind_stride = e->wind_stride;
     P.vol = e->vol.p; P.vol_plane = e->nodes;
     P.cons = e->cons.p; P.lift = e->lift.p; P.topo = e->topo.p;
@@ -1271,11 +1281,12 @@ __global__ void finalize_retired_kernel(StateView R, const int32_t *n_ret, int a
 
 using KernelFn = void (*)(const KParams);
 
-KernelFn pick_kernel(const gr_engine *e) {
+KernelFn pick_kernel(const gr_engine *e, const KParams &P) {
     const bool rk4 = e->s.integrator == 1;
     const int st = e->s.storage;
-    return st == GR_STORE_BF16 ? advance_bf16(e->dim, rk4, e->use_pair)
-         : st == GR_STORE_F16 ? advance_f16(e->dim, rk4, e->use_pair) : advance_f32(e->dim, rk4, e->use_pair);
+    const int ft = kernel_features(P, e->use_pair);
+    return st == GR_STORE_BF16 ? advance_bf16(e->dim, rk4, e->use_pair, ft)
+         : st == GR_STORE_F16 ? advance_f16(e->dim, rk4, e->use_pair, ft) : advance_f32(e->dim, rk4, e->use_pair, ft);
 }
 
 int block_size_for(const gr_engine *e) {
@@ -1300,11 +1311,19 @@ cudaEvent_t pool_event(gr_engine *e, size_t k) {
 int pack_pair(gr_engine *e, int64_t w, cudaStream_t stream) {
     const int b = (int)(w & 1);
     const int elem = pair_elem(e);
-    CK(e->pairbuf[b].alloc((size_t)e->nodes * 2 * elem));
+    CK(e->pairbuf[b].alloc(pair_bytes(e)));
     const char *back = e->wind.p + (int64_t)(w % e->K) * e->wind_stride;
     const char *front = e->wind.p + (int64_t)((w + 1) % e->K) * e->wind_stride;
     const int threads = 256, blocks = grid_for(e->nodes, threads);
-    if (elem == 16)
+    if (e->dim == 3) {
+        const int32_t nx = (int32_t)e->nx, ny = (int32_t)e->ny, nz = (int32_t)e->nz;
+        if (elem == 16)
+            pair_pack_padded_kernel<uint4><<<blocks, threads, 0, stream>>>((const uint4 *)back, (const uint4 *)front,
+                                                                          (uint4 *)e->pairbuf[b].p, nx, ny, nz);
+        else
+            pair_pack_padded_kernel<uint2><<<blocks, threads, 0, stream>>>((const uint2 *)back, (const uint2 *)front,
+                                                                          (uint2 *)e->pairbuf[b].p, nx, ny, nz);
+    } else if (elem == 16)
         pair_pack_kernel<uint4><<<blocks, threads, 0, stream>>>((const uint4 *)back, (const uint4 *)front, (uint4 *)e->pairbuf[b].p, e->nodes);
     else if (elem == 8)
         pair_pack_kernel<uint2><<<blocks, threads, 0, stream>>>((const uint2 *)back, (const uint2 *)front, (uint2 *)e->pairbuf[b].p, e->nodes);
@@ -1377,7 +1396,7 @@ int make_ctx(gr_engine *e, RunPlan &R, RunCtx &r) {
     r.e = e;
     r.R = &R;
     r.P = make_params(e);
-    r.fn = pick_kernel(e);
+    r.fn = pick_kernel(e, r.P);
     r.threads = block_size_for(e);
     // some step kernels are built for smaller blocks (their launch bounds)
     cudaFuncAttributes fa{};

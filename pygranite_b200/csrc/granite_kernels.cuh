@@ -27,6 +27,14 @@ constexpr int GR_MAX_VOL = 8;
 constexpr int GR_MAX_EXPR = 4;
 constexpr int GR_MAX_CON = 4;
 
+// Compile-time feature sets of the step kernel.  FT_GENERIC honours every runtime option.  A
+// lean variant (FT_LEAN) is picked by the host (kernel_features in advance.h) when the launch has
+// no Kahan positions, uplift, length abort, topography, sphere coordinates, loop borders or
+// per-step alive counts, and curvature Off or Total; FT_CURV / FT_EXTRAS say whether it keeps
+// total curvature and volume / expression values.  The lean variants drop the dead state from
+// registers; their arithmetic is the generic variant's.
+constexpr int FT_GENERIC = 0, FT_LEAN = 1, FT_CURV = 2, FT_EXTRAS = 4;
+
 // Step-schedule flags.
 constexpr int SF_SAVE = 1;       // position / info record after this step
 constexpr int SF_TIME_POS = 2;   // data.Time > 0 at the start of the step
@@ -48,6 +56,9 @@ struct KParams {
     const void *wind;
     int64_t wind_stride;          // bytes per slot
     const void *pair;             // window-pair buffer of the launch's window (pair layouts)
+    int32_t pnx, pnxy;            // 3D window pair: padded row length (nx + 3) and plane size
+                                  // ((nx + 3) * (ny + 3)); node (x, y, z) at
+                                  // (z + 1) * pnxy + (y + 1) * pnx + (x + 1), zeros outside the grid
     const float *vol;             // [slot][8][plane]
     int64_t vol_plane;            // floats per plane
     const float *cons;            // [slot][4][n_total]
@@ -258,35 +269,95 @@ __device__ __forceinline__ float tri_corners(const float (&c)[8], const Cell3 &c
 
 // Pair nodes of the last cell a particle sampled (window-pair layouts).  Consecutive samples of
 // one particle (its RK4 stages, its next step) mostly fall in the same cell, whose nodes then
-// need no new gathers; the values and the arithmetic are the same either way.  3D 16-bit kernels
-// keep the raw nodes (32 registers, within their 128-register bound); the float32 3D kernel
-// keeps the 48 floats and is built for 128-thread blocks, 3 per SM (AdvBounds); 2D keeps the 4
-// corners as floats (16 registers).
+// need no new gathers; the values and the arithmetic are the same either way.  In 3D the cell is
+// identified by its first corner's index in the padded pair buffer (`base`); 16-bit kernels keep
+// the raw nodes (32 registers), the float32 kernel the 48 floats (AdvBounds gives its launch
+// shape); 2D keeps the 4 corners as floats (16 registers), keyed by their indices.
 struct SampleCache {
-    int32_t base, sx, sy, sz;
-    unsigned valid;
+    int32_t base;
     uint4 q[8];
     int32_t i00, i10, i01, i11;
     float b2[4][2], f2[4][2];
     float c32[6][8];   // float32 3D: u, v, w back and front of the 8 corners
     __device__ __forceinline__ void reset() {
-        base = -1; sx = sy = sz = 0; valid = 0;
+        base = -1;
         i00 = i10 = i01 = i11 = -1;
     }
 };
 
+// 3D window pair with a zero border (one node below, two above the grid on every axis): the
+// coordinate is clamped to [-1, n], so every corner of the footprint is a node of the padded
+// buffer and needs no validity test, and the footprint's first corner alone identifies the cell.
+// Same values as make_cell3 + border addressing: inside [-1, n] the cell and fraction are
+// identical; outside it every corner the original reads is outside the grid (0), and here the
+// fraction is 0 with the weighted-away corner finite, so the interpolation is +0 either way.
+// Padded node count of a 3D window-pair buffer.
+inline int64_t padded_pair_nodes(int64_t nx, int64_t ny, int64_t nz) { return (nx + 3) * (ny + 3) * (nz + 3); }
+
+struct PCell {
+    int32_t base;        // padded node index of corner (ix, iy, iz)
+    float fx, fy, fz;
+};
+
+__device__ __forceinline__ void pcell1(float a, int n, int fw, int &i, float &f) {
+    a = fminf(fmaxf(a, -1.0f), (float)n);
+    const float fl = floorf(a);
+    i = (int)fl;
+    f = a - fl;
+    if (fw) f = floorf(f * 256.0f + 0.5f) * (1.0f / 256.0f);
+}
+
+__device__ __forceinline__ PCell make_pcell(const KParams &P, float ax, float ay, float az) {
+    int ix, iy, iz;
+    PCell c;
+    pcell1(ax, P.nx, P.filter_weights, ix, c.fx);
+    pcell1(ay, P.ny, P.filter_weights, iy, c.fy);
+    pcell1(az, P.nz, P.filter_weights, iz, c.fz);
+    c.base = (iz + 1) * P.pnxy + (iy + 1) * P.pnx + (ix + 1);
+    return c;
+}
+
+__device__ __forceinline__ float tri8(const float (&c)[8], float fx, float fy, float fz) {
+    const float a00 = lerp_(c[0], c[1], fx), a10 = lerp_(c[2], c[3], fx);
+    const float a01 = lerp_(c[4], c[5], fx), a11 = lerp_(c[6], c[7], fx);
+    return lerp_(lerp_(a00, a10, fy), lerp_(a01, a11, fy), fz);
+}
+
+// Loads the 8 padded corners of the cell at `base` into the sample cache: float32 as 48 floats
+// (back / front u, v, w per corner), 16-bit as the raw 16-byte pair nodes.
 template <typename H>
-__device__ __forceinline__ void tri3p_cached16(const void *pairs, const Cell3 &c, SampleCache &cc, float (&ob)[3],
-                                               float (&of)[3]) {
-    if (c.base != cc.base || c.sx != cc.sx || c.sy != cc.sy || c.sz != cc.sz || c.valid != cc.valid) {
+__device__ __forceinline__ void fill_padded(const KParams &P, const void *pairs, int32_t base, SampleCache &cc) {
+    const int32_t sy = P.pnx, sz = P.pnxy;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
-            const int32_t idx = c.base + (dx ? c.sx : 0) + (dy ? c.sy : 0) + (dz ? c.sz : 0);
-            cc.q[k] = (c.valid & (1u << k)) ? __ldg(reinterpret_cast<const uint4 *>(pairs) + idx) : make_uint4(0, 0, 0, 0);
+    for (int k = 0; k < 8; ++k) {
+        const int32_t idx = base + ((k & 1) ? 1 : 0) + ((k & 2) ? sy : 0) + ((k & 4) ? sz : 0);
+        if constexpr (std::is_same<H, float>::value) {
+            float b[3], f[3];
+            Store<Pair<float>>::load3p(pairs, idx, b, f);
+            cc.c32[0][k] = b[0]; cc.c32[1][k] = b[1]; cc.c32[2][k] = b[2];
+            cc.c32[3][k] = f[0]; cc.c32[4][k] = f[1]; cc.c32[5][k] = f[2];
+        } else {
+            cc.q[k] = __ldg(reinterpret_cast<const uint4 *>(pairs) + idx);
         }
-        cc.base = c.base; cc.sx = c.sx; cc.sy = c.sy; cc.sz = c.sz; cc.valid = c.valid;
     }
+    cc.base = base;
+}
+
+// float32: the 8 padded corners' back / front values as 48 floats, reloaded when the cell changes.
+__device__ __forceinline__ void tri3p_padded32(const KParams &P, const void *pairs, const PCell &c, SampleCache &cc,
+                                               float (&ob)[3], float (&of)[3]) {
+    if (c.base != cc.base) fill_padded<float>(P, pairs, c.base, cc);
+    ob[0] = tri8(cc.c32[0], c.fx, c.fy, c.fz); ob[1] = tri8(cc.c32[1], c.fx, c.fy, c.fz);
+    ob[2] = tri8(cc.c32[2], c.fx, c.fy, c.fz);
+    of[0] = tri8(cc.c32[3], c.fx, c.fy, c.fz); of[1] = tri8(cc.c32[4], c.fx, c.fy, c.fz);
+    of[2] = tri8(cc.c32[5], c.fx, c.fy, c.fz);
+}
+
+// 16-bit: the 8 padded corners as raw 16-byte pair nodes, converted per sample.
+template <typename H>
+__device__ __forceinline__ void tri3p_padded16(const KParams &P, const void *pairs, const PCell &c, SampleCache &cc,
+                                               float (&ob)[3], float (&of)[3]) {
+    if (c.base != cc.base) fill_padded<H>(P, pairs, c.base, cc);
     float u[8], v[8], w[8], uf[8], vf[8], wf[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
@@ -294,48 +365,12 @@ __device__ __forceinline__ void tri3p_cached16(const void *pairs, const Cell3 &c
         const float2 f01 = Store<Pair<H>>::cvt(cc.q[k].z), f2 = Store<Pair<H>>::cvt(cc.q[k].w);
         u[k] = b01.x; v[k] = b01.y; w[k] = b2.x; uf[k] = f01.x; vf[k] = f01.y; wf[k] = f2.x;
     }
-    ob[0] = tri_corners(u, c); ob[1] = tri_corners(v, c); ob[2] = tri_corners(w, c);
-    of[0] = tri_corners(uf, c); of[1] = tri_corners(vf, c); of[2] = tri_corners(wf, c);
-}
-
-// float32 3D: the 8 corners as floats (48 registers; see AdvBounds for the launch shape).
-__device__ __forceinline__ void tri3p_cached32(const void *pairs, const Cell3 &c, SampleCache &cc, float (&ob)[3],
-                                               float (&of)[3]) {
-    if (c.base != cc.base || c.sx != cc.sx || c.sy != cc.sy || c.sz != cc.sz || c.valid != cc.valid) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
-            const int32_t idx = c.base + (dx ? c.sx : 0) + (dy ? c.sy : 0) + (dz ? c.sz : 0);
-            float b[3] = {0.f, 0.f, 0.f}, f[3] = {0.f, 0.f, 0.f};
-            if (c.valid & (1u << k)) Store<Pair<float>>::load3p(pairs, idx, b, f);
-            cc.c32[0][k] = b[0]; cc.c32[1][k] = b[1]; cc.c32[2][k] = b[2];
-            cc.c32[3][k] = f[0]; cc.c32[4][k] = f[1]; cc.c32[5][k] = f[2];
-        }
-        cc.base = c.base; cc.sx = c.sx; cc.sy = c.sy; cc.sz = c.sz; cc.valid = c.valid;
-    }
-    ob[0] = tri_corners(cc.c32[0], c); ob[1] = tri_corners(cc.c32[1], c); ob[2] = tri_corners(cc.c32[2], c);
-    of[0] = tri_corners(cc.c32[3], c); of[1] = tri_corners(cc.c32[4], c); of[2] = tri_corners(cc.c32[5], c);
+    ob[0] = tri8(u, c.fx, c.fy, c.fz); ob[1] = tri8(v, c.fx, c.fy, c.fz); ob[2] = tri8(w, c.fx, c.fy, c.fz);
+    of[0] = tri8(uf, c.fx, c.fy, c.fz); of[1] = tri8(vf, c.fx, c.fy, c.fz); of[2] = tri8(wf, c.fx, c.fy, c.fz);
 }
 
 template <typename W> struct PairElem { using type = void; };
 template <typename H> struct PairElem<Pair<H>> { using type = H; };
-
-// Back and front snapshot at once from a window-pair layout; same arithmetic as tri3 on each.
-template <typename W>
-__device__ __forceinline__ void tri3p(const void *pairs, const Cell3 &c, float (&ob)[3], float (&of)[3]) {
-    float u[8], v[8], w[8], uf[8], vf[8], wf[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
-        const int32_t idx = c.base + (dx ? c.sx : 0) + (dy ? c.sy : 0) + (dz ? c.sz : 0);
-        float b[3] = {0.f, 0.f, 0.f}, f[3] = {0.f, 0.f, 0.f};
-        if (c.valid & (1u << k)) Store<W>::load3p(pairs, idx, b, f);
-        u[k] = b[0]; v[k] = b[1]; w[k] = b[2];
-        uf[k] = f[0]; vf[k] = f[1]; wf[k] = f[2];
-    }
-    ob[0] = tri_corners(u, c); ob[1] = tri_corners(v, c); ob[2] = tri_corners(w, c);
-    of[0] = tri_corners(uf, c); of[1] = tri_corners(vf, c); of[2] = tri_corners(wf, c);
-}
 
 // Trilinear interpolation of one scalar float32 plane.
 __device__ __forceinline__ float tri1(const float *plane, const Cell3 &c) {
@@ -442,15 +477,13 @@ __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, co
         // window-pair layout (dynamic wind only): wb points at the pair buffer
         if (DIM == 3) {
             const float az = (p.z - P.off[2]) * P.inv_scale[2];
-            const Cell3 c = make_cell3(P, ax, ay, az);
+            const PCell c = make_pcell(P, ax, ay, az);
             float b[3], f[3];
             using H = typename PairElem<W>::type;
-            if constexpr (!std::is_same<H, float>::value && !std::is_same<H, void>::value)
-                tri3p_cached16<H>(wb, c, cc, b, f);
-            else if constexpr (std::is_same<H, float>::value)
-                tri3p_cached32(wb, c, cc, b, f);
+            if constexpr (std::is_same<H, float>::value)
+                tri3p_padded32(P, wb, c, cc, b, f);
             else
-                tri3p<W>(wb, c, b, f);
+                tri3p_padded16<H>(P, wb, c, cc, b, f);
             r.x = lerp_(b[0], f[0], t); r.y = lerp_(b[1], f[1], t); r.z = lerp_(b[2], f[2], t);
         } else {
             const Cell2 c = make_cell2(P.nx, P.ny, P.filter_weights, ax, ay);
@@ -621,6 +654,28 @@ __device__ __forceinline__ void eval_extras(const KParams &P, const StepEntry &E
     }
 }
 
+// The volume / expression values of slot i kept in the state arrays between evaluations.  For
+// an evaluation (`evaluating`) only what eval_extras reads but does not overwrite is loaded:
+// volumes when no volume is sampled (their stored values enter the expressions).
+__device__ __forceinline__ void load_extras(const KParams &P, int64_t i, bool evaluating, float (&vol)[GR_MAX_VOL],
+                                            float (&cmp)[GR_MAX_EXPR]) {
+    const bool vols = !evaluating || P.volume_mode == 0;
+#pragma unroll
+    for (int k = 0; k < GR_MAX_VOL; ++k) vol[k] = (k < P.nvol && vols) ? P.volc[k * P.n_state + i] : 0.f;
+#pragma unroll
+    for (int k = 0; k < GR_MAX_EXPR; ++k) cmp[k] = (k < P.nexpr && !evaluating) ? P.cmpc[k * P.n_state + i] : 0.f;
+}
+
+__device__ __forceinline__ void store_extras(const KParams &P, int64_t i, const float (&vol)[GR_MAX_VOL],
+                                             const float (&cmp)[GR_MAX_EXPR]) {
+#pragma unroll
+    for (int k = 0; k < GR_MAX_VOL; ++k)
+        if (k < P.nvol) P.volc[k * P.n_state + i] = vol[k];
+#pragma unroll
+    for (int k = 0; k < GR_MAX_EXPR; ++k)
+        if (k < P.nexpr) P.cmpc[k * P.n_state + i] = cmp[k];
+}
+
 // ------------------------------------------------------------------ the step kernel
 
 #ifndef GR_ADV_MIN_BLOCKS
@@ -628,9 +683,19 @@ __device__ __forceinline__ void eval_extras(const KParams &P, const StepEntry &E
 #endif
 
 // Advances the particle in slot i through steps [s0, s1) (or until its lifetime ends).
-template <int DIM, bool RK4, typename W>
+template <int DIM, bool RK4, typename W, int FT>
 __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t i, const int64_t n_live,
                                                  unsigned long long &steps_acc, unsigned &alive_acc) {
+    // options: runtime values in the generic variant; in a lean variant (FT_LEAN) the ones the
+    // host checked are off, and curvature / extras are the variant's compile-time choice
+    constexpr bool LEAN = (FT & FT_LEAN) != 0;
+    const int curvature_mode = LEAN ? ((FT & FT_CURV) ? 1 : 0) : P.curvature_mode;
+    const int abort_mode = LEAN ? 0 : P.abort_mode;
+    const int uplift_mode = LEAN ? 0 : P.uplift_mode;
+    const bool compensated = LEAN ? false : P.compensated != 0;
+    const bool topography = LEAN ? false : P.topography != 0;
+    const int border_mode = LEAN ? 0 : P.border_mode;
+    unsigned *const alive_at = LEAN ? nullptr : P.alive_at;
     const bool valid = i < n_live;
     int32_t st = valid ? P.status[i] : 1;
     bool alive = st == 0;
@@ -638,38 +703,27 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
 
     V3 p{0.f, 0.f, 0.f}, q{0.f, 0.f, 0.f}, comp{0.f, 0.f, 0.f}, ld{0.f, 0.f, 0.f};
     float len = 0.f, tc = 0.f, cv = 0.f;
-    float vol[GR_MAX_VOL], cmp[GR_MAX_EXPR];
-#pragma unroll
-    for (int k = 0; k < GR_MAX_VOL; ++k) vol[k] = 0.f;
-#pragma unroll
-    for (int k = 0; k < GR_MAX_EXPR; ++k) cmp[k] = 0.f;
 
-    const bool curv_prev = P.curvature_mode == 1 || P.curvature_mode == 3;
+    const bool curv_prev = curvature_mode == 1 || curvature_mode == 3;
     if (valid) {
         p.x = P.px[i]; p.y = P.py[i];
         if (DIM == 3) p.z = P.pz[i];
         if (curv_prev) { q.x = P.qx[i]; q.y = P.qy[i]; if (DIM == 3) q.z = P.qz[i]; }
-        if (P.compensated) { comp.x = P.kx[i]; comp.y = P.ky[i]; if (DIM == 3) comp.z = P.kz[i]; }
-        if (P.curvature_mode == 2) { ld.x = P.lx[i]; ld.y = P.ly[i]; if (DIM == 3) ld.z = P.lz[i]; }
-        if (P.abort_mode != 0) len = P.length[i];
-        if (P.curvature_mode != 0) tc = P.tc[i];
-        if (P.curvature_mode == 3) cv = P.curv[i];
-#pragma unroll
-        for (int k = 0; k < GR_MAX_VOL; ++k)
-            if (k < P.nvol) vol[k] = P.volc[k * P.n_state + i];
-#pragma unroll
-        for (int k = 0; k < GR_MAX_EXPR; ++k)
-            if (k < P.nexpr) cmp[k] = P.cmpc[k * P.n_state + i];
+        if (compensated) { comp.x = P.kx[i]; comp.y = P.ky[i]; if (DIM == 3) comp.z = P.kz[i]; }
+        if (curvature_mode == 2) { ld.x = P.lx[i]; ld.y = P.ly[i]; if (DIM == 3) ld.z = P.lz[i]; }
+        if (abort_mode != 0) len = P.length[i];
+        if (curvature_mode != 0) tc = P.tc[i];
+        if (curvature_mode == 3) cv = P.curv[i];
     }
     const bool was_alive = alive;
     unsigned long long my_steps = 0;
     const int32_t life = (valid && P.life) ? P.life[i] : 0x7fffffff;   // steps this particle may run
     const int32_t birth = (valid && P.birth) ? P.birth[i] : 0;          // first step it runs
-    const bool extras = (P.volume_mode != 0 && P.nvol > 0) || P.nexpr > 0;
+    const bool extras = LEAN ? (FT & FT_EXTRAS) != 0 : ((P.volume_mode != 0 && P.nvol > 0) || P.nexpr > 0);
     V3 vc_last{0.f, 0.f, 0.f};
     int last_s = P.s0;
     bool dirty = false;   // volumes / expressions not yet evaluated for the last alive step
-    const int sph = P.sphere && DIM == 2;
+    const int sph = !LEAN && P.sphere && DIM == 2;
 
     SampleCache cc;
     cc.reset();
@@ -715,11 +769,11 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
             // displacement, reverse and uplift (tpp:233-250)
             V3 dp{v.x * P.h, v.y * P.h, DIM == 3 ? v.z * P.h : 0.f};
             if (P.reverse) { dp.x = -dp.x; dp.y = -dp.y; dp.z = -dp.z; }
-            if (DIM == 3 && P.uplift_mode != 0) {
-                const int lb = P.uplift_mode == 2 ? E.slot_back : 0, lf = P.uplift_mode == 2 ? E.slot_front : 0;
+            if (DIM == 3 && uplift_mode != 0) {
+                const int lb = uplift_mode == 2 ? E.slot_back : 0, lf = uplift_mode == 2 ? E.slot_front : 0;
                 const float *LB = P.lift + (int64_t)lb * P.n_total * 3 + pid * 3;
                 const float *LF = P.lift + (int64_t)lf * P.n_total * 3 + pid * 3;
-                if (P.uplift_mode == 1) {
+                if (uplift_mode == 1) {
                     dp.x = dp.x + LB[0]; dp.y = dp.y + LB[1]; dp.z = dp.z + LB[2];
                 } else {
                     dp.x = dp.x + lerp_(LB[0], LF[0], t0);
@@ -730,10 +784,10 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
 
             // length abort (tpp:252-280)
             int32_t abort = 0;
-            if (P.abort_mode != 0) {
+            if (abort_mode != 0) {
                 const float dpl = sqrtf(dot3(dp, dp, DIM));
                 const float nl = len + dpl;
-                if (P.abort_mode == 2) {
+                if (abort_mode == 2) {
                     if (nl > P.max_length) {
                         const float sc = (P.max_length - len) / dpl;
                         dp.x = sc * dp.x; dp.y = sc * dp.y; dp.z = sc * dp.z;
@@ -750,7 +804,7 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
 
             // new position (tpp:282); Kahan-compensated in the precision form
             V3 np;
-            if (P.compensated) {
+            if (compensated) {
                 const V3 sd{P.reverse ? -dp.x : dp.x, P.reverse ? -dp.y : dp.y, P.reverse ? -dp.z : dp.z};
                 float y = sd.x - comp.x, t = p.x + y;
                 np.x = t; comp.x = (t - p.x) - y;
@@ -767,10 +821,10 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
             // border and abort checks (tpp:284-323, icc:7-20, tpp:13-96)
             if (abort == 0) {
                 const float dp2 = dot3(dp, dp, DIM);
-                const int bm = DIM == 3 ? 0 : P.border_mode;
+                const int bm = DIM == 3 ? 0 : border_mode;
                 if (bm == 0) {
                     bool topo = false;
-                    if (DIM == 3 && P.topography) {
+                    if (DIM == 3 && topography) {
                         const Cell2 c = make_cell2(P.nx, P.ny, P.filter_weights, np.x / P.scale[0], np.y / P.scale[1]);
                         topo = bil1(P.topo, c) > np.z;
                     }
@@ -819,11 +873,11 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
             st = abort;
             if (abort == 2 || abort == 3 || abort == 4) {
                 // old position kept, total curvature flagged (tpp:327-332)
-                if (P.curvature_mode != 0) tc = -1.f;
+                if (curvature_mode != 0) tc = -1.f;
                 alive = false;
             } else {
                 // curvature (tpp:335-361)
-                if (P.curvature_mode == 2) {
+                if (curvature_mode == 2) {
                     const float inv = 1.0f / sqrtf(dot3(v, v, DIM));
                     const V3 u{v.x * inv, v.y * inv, v.z * inv};
                     if (E.flags & SF_TIME_POS) {
@@ -844,7 +898,7 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
                     }
                     const V3 a{p.x - q.x, p.y - q.y, p.z - q.z}, b{np.x - p.x, np.y - p.y, np.z - p.z};
                     const float ds = 0.5f * (sqrtf(dot3(a, a, DIM)) + sqrtf(dot3(b, b, DIM)));
-                    if (P.curvature_mode == 3) cv = k;
+                    if (curvature_mode == 3) cv = k;
                     if (!isnan(k)) tc += k * ds;
                 }
 
@@ -860,50 +914,64 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
         }
 
         if (valid && (E.flags & SF_SAVE)) {
-            if (extras && dirty) {
-                eval_extras<DIM>(P, P.sched[last_s], pid, p, vc_last, cv, vol, cmp);
-                dirty = false;
-            }
             float *hp = P.hpos + (pid * P.L + E.rec) * DIM;
             hp[0] = p.x; hp[1] = p.y;
             if (DIM == 3) hp[2] = p.z;
-            if (P.curvature_mode == 3 && (E.flags & SF_CURV_REC)) P.hcurv[pid * P.Lc + E.crec] = cv;
-            if (P.volume_mode != 0) {
+            if (curvature_mode == 3 && (E.flags & SF_CURV_REC)) P.hcurv[pid * P.Lc + E.crec] = cv;
+            if (extras) {
+                // volume / expression values: evaluated now if an alive step has passed since the
+                // last evaluation (and kept in the state arrays), else the state arrays' values
+                float vol[GR_MAX_VOL], cmp[GR_MAX_EXPR];
+                load_extras(P, i, dirty, vol, cmp);
+                if (dirty) {
+                    eval_extras<DIM>(P, P.sched[last_s], pid, p, vc_last, cv, vol, cmp);
+                    store_extras(P, i, vol, cmp);
+                    dirty = false;
+                }
+                if (P.volume_mode != 0) {
 #pragma unroll
-                for (int k = 0; k < GR_MAX_VOL; ++k)
-                    if (k < P.nvol) P.hvol[((int64_t)k * P.n_total + pid) * P.Li + E.irec] = vol[k];
+                    for (int k = 0; k < GR_MAX_VOL; ++k)
+                        if (k < P.nvol) P.hvol[((int64_t)k * P.n_total + pid) * P.Li + E.irec] = vol[k];
+                }
+#pragma unroll
+                for (int e = 0; e < GR_MAX_EXPR; ++e)
+                    if (e < P.nexpr) P.hcmp[((int64_t)e * P.n_total + pid) * P.Li + E.irec] = cmp[e];
+                // refill the sample cache for the next step's first sample (at p): the cached
+                // nodes are then dead while the values above are evaluated, which frees their
+                // registers there
+                if constexpr (IsPair<W>::value && DIM == 3) {
+                    const PCell c = make_pcell(P, (p.x - P.off[0]) * P.inv_scale[0], (p.y - P.off[1]) * P.inv_scale[1],
+                                               (p.z - P.off[2]) * P.inv_scale[2]);
+                    fill_padded<typename PairElem<W>::type>(P, P.pair, c.base, cc);
+                }
             }
-#pragma unroll
-            for (int e = 0; e < GR_MAX_EXPR; ++e)
-                if (e < P.nexpr) P.hcmp[((int64_t)e * P.n_total + pid) * P.Li + E.irec] = cmp[e];
         }
 
         // MinimumAliveParticles: particles alive after this step, one atomic per warp, spread
         // over 32 counters so that one address does not serialise the warps of the grid
-        if (P.alive_at) {
+        if (alive_at) {
             const unsigned m = __ballot_sync(0xffffffffu, valid && alive);
             if ((threadIdx.x & 31) == 0 && m)
-                atomicAdd(P.alive_at + (int64_t)(s - P.s0) * 32 + (blockIdx.x & 31), (unsigned)__popc(m));
+                atomicAdd(alive_at + (int64_t)(s - P.s0) * 32 + (blockIdx.x & 31), (unsigned)__popc(m));
         }
     }
 
     if (valid && was_alive) {
-        if (extras && dirty) eval_extras<DIM>(P, P.sched[last_s], pid, p, vc_last, cv, vol, cmp);
+        if (extras && dirty) {
+            float vol[GR_MAX_VOL], cmp[GR_MAX_EXPR];
+            load_extras(P, i, true, vol, cmp);
+            eval_extras<DIM>(P, P.sched[last_s], pid, p, vc_last, cv, vol, cmp);
+            store_extras(P, i, vol, cmp);
+        }
         P.status[i] = st;
         P.px[i] = p.x; P.py[i] = p.y;
         if (DIM == 3) P.pz[i] = p.z;
         if (curv_prev) { P.qx[i] = q.x; P.qy[i] = q.y; if (DIM == 3) P.qz[i] = q.z; }
-        if (P.compensated) { P.kx[i] = comp.x; P.ky[i] = comp.y; if (DIM == 3) P.kz[i] = comp.z; }
-        if (P.curvature_mode == 2) { P.lx[i] = ld.x; P.ly[i] = ld.y; if (DIM == 3) P.lz[i] = ld.z; }
-        if (P.abort_mode != 0) P.length[i] = len;
-        if (P.curvature_mode != 0) P.tc[i] = tc;
-        if (P.curvature_mode == 3) P.curv[i] = cv;
-#pragma unroll
-        for (int k = 0; k < GR_MAX_VOL; ++k)
-            if (k < P.nvol) P.volc[k * P.n_state + i] = vol[k];
-#pragma unroll
-        for (int k = 0; k < GR_MAX_EXPR; ++k)
-            if (k < P.nexpr) P.cmpc[k * P.n_state + i] = cmp[k];
+        if (compensated) { P.kx[i] = comp.x; P.ky[i] = comp.y; if (DIM == 3) P.kz[i] = comp.z; }
+        if (curvature_mode == 2) { P.lx[i] = ld.x; P.ly[i] = ld.y; if (DIM == 3) P.lz[i] = ld.z; }
+        if (abort_mode != 0) P.length[i] = len;
+        if (curvature_mode != 0) P.tc[i] = tc;
+        if (curvature_mode == 3) P.curv[i] = cv;
     }
 
     steps_acc += my_steps;
@@ -915,20 +983,24 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
 // count shrinks, as a captured CUDA graph needs.
 // Launch bounds: 256 threads, 2 blocks per SM (128 registers); the float32 3D pair kernel keeps
 // 48 cached floats and runs 128-thread blocks, 3 per SM (up to 170 registers).
-template <int DIM, typename W> struct AdvBounds { static constexpr int threads = 256, blocks = GR_ADV_MIN_BLOCKS; };
-template <> struct AdvBounds<3, Pair<float>> { static constexpr int threads = 128, blocks = 3; };
+template <int DIM, typename W, int FT> struct AdvBounds { static constexpr int threads = 256, blocks = GR_ADV_MIN_BLOCKS; };
+#ifndef GR_F32_PAIR_BLOCKS
+#define GR_F32_PAIR_BLOCKS 4
+#endif
+template <int FT> struct AdvBounds<3, Pair<float>, FT> { static constexpr int threads = 128, blocks = GR_F32_PAIR_BLOCKS; };
 
-template <int DIM, bool RK4, typename W>
-__global__ void __launch_bounds__(AdvBounds<DIM, W>::threads, AdvBounds<DIM, W>::blocks) advance_kernel(const __grid_constant__ KParams P) {
+template <int DIM, bool RK4, typename W, int FT>
+__global__ void __launch_bounds__(AdvBounds<DIM, W, FT>::threads, AdvBounds<DIM, W, FT>::blocks)
+    advance_kernel(const __grid_constant__ KParams P) {
     const int64_t n_live = P.n_dev ? (int64_t)*P.n_dev : P.n;
     unsigned long long steps = 0;
     unsigned alive = 0;
     if (P.grid_stride) {
         const int64_t stride = (int64_t)gridDim.x * blockDim.x;
         for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n_live; base += stride)
-            advance_particle<DIM, RK4, W>(P, base + threadIdx.x, n_live, steps, alive);
+            advance_particle<DIM, RK4, W, FT>(P, base + threadIdx.x, n_live, steps, alive);
     } else {
-        advance_particle<DIM, RK4, W>(P, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, n_live, steps, alive);
+        advance_particle<DIM, RK4, W, FT>(P, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, n_live, steps, alive);
     }
     // counters: particle-steps and the alive count after the launch (warp-aggregated)
     const unsigned long long warp_steps = __reduce_add_sync(0xffffffffu, (unsigned)steps);

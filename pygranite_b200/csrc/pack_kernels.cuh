@@ -70,4 +70,28 @@ static __global__ void pair_pack_kernel(const T *__restrict__ back, const T *__r
     }
 }
 
+// 3D window pair with a zero border: padded node (x, y, z), x in [-1, nx + 1] and likewise y,
+// z, of a (nx + 3) x (ny + 3) x (nz + 3) buffer holds the back slot's node (x, y, z) followed by
+// the front slot's, or zeros outside the grid (the step kernel's border addressing).  T is one
+// packed node (16 bytes float32, 8 bytes 16-bit); every padded node is written, so the buffer
+// needs no clearing.  The padded node count must stay below 2^31.
+template <typename T>
+static __global__ void pair_pack_padded_kernel(const T *__restrict__ back, const T *__restrict__ front, T *out,
+                                               int32_t nx, int32_t ny, int32_t nz) {
+    const int32_t pnx = nx + 3, pny = ny + 3;
+    const int32_t total = pnx * pny * (nz + 3);
+    for (int32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < total; o += gridDim.x * blockDim.x) {
+        const int32_t x = o % pnx - 1, r = o / pnx;
+        const int32_t y = r % pny - 1, z = r / pny - 1;
+        T b{}, f{};
+        if ((unsigned)x < (unsigned)nx && (unsigned)y < (unsigned)ny && (unsigned)z < (unsigned)nz) {
+            const int64_t i = ((int64_t)z * ny + y) * nx + x;
+            b = back[i];
+            f = front[i];
+        }
+        out[2 * (int64_t)o] = b;
+        out[2 * (int64_t)o + 1] = f;
+    }
+}
+
 }  // namespace granite_b200

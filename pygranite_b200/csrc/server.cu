@@ -246,21 +246,35 @@ __global__ void planar_pack_kernel(const float *__restrict__ u, const float *__r
 
 // Two planar slots -> the window-pair layout the step kernel reads: per node
 // {u_b, v_b, w_b, 0, u_f, v_f, w_f, 0} (3D) or {u_b, v_b, u_f, v_f} (2D), vector stores.
+// 3D pairs carry the zero border of pair_pack_padded_kernel (pack_kernels.cuh): every padded
+// node (nx + 3) x (ny + 3) x (nz + 3) is written, zeros outside the grid.
 template <typename T>
 __global__ void planar_pair_kernel(const T *__restrict__ b, const T *__restrict__ f, T *__restrict__ out,
-                                   int64_t nodes, int dim) {
+                                   int64_t nodes, int dim, int32_t nx, int32_t ny, int32_t nz) {
     using V = typename std::conditional<sizeof(T) == 4, uint4, uint2>::type;   // 4 values of T
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
-        if (dim == 3) {
-            alignas(sizeof(V)) T lo[4] = {b[i], b[nodes + i], b[2 * nodes + i], to_storage<T>(0.f)};
-            alignas(sizeof(V)) T hi[4] = {f[i], f[nodes + i], f[2 * nodes + i], to_storage<T>(0.f)};
-            V *o = reinterpret_cast<V *>(out + 8 * i);
-            o[0] = *reinterpret_cast<const V *>(lo);
-            o[1] = *reinterpret_cast<const V *>(hi);
-        } else {
-            alignas(sizeof(V)) T q[4] = {b[i], b[nodes + i], f[i], f[nodes + i]};
-            *reinterpret_cast<V *>(out + 4 * i) = *reinterpret_cast<const V *>(q);
+    if (dim == 3) {
+        const int32_t pnx = nx + 3, pny = ny + 3;
+        const int32_t total = pnx * pny * (nz + 3);
+        for (int32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < total; o += gridDim.x * blockDim.x) {
+            const int32_t x = o % pnx - 1, r = o / pnx;
+            const int32_t y = r % pny - 1, z = r / pny - 1;
+            const T zero = to_storage<T>(0.f);
+            alignas(sizeof(V)) T lo[4] = {zero, zero, zero, zero};
+            alignas(sizeof(V)) T hi[4] = {zero, zero, zero, zero};
+            if ((unsigned)x < (unsigned)nx && (unsigned)y < (unsigned)ny && (unsigned)z < (unsigned)nz) {
+                const int64_t i = ((int64_t)z * ny + y) * nx + x;
+                lo[0] = b[i]; lo[1] = b[nodes + i]; lo[2] = b[2 * nodes + i];
+                hi[0] = f[i]; hi[1] = f[nodes + i]; hi[2] = f[2 * nodes + i];
+            }
+            V *po = reinterpret_cast<V *>(out + 8 * (int64_t)o);
+            po[0] = *reinterpret_cast<const V *>(lo);
+            po[1] = *reinterpret_cast<const V *>(hi);
         }
+        return;
+    }
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+        alignas(sizeof(V)) T q[4] = {b[i], b[nodes + i], f[i], f[nodes + i]};
+        *reinterpret_cast<V *>(out + 4 * i) = *reinterpret_cast<const V *>(q);
     }
 }
 
@@ -293,7 +307,11 @@ int setup(gr_server *S, int64_t nz, int64_t ny, int64_t nx) {
     S->snap_bytes = S->nodes * S->dim * S->elem;                  // planar, unpadded
     S->slot_stride = ((S->snap_bytes + 255) / 256) * 256;
     SK(S->ring.alloc((size_t)S->slot_stride * kRing));
-    SK(S->pair.alloc((size_t)S->nodes * (S->dim == 3 ? 8 : 4) * S->elem));
+    // 3D window pairs carry a zero border (padded_pair_nodes); the kernel indexes them with int32
+    if ((S->dim == 3 ? padded_pair_nodes(S->nx, S->ny, S->nz) : S->nodes) > (int64_t(1) << 31) - 1)
+        return SUSER("Invalid dataset was provided. Grid too large.");
+    SK(S->pair.alloc(S->dim == 3 ? (size_t)padded_pair_nodes(S->nx, S->ny, S->nz) * 8 * S->elem
+                                 : (size_t)S->nodes * 4 * S->elem));
     SK(S->raw.alloc((size_t)S->nodes * S->dim));
     S->host_snap.assign((size_t)S->n_snap, nullptr);
     for (int k = 0; k < kRing; ++k) S->ring_holds[k] = -1;
@@ -354,8 +372,12 @@ int allocate(gr_server *S, int64_t budget) {
         SK(cudaGetLastError());
         P.threads = 256;
         const int st = S->s.storage;
-        P.fn = st == GR_STORE_BF16 ? advance_bf16(S->dim, p == 1, true)
-             : st == GR_STORE_F16 ? advance_f16(S->dim, p == 1, true) : advance_f32(S->dim, p == 1, true);
+        // positions only (no curvature, volumes, constants, uplift, length abort, compensation):
+        // the lean variant unless 2D loop borders or sphere coordinates are on
+        const bool lean = !(S->dim == 2 && (S->s.border_mode != 0 || S->s.sphere_radius > 0.f));
+        const int ft = lean ? FT_LEAN : FT_GENERIC;
+        P.fn = st == GR_STORE_BF16 ? advance_bf16(S->dim, p == 1, true, ft)
+             : st == GR_STORE_F16 ? advance_f16(S->dim, p == 1, true, ft) : advance_f32(S->dim, p == 1, true, ft);
         cudaFuncAttributes fa{};
         SK(cudaFuncGetAttributes(&fa, reinterpret_cast<const void *>(P.fn)));
         P.threads = std::min(P.threads, fa.maxThreadsPerBlock);   // the kernel's launch bounds
@@ -388,6 +410,7 @@ KParams pool_params(gr_server *S, Pool &P) {
     K.wind = S->ring.p;
     K.wind_stride = S->slot_stride;
     K.pair = S->pair.p;
+    K.pnx = (int32_t)(S->nx + 3); K.pnxy = (int32_t)((S->nx + 3) * (S->ny + 3));
     Pool::Arrays &A = P.st[P.cur];
     K.px = A.px.p; K.py = A.py.p; K.pz = A.pz.p;
     K.status = A.status.p; K.id = A.id.p; K.life = A.life.p; K.birth = A.birth.p;
@@ -482,15 +505,18 @@ int pack_pair(gr_server *S, int64_t v) {
     switch (S->s.storage) {
         case GR_STORE_BF16:
             planar_pair_kernel<__nv_bfloat16><<<blocks, threads, 0, S->cs>>>(
-                (const __nv_bfloat16 *)back, (const __nv_bfloat16 *)front, (__nv_bfloat16 *)S->pair.p, S->nodes, S->dim);
+                (const __nv_bfloat16 *)back, (const __nv_bfloat16 *)front, (__nv_bfloat16 *)S->pair.p, S->nodes, S->dim,
+                (int32_t)S->nx, (int32_t)S->ny, (int32_t)S->nz);
             break;
         case GR_STORE_F16:
             planar_pair_kernel<__half><<<blocks, threads, 0, S->cs>>>((const __half *)back, (const __half *)front,
-                                                                     (__half *)S->pair.p, S->nodes, S->dim);
+                                                                     (__half *)S->pair.p, S->nodes, S->dim,
+                                                                     (int32_t)S->nx, (int32_t)S->ny, (int32_t)S->nz);
             break;
         default:
             planar_pair_kernel<float><<<blocks, threads, 0, S->cs>>>((const float *)back, (const float *)front,
-                                                                    (float *)S->pair.p, S->nodes, S->dim);
+                                                                    (float *)S->pair.p, S->nodes, S->dim,
+                                                                    (int32_t)S->nx, (int32_t)S->ny, (int32_t)S->nz);
             break;
     }
     SK(cudaGetLastError());

@@ -9,7 +9,9 @@ The inputs are regenerated from seeds by pygranite_b200.workloads, so the fixtur
 the reference's outputs: positions every 10 steps, abort codes and, for the 3D case, total
 curvature, the temperature samples and the expression values; and, in filter_reference.npz,
 one Euler step through a field equal to its own grid coordinates (2D and 3D), which exposes
-the texture filter's interpolation weights.  The reference filters through
+the texture filter's interpolation weights; in options_reference.npz, the option combinations
+of OPTION_CASES (loop borders, sphere coordinates, FastTotal / Individual curvature, length and
+fit-length aborts, uplift, topography, constants, constant wind, reverse).  The reference filters through
 texture hardware with 8-bit interpolation weights, so its outputs are matched within a
 tolerance, not bit for bit.
 """
@@ -60,6 +62,79 @@ def filter_case(dim, n=12288):
     return settings, W.SnapshotSource(wind), seeds
 
 
+# ------------------------------------------------------------ the option matrix
+# Option combinations of the reference's kernel beyond the two benchmark configurations, each
+# instantiated unmodified by oracle/ref_harness (OPT_VARIANTS).  2D: a 32 x 24 Fourier field (1 km)
+# or a 36 x 18 field in degrees for sphere coordinates; 3D: a 24 x 20 x 12 field (1 km, 250 m).
+OPTION_CASES = {
+    "2d_loopx_euler": dict(Integrator=0, BorderMode=1),
+    "2d_loopy_rk4": dict(BorderMode=2),
+    "2d_loopxy_rk4": dict(BorderMode=3),
+    "2d_loopxy_sphere": dict(BorderMode=3, SphereRadius=6.371e6),
+    "2d_loopy_sphere_euler": dict(Integrator=0, BorderMode=2, SphereRadius=6.371e6),
+    "2d_fasttotal_reverse": dict(CurvatureMode=2, Reverse=True),
+    "2d_windfield_constant": dict(WindfieldMode=0),
+    "2d_loopx_fasttotal_sphere": dict(BorderMode=1, CurvatureMode=2, SphereRadius=6.371e6),
+    "3d_individual_length": dict(CurvatureMode=3, AbortMode=1, MaximumLength=15000.0),
+    "3d_fitlength_uplift_constant_euler": dict(Integrator=0, AbortMode=2, MaximumLength=15000.0, UpLiftMode=1),
+    "3d_uplift_dynamic_topography": dict(UpLiftMode=2, topography=True),
+    "3d_constants_volume_expression": dict(CurvatureMode=1, ConstantsMode=1, AdditionalVolumeMode=1,
+                                           AdditionalCompute=["T*ka + kb - z/1000"]),
+    "3d_constants_dynamic_reverse": dict(ConstantsMode=2, Reverse=True, AdditionalCompute=["ka*u + kb*v"]),
+    "3d_constant_wind_length_reverse_euler": dict(Integrator=0, CurvatureMode=1, AbortMode=1,
+                                                  MaximumLength=12000.0, WindfieldMode=0, Reverse=True),
+}
+OPTION_N = 400
+
+
+def option_case(name):
+    """Settings and inputs of an option-matrix case, regenerated from seeds: (settings, wind,
+    seeds, volumes, constants, uplift, topography)."""
+    opts = dict(OPTION_CASES[name])
+    topo = opts.pop("topography", False)
+    dim = 2 if name.startswith("2d") else 3
+    seed = sum(map(ord, name)) % 1000
+    n_snap = 8
+    rng = np.random.default_rng(seed)
+    volumes = constants = uplift = topography = None
+    if dim == 2:
+        sphere = opts.get("SphereRadius", 0.0) > 0
+        shape = (18, 36) if sphere else (24, 32)
+        field = W.FourierField(shape, (1000.0, 1000.0), n_modes=16, seed=seed, rms=(7.0710678, 7.0710678))
+        base = dict(Space=1, Integrator=1, WindfieldMode=1, DeltaT=60.0, DataTimeDistance=600.0,
+                    GridScale=[1000.0, 1000.0], Offset=[0.0, 0.0], SaveInterval=5, BorderMode=0, CurvatureMode=0,
+                    MaximumSimulationTime=3600.0)
+        lo, hi = [0.0, 0.0], [32000.0, 24000.0]
+        if sphere:
+            # degrees: 10-degree cells, latitude -90..90, 10-hour steps
+            base.update(GridScale=[10.0, 10.0], Offset=[0.0, -90.0], DeltaT=36000.0, DataTimeDistance=360000.0,
+                        MaximumSimulationTime=36000.0 * 60)
+            lo, hi = [0.0, -85.0], [360.0, 85.0]
+        wind = [field.snapshot(600.0 * k) for k in range(n_snap)]
+    else:
+        shape = (12, 20, 24)
+        field = W.FourierField(shape, (250.0, 1000.0, 1000.0), n_modes=16, seed=seed)
+        base = dict(Space=0, Integrator=1, WindfieldMode=1, DeltaT=60.0, DataTimeDistance=600.0,
+                    GridScale=[1000.0, 1000.0, 250.0], Offset=[0.0, 0.0, 0.0], SaveInterval=5, BorderMode=0,
+                    CurvatureMode=0, MaximumSimulationTime=3600.0)
+        lo, hi = [0.0, 0.0, 0.0], [24000.0, 20000.0, 1500.0]
+        wind = [field.snapshot(600.0 * k) for k in range(n_snap)]
+    settings = dict(base, **opts)
+    seeds = W.uniform_seeds(OPTION_N, seed + 1, lo, hi)
+    if settings.get("AdditionalVolumeMode", 0):
+        volumes = [{"T": W.temperature(shape, 250.0, seed=seed + 2)}]
+    if settings.get("ConstantsMode", 0):
+        constants = [{"ka": rng.uniform(0.5, 1.5, OPTION_N).astype(np.float32),
+                      "kb": rng.uniform(-2.0, 2.0, OPTION_N).astype(np.float32)} for _ in range(n_snap)]
+    if settings.get("UpLiftMode", 0):
+        uplift = [(rng.standard_normal((OPTION_N, 3)) * np.array([40.0, 40.0, 15.0])).astype(np.float32)
+                  for _ in range(n_snap)]
+    if topo:
+        topography = np.zeros(shape[1:], np.float32)
+        topography[:, 16:] = 900.0          # a plateau in x >= 16 km, 900 m high
+    return settings, wind, seeds, volumes, constants, uplift, topography
+
+
 def main(out):
     os.makedirs(out, exist_ok=True)
     settings, src, seeds = gyre_case()
@@ -80,6 +155,19 @@ def main(out):
         arrays[f"positions{dim}d"] = r["trajectories"][:, 1]     # record 0 is the seeds
         arrays[f"status{dim}d"] = r["status"]
     np.savez_compressed(os.path.join(out, "filter_reference.npz"), **arrays)
+    options = {}
+    for name in OPTION_CASES:
+        settings, wind, seeds, volumes, constants, uplift, topography = option_case(name)
+        r = refrun.run_options(settings, wind, seeds, volumes=volumes, constants=constants, uplift=uplift,
+                               topography=topography)
+        for k in ("trajectories", "status", "total_curvature", "lengths", "curvatures"):
+            options[f"{name}/{k}"] = r[k]
+        for k, v in r["volume_info"].items():
+            options[f"{name}/volume_{k}"] = v
+        if r["compute_info"]:
+            options[f"{name}/compute_0"] = r["compute_info"][0]
+        options[f"{name}/steps"] = np.int64(r["steps"])
+    np.savez_compressed(os.path.join(out, "options_reference.npz"), **options)
     print("fixtures written to", out)
 
 
