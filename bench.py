@@ -220,8 +220,8 @@ def plain_oracle(settings, src, seeds, ids):
 def check_plain(got, ref32, ref64):
     """got: the sampled rows of a run (trajectories, status, total_curvature, T samples,
     expression values).  Bit-for-bit comparison with the float32 oracle, and the position
-    error in grid cells against the float64 oracle after 100 steps (record 10) and at the end,
-    over particles not yet aborted in either run at that record."""
+    error in grid cells against the float64 oracle after 100 and 400 steps (records 10, 40) and at
+    the end, over particles not yet aborted in either run at that record."""
     traj, status = got["trajectories"], got["status"]
     checks = {
         "positions": bool(np.array_equal(traj, ref32["trajectories"])),
@@ -233,7 +233,7 @@ def check_plain(got, ref32, ref64):
     bad = np.any(traj != ref32["trajectories"], axis=(1, 2)) | (status != ref32["status"])
     L = traj.shape[1]
     f64 = {}
-    for rec in sorted({min(10, L - 1), L - 1}):
+    for rec in sorted({min(10, L - 1), min(40, L - 1), L - 1}):
         k = 10 * rec
         live = ((ref64["step_of_abort"] < 0) | (ref64["step_of_abort"] >= k)) & \
                ((ref32["step_of_abort"] < 0) | (ref32["step_of_abort"] >= k))

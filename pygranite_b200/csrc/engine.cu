@@ -307,7 +307,7 @@ int setup_grid(gr_engine *e, int64_t nz, int64_t ny, int64_t nx) {
     e->nx = nx; e->ny = ny; e->nz = e->dim == 3 ? nz : 1;
     e->nodes = e->nx * e->ny * e->nz;
     // the step kernel indexes nodes (and the padded 3D window pair) with 32-bit integers
-    if ((e->dim == 3 ? padded_pair_nodes(e->nx, e->ny, e->nz) : e->nodes) > (int64_t(1) << 31) - 1)
+    if (padded_pair_nodes(e->dim, e->nx, e->ny, e->nz) > (int64_t(1) << 31) - 1)
         return USER_ERR("Invalid dataset was provided. Grid too large. >");
     const gr_settings &s = e->s;
     // GridScale / Offset / Domain (TrajectoryIntegrator.tpp:521-574)
@@ -953,10 +953,10 @@ int pair_elem(const gr_engine *e) {
     return e->s.storage == GR_STORE_F32 ? (e->dim == 3 ? 16 : 8) : (e->dim == 3 ? 8 : 4);
 }
 
-// Bytes of one window-pair buffer: 3D pairs carry a zero border (pair_pack_padded_kernel).
+// Bytes of one window-pair buffer: pairs carry a border (pair_pack_padded_kernel,
+// pair_pack_edge2_kernel).
 size_t pair_bytes(const gr_engine *e) {
-    const int64_t nodes = e->dim == 3 ? padded_pair_nodes(e->nx, e->ny, e->nz) : e->nodes;
-    return (size_t)nodes * 2 * pair_elem(e);
+    return (size_t)padded_pair_nodes(e->dim, e->nx, e->ny, e->nz) * 2 * pair_elem(e);
 }
 
 // Validation, schedule, device schedule and programs, state and history buffers.
@@ -1323,12 +1323,15 @@ int pack_pair(gr_engine *e, int64_t w, cudaStream_t stream) {
         else
             pair_pack_padded_kernel<uint2><<<blocks, threads, 0, stream>>>((const uint2 *)back, (const uint2 *)front,
                                                                           (uint2 *)e->pairbuf[b].p, nx, ny, nz);
-    } else if (elem == 16)
-        pair_pack_kernel<uint4><<<blocks, threads, 0, stream>>>((const uint4 *)back, (const uint4 *)front, (uint4 *)e->pairbuf[b].p, e->nodes);
-    else if (elem == 8)
-        pair_pack_kernel<uint2><<<blocks, threads, 0, stream>>>((const uint2 *)back, (const uint2 *)front, (uint2 *)e->pairbuf[b].p, e->nodes);
-    else
-        pair_pack_kernel<unsigned><<<blocks, threads, 0, stream>>>((const unsigned *)back, (const unsigned *)front, (unsigned *)e->pairbuf[b].p, e->nodes);
+    } else {
+        const int32_t nx = (int32_t)e->nx, ny = (int32_t)e->ny;
+        if (elem == 8)
+            pair_pack_edge2_kernel<uint2><<<blocks, threads, 0, stream>>>((const uint2 *)back, (const uint2 *)front,
+                                                                         (uint2 *)e->pairbuf[b].p, nx, ny);
+        else
+            pair_pack_edge2_kernel<unsigned><<<blocks, threads, 0, stream>>>(
+                (const unsigned *)back, (const unsigned *)front, (unsigned *)e->pairbuf[b].p, nx, ny);
+    }
     CK(cudaGetLastError());
     e->pair_window[b] = w;
     e->stats.aux_launches++;

@@ -56,9 +56,10 @@ struct KParams {
     const void *wind;
     int64_t wind_stride;          // bytes per slot
     const void *pair;             // window-pair buffer of the launch's window (pair layouts)
-    int32_t pnx, pnxy;            // 3D window pair: padded row length (nx + 3) and plane size
+    int32_t pnx, pnxy;            // window pair: padded row length (nx + 3) and plane size
                                   // ((nx + 3) * (ny + 3)); node (x, y, z) at
-                                  // (z + 1) * pnxy + (y + 1) * pnx + (x + 1), zeros outside the grid
+                                  // (z + 1) * pnxy + (y + 1) * pnx + (x + 1): zeros outside the
+                                  // grid in 3D, the clamped edge node in 2D
     const float *vol;             // [slot][8][plane]
     int64_t vol_plane;            // floats per plane
     const float *cons;            // [slot][4][n_total]
@@ -165,7 +166,8 @@ template <> struct Store<__half> {
 
 // Window-pair layouts: node n holds the back snapshot's node followed by the front
 // snapshot's node, so one load returns both (32 bytes for float32 3D, 16 bytes for 16-bit 3D or
-// float32 2D, 8 bytes for 16-bit 2D).  Built per window by pair_pack_kernel from the ring.
+// float32 2D, 8 bytes for 16-bit 2D).  Built per window from the ring (pack_kernels.cuh), with a
+// border (make_pcell, bil2p_padded).
 template <typename W> struct Pair {};
 
 template <typename W> struct IsPair { static constexpr bool value = false; };
@@ -269,20 +271,16 @@ __device__ __forceinline__ float tri_corners(const float (&c)[8], const Cell3 &c
 
 // Pair nodes of the last cell a particle sampled (window-pair layouts).  Consecutive samples of
 // one particle (its RK4 stages, its next step) mostly fall in the same cell, whose nodes then
-// need no new gathers; the values and the arithmetic are the same either way.  In 3D the cell is
-// identified by its first corner's index in the padded pair buffer (`base`); 16-bit kernels keep
-// the raw nodes (32 registers), the float32 kernel the 48 floats (AdvBounds gives its launch
-// shape); 2D keeps the 4 corners as floats (16 registers), keyed by their indices.
+// need no new gathers; the values and the arithmetic are the same either way.  The cell is
+// identified by its first corner's index in the padded pair buffer (`base`); 3D 16-bit kernels
+// keep the raw nodes (32 registers), the float32 kernel the 48 floats (AdvBounds gives its launch
+// shape); 2D keeps the 4 corners as floats (16 registers).
 struct SampleCache {
     int32_t base;
     uint4 q[8];
-    int32_t i00, i10, i01, i11;
     float b2[4][2], f2[4][2];
     float c32[6][8];   // float32 3D: u, v, w back and front of the 8 corners
-    __device__ __forceinline__ void reset() {
-        base = -1;
-        i00 = i10 = i01 = i11 = -1;
-    }
+    __device__ __forceinline__ void reset() { base = -1; }
 };
 
 // 3D window pair with a zero border (one node below, two above the grid on every axis): the
@@ -291,8 +289,11 @@ struct SampleCache {
 // Same values as make_cell3 + border addressing: inside [-1, n] the cell and fraction are
 // identical; outside it every corner the original reads is outside the grid (0), and here the
 // fraction is 0 with the weighted-away corner finite, so the interpolation is +0 either way.
-// Padded node count of a 3D window-pair buffer.
-inline int64_t padded_pair_nodes(int64_t nx, int64_t ny, int64_t nz) { return (nx + 3) * (ny + 3) * (nz + 3); }
+// Padded node count of a window-pair buffer: (nx + 3) (ny + 3) (nz + 3) in 3D, (nx + 3) (ny + 3)
+// in 2D.
+inline int64_t padded_pair_nodes(int dim, int64_t nx, int64_t ny, int64_t nz) {
+    return (nx + 3) * (ny + 3) * (dim == 3 ? nz + 3 : 1);
+}
 
 struct PCell {
     int32_t base;        // padded node index of corner (ix, iy, iz)
@@ -417,35 +418,31 @@ __device__ __forceinline__ void bil2(const void *slot, const Cell2 &c, float &ou
     ov = lerp_(lerp_(v0, v1, c.fx), lerp_(v2, v3, c.fx), c.fy);
 }
 
+// 2D window pair with replicated edges: padded node (x, y), x in [-1, nx + 1] and y in
+// [-1, ny + 1], of a (nx + 3) x (ny + 3) buffer holds node (clamp(x), clamp(y)), so a coordinate
+// clamped to [-1, n] reads the clamp-addressed corners of make_cell2 without index clamps.  Same
+// values: inside [-1, n] cell, fraction and corners are unchanged; outside it both corners of the
+// axis are the same edge node, interpolated with any fraction to that node's value exactly.
+// The cache keeps the 4 corners as floats (16 registers), keyed by the first corner's index.
 template <typename W>
-__device__ __forceinline__ void bil2p(const void *pairs, const Cell2 &c, float (&ob)[2], float (&of)[2]) {
-    float b0[2], f0[2], b1[2], f1[2], b2[2], f2[2], b3[2], f3[2];
-    Store<W>::load2p(pairs, c.i00, b0, f0);
-    Store<W>::load2p(pairs, c.i10, b1, f1);
-    Store<W>::load2p(pairs, c.i01, b2, f2);
-    Store<W>::load2p(pairs, c.i11, b3, f3);
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        ob[k] = lerp_(lerp_(b0[k], b1[k], c.fx), lerp_(b2[k], b3[k], c.fx), c.fy);
-        of[k] = lerp_(lerp_(f0[k], f1[k], c.fx), lerp_(f2[k], f3[k], c.fx), c.fy);
-    }
-}
-
-// 2D: the 4 corners of the last cell, converted to float; bil2p's arithmetic.
-template <typename W>
-__device__ __forceinline__ void bil2p_cached(const void *pairs, const Cell2 &c, SampleCache &cc, float (&ob)[2],
-                                             float (&of)[2]) {
-    if (c.i00 != cc.i00 || c.i10 != cc.i10 || c.i01 != cc.i01 || c.i11 != cc.i11) {
-        Store<W>::load2p(pairs, c.i00, cc.b2[0], cc.f2[0]);
-        Store<W>::load2p(pairs, c.i10, cc.b2[1], cc.f2[1]);
-        Store<W>::load2p(pairs, c.i01, cc.b2[2], cc.f2[2]);
-        Store<W>::load2p(pairs, c.i11, cc.b2[3], cc.f2[3]);
-        cc.i00 = c.i00; cc.i10 = c.i10; cc.i01 = c.i01; cc.i11 = c.i11;
+__device__ __forceinline__ void bil2p_padded(const KParams &P, const void *pairs, float ax, float ay, SampleCache &cc,
+                                             float (&ob)[2], float (&of)[2]) {
+    int ix, iy;
+    float fx, fy;
+    pcell1(ax, P.nx, P.filter_weights, ix, fx);
+    pcell1(ay, P.ny, P.filter_weights, iy, fy);
+    const int32_t base = (iy + 1) * P.pnx + (ix + 1);
+    if (base != cc.base) {
+        Store<W>::load2p(pairs, base, cc.b2[0], cc.f2[0]);
+        Store<W>::load2p(pairs, base + 1, cc.b2[1], cc.f2[1]);
+        Store<W>::load2p(pairs, base + P.pnx, cc.b2[2], cc.f2[2]);
+        Store<W>::load2p(pairs, base + P.pnx + 1, cc.b2[3], cc.f2[3]);
+        cc.base = base;
     }
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
-        ob[k] = lerp_(lerp_(cc.b2[0][k], cc.b2[1][k], c.fx), lerp_(cc.b2[2][k], cc.b2[3][k], c.fx), c.fy);
-        of[k] = lerp_(lerp_(cc.f2[0][k], cc.f2[1][k], c.fx), lerp_(cc.f2[2][k], cc.f2[3][k], c.fx), c.fy);
+        ob[k] = lerp_(lerp_(cc.b2[0][k], cc.b2[1][k], fx), lerp_(cc.b2[2][k], cc.b2[3][k], fx), fy);
+        of[k] = lerp_(lerp_(cc.f2[0][k], cc.f2[1][k], fx), lerp_(cc.f2[2][k], cc.f2[3][k], fx), fy);
     }
 }
 
@@ -486,9 +483,8 @@ __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, co
                 tri3p_padded16<H>(P, wb, c, cc, b, f);
             r.x = lerp_(b[0], f[0], t); r.y = lerp_(b[1], f[1], t); r.z = lerp_(b[2], f[2], t);
         } else {
-            const Cell2 c = make_cell2(P.nx, P.ny, P.filter_weights, ax, ay);
             float b[2], f[2];
-            bil2p_cached<W>(wb, c, cc, b, f);
+            bil2p_padded<W>(P, wb, ax, ay, cc, b, f);
             r.x = lerp_(b[0], f[0], t); r.y = lerp_(b[1], f[1], t);
         }
         return r;
@@ -739,24 +735,32 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
             // integrator (tpp:135-231)
             V3 v, vc;
             if (RK4) {
-                const float t1 = E.t1, t2 = E.t2;
-                const V3 k1c = wind_at<DIM, W>(P, p, t0, wb, wf, cc);
-                const V3 k1 = sph ? sphere_(P, p.y, k1c) : k1c;
-                V3 a{__fmaf_rn(k1.x, P.hh, p.x), __fmaf_rn(k1.y, P.hh, p.y), DIM == 3 ? __fmaf_rn(k1.z, P.hh, p.z) : 0.f};
-                const V3 k2c = wind_at<DIM, W>(P, a, t1, wb, wf, cc);
-                const V3 k2 = sph ? sphere_(P, a.y, k2c) : k2c;
-                a = V3{__fmaf_rn(k2.x, P.hh, p.x), __fmaf_rn(k2.y, P.hh, p.y), DIM == 3 ? __fmaf_rn(k2.z, P.hh, p.z) : 0.f};
-                const V3 k3c = wind_at<DIM, W>(P, a, t1, wb, wf, cc);
-                const V3 k3 = sph ? sphere_(P, a.y, k3c) : k3c;
-                a = V3{__fmaf_rn(k3.x, P.h, p.x), __fmaf_rn(k3.y, P.h, p.y), DIM == 3 ? __fmaf_rn(k3.z, P.h, p.z) : 0.f};
-                const V3 k4c = wind_at<DIM, W>(P, a, t2, wb, wf, cc);
-                const V3 k4 = sph ? sphere_(P, a.y, k4c) : k4c;
-                v.x = (((k1.x + 2.f * k2.x) + 2.f * k3.x) + k4.x) * P.sixth;
-                v.y = (((k1.y + 2.f * k2.y) + 2.f * k3.y) + k4.y) * P.sixth;
-                v.z = DIM == 3 ? (((k1.z + 2.f * k2.z) + 2.f * k3.z) + k4.z) * P.sixth : 0.f;
+                // the four stages as one loop (one copy of the sampling code, which keeps the
+                // step loop within the instruction cache): stage k samples at a with its time
+                // weight, and the sum ((k1 + 2 k2) + 2 k3) + k4 is accumulated in that order
+                V3 a = p, acc{0.f, 0.f, 0.f}, accc{0.f, 0.f, 0.f};
+#pragma unroll 1
+                for (int stage = 0; stage < 4; ++stage) {
+                    const float tw = stage == 0 ? t0 : (stage == 3 ? E.t2 : E.t1);
+                    const V3 kc = wind_at<DIM, W>(P, a, tw, wb, wf, cc);
+                    const V3 k = sph ? sphere_(P, a.y, kc) : kc;
+                    if (stage == 0) {
+                        acc = k;
+                        accc = kc;
+                    } else {
+                        const float wgt = stage == 3 ? 1.f : 2.f;   // 1 * k is exact: the same sum
+                        acc = V3{acc.x + wgt * k.x, acc.y + wgt * k.y, acc.z + wgt * k.z};
+                        if (sph) accc = V3{accc.x + wgt * kc.x, accc.y + wgt * kc.y, 0.f};
+                    }
+                    const float c = stage < 2 ? P.hh : P.h;
+                    a = V3{__fmaf_rn(k.x, c, p.x), __fmaf_rn(k.y, c, p.y), DIM == 3 ? __fmaf_rn(k.z, c, p.z) : 0.f};
+                }
+                v.x = acc.x * P.sixth;
+                v.y = acc.y * P.sixth;
+                v.z = DIM == 3 ? acc.z * P.sixth : 0.f;
                 if (sph) {
-                    vc.x = (((k1c.x + 2.f * k2c.x) + 2.f * k3c.x) + k4c.x) * P.sixth;
-                    vc.y = (((k1c.y + 2.f * k2c.y) + 2.f * k3c.y) + k4c.y) * P.sixth;
+                    vc.x = accc.x * P.sixth;
+                    vc.y = accc.y * P.sixth;
                     vc.z = 0.f;
                 } else {
                     vc = v;

@@ -60,13 +60,20 @@ __global__ void pack_wind_kernel<__half>(const float *__restrict__ u, const floa
     }
 }
 
-// Window pair: node n of the pair buffer = node n of the back slot followed by node n of the
-// front slot (elements of E bytes, E = 4, 8 or 16).
+// 2D window pair with replicated edges: padded node (x, y), x in [-1, nx + 1], y in [-1, ny + 1],
+// of a (nx + 3) x (ny + 3) buffer holds the back slot's node (clamp(x), clamp(y)) followed by the
+// front slot's (the step kernel's clamp addressing).  T is one packed node (8 bytes float32, 4
+// bytes 16-bit); every padded node is written.
 template <typename T>
-static __global__ void pair_pack_kernel(const T *__restrict__ back, const T *__restrict__ front, T *out, int64_t nodes) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
-        out[2 * i] = back[i];
-        out[2 * i + 1] = front[i];
+static __global__ void pair_pack_edge2_kernel(const T *__restrict__ back, const T *__restrict__ front, T *out,
+                                              int32_t nx, int32_t ny) {
+    const int32_t pnx = nx + 3;
+    const int32_t total = pnx * (ny + 3);
+    for (int32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < total; o += gridDim.x * blockDim.x) {
+        const int32_t x = min(max(o % pnx - 1, 0), nx - 1), y = min(max(o / pnx - 1, 0), ny - 1);
+        const int64_t i = (int64_t)y * nx + x;
+        out[2 * (int64_t)o] = back[i];
+        out[2 * (int64_t)o + 1] = front[i];
     }
 }
 

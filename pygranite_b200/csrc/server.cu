@@ -247,7 +247,8 @@ __global__ void planar_pack_kernel(const float *__restrict__ u, const float *__r
 // Two planar slots -> the window-pair layout the step kernel reads: per node
 // {u_b, v_b, w_b, 0, u_f, v_f, w_f, 0} (3D) or {u_b, v_b, u_f, v_f} (2D), vector stores.
 // 3D pairs carry the zero border of pair_pack_padded_kernel (pack_kernels.cuh): every padded
-// node (nx + 3) x (ny + 3) x (nz + 3) is written, zeros outside the grid.
+// node (nx + 3) x (ny + 3) x (nz + 3) is written, zeros outside the grid; 2D pairs replicate the
+// edge nodes.
 template <typename T>
 __global__ void planar_pair_kernel(const T *__restrict__ b, const T *__restrict__ f, T *__restrict__ out,
                                    int64_t nodes, int dim, int32_t nx, int32_t ny, int32_t nz) {
@@ -272,9 +273,14 @@ __global__ void planar_pair_kernel(const T *__restrict__ b, const T *__restrict_
         }
         return;
     }
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nodes; i += (int64_t)gridDim.x * blockDim.x) {
+    // 2D: replicated edges (pair_pack_edge2_kernel, pack_kernels.cuh)
+    const int32_t pnx = nx + 3;
+    const int32_t total = pnx * (ny + 3);
+    for (int32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < total; o += gridDim.x * blockDim.x) {
+        const int32_t x = min(max(o % pnx - 1, 0), nx - 1), y = min(max(o / pnx - 1, 0), ny - 1);
+        const int64_t i = (int64_t)y * nx + x;
         alignas(sizeof(V)) T q[4] = {b[i], b[nodes + i], f[i], f[nodes + i]};
-        *reinterpret_cast<V *>(out + 4 * i) = *reinterpret_cast<const V *>(q);
+        *reinterpret_cast<V *>(out + 4 * (int64_t)o) = *reinterpret_cast<const V *>(q);
     }
 }
 
@@ -307,11 +313,10 @@ int setup(gr_server *S, int64_t nz, int64_t ny, int64_t nx) {
     S->snap_bytes = S->nodes * S->dim * S->elem;                  // planar, unpadded
     S->slot_stride = ((S->snap_bytes + 255) / 256) * 256;
     SK(S->ring.alloc((size_t)S->slot_stride * kRing));
-    // 3D window pairs carry a zero border (padded_pair_nodes); the kernel indexes them with int32
-    if ((S->dim == 3 ? padded_pair_nodes(S->nx, S->ny, S->nz) : S->nodes) > (int64_t(1) << 31) - 1)
+    // window pairs carry a border (padded_pair_nodes); the kernel indexes them with int32
+    if (padded_pair_nodes(S->dim, S->nx, S->ny, S->nz) > (int64_t(1) << 31) - 1)
         return SUSER("Invalid dataset was provided. Grid too large.");
-    SK(S->pair.alloc(S->dim == 3 ? (size_t)padded_pair_nodes(S->nx, S->ny, S->nz) * 8 * S->elem
-                                 : (size_t)S->nodes * 4 * S->elem));
+    SK(S->pair.alloc((size_t)padded_pair_nodes(S->dim, S->nx, S->ny, S->nz) * (S->dim == 3 ? 8 : 4) * S->elem));
     SK(S->raw.alloc((size_t)S->nodes * S->dim));
     S->host_snap.assign((size_t)S->n_snap, nullptr);
     for (int k = 0; k < kRing; ++k) S->ring_holds[k] = -1;
