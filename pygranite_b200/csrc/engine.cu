@@ -84,10 +84,36 @@ __global__ void seed_kernel(const float *__restrict__ seeds, int64_t n, int dim,
     }
 }
 
-// Record 0 of the history = the seeds (TrajectoryIntegrator.cpp:424-442).
-__global__ void seed_record_kernel(const float *__restrict__ seeds, int64_t n, int dim, float *hpos, int64_t L) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        for (int d = 0; d < dim; ++d) hpos[i * L * dim + d] = seeds[i * dim + d];
+// Record 0 of the history = the seeds (TrajectoryIntegrator.cpp:424-442): the first row of the
+// record-major history.
+__global__ void seed_record_kernel(const float *__restrict__ seeds, int64_t n, int dim, float *hpos) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n * dim; i += (int64_t)gridDim.x * blockDim.x)
+        hpos[i] = seeds[i];
+}
+
+// Record-major history rows -> particle-major rows: records [r0, r1) of particles [p0, p1), D
+// floats each, from src[(r * n + p) * D + d] to dst[((p - p0) * nr + r - r0) * D + d], rows of nr
+// records (the layout of TrajectorySet's accessors, TrajectorySet.cpp:110-160).  A 32-record x 32-particle
+// tile through shared memory: reads run along a record row, writes along a particle's records,
+// both coalesced.
+template <int D>
+__global__ void __launch_bounds__(256) records_to_rows_kernel(const float *__restrict__ src, int64_t n, int32_t r0,
+                                                              int32_t r1, int64_t p0, int64_t p1,
+                                                              float *__restrict__ dst, int32_t nr) {
+    __shared__ float tile[32][32 * D + 1];
+    const int32_t rt = r0 + (int32_t)blockIdx.y * 32;
+    const int64_t pt = p0 + (int64_t)blockIdx.x * 32;
+    for (int idx = threadIdx.x; idx < 32 * 32 * D; idx += blockDim.x) {
+        const int rr = idx / (32 * D), f = idx - rr * (32 * D);
+        if (rt + rr < r1 && pt + f / D < p1) tile[rr][f] = src[((int64_t)(rt + rr) * n + pt) * D + f];
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < 32 * 32 * D; idx += blockDim.x) {
+        const int q = idx / (32 * D), g = idx - q * (32 * D);
+        const int rr = g / D, d = g - rr * D;
+        if (rt + rr < r1 && pt + q < p1)
+            dst[((pt + q - p0) * nr + (rt + rr - r0)) * D + d] = tile[rr][q * D + d];
+    }
 }
 
 // Writes one record from the state (the SaveInterval == 0 final record, tpp:914-915).
@@ -97,14 +123,14 @@ __global__ void save_state_kernel(const __grid_constant__ KParams P, int32_t rec
     const int64_t n = P.n_dev ? (int64_t)*P.n_dev : P.n;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t pid = P.id[i];
-        float *hp = P.hpos + (pid * P.L + rec) * DIM;
+        float *hp = P.hpos + ((int64_t)rec * P.n_total + pid) * DIM;
         hp[0] = P.px[i];
         hp[1] = P.py[i];
         if (DIM == 3) hp[2] = P.pz[i];
-        if (P.curvature_mode == 3 && write_curv) P.hcurv[pid * P.Lc + crec] = P.curv[i];
+        if (P.curvature_mode == 3 && write_curv) P.hcurv[(int64_t)crec * P.n_total + pid] = P.curv[i];
         if (P.volume_mode != 0)
-            for (int k = 0; k < P.nvol; ++k) P.hvol[((int64_t)k * P.n_total + pid) * P.Li + irec] = P.volc[k * P.n_state + i];
-        for (int e = 0; e < P.nexpr; ++e) P.hcmp[((int64_t)e * P.n_total + pid) * P.Li + irec] = P.cmpc[e * P.n_state + i];
+            for (int k = 0; k < P.nvol; ++k) P.hvol[((int64_t)k * P.Li + irec) * P.n_total + pid] = P.volc[k * P.n_state + i];
+        for (int e = 0; e < P.nexpr; ++e) P.hcmp[((int64_t)e * P.Li + irec) * P.n_total + pid] = P.cmpc[e * P.n_state + i];
     }
 }
 
@@ -188,7 +214,8 @@ struct gr_engine {
     DevBuf<int32_t> c_key, c_hist, c_bintab, c_chunk, c_perm;
     int bx = 4, by = 4, bz = 2, nbx = 0, nby = 0, nbz = 0, nbins = 0;
     DevBuf<int32_t> crec_of_rec;
-    DevBuf<float> hpos, hcurv, hvol, hcmp;
+    DevBuf<float> hpos, hcurv, hvol, hcmp;   // record-major (KParams)
+    DevBuf<float> stage, sstage;             // particle-major chunks for the fetch / the streaming
     DevBuf<int32_t> out_status;
     DevBuf<float> out_length, out_tc;
     DevBuf<unsigned long long> counters;
@@ -875,7 +902,7 @@ int reset_state(gr_engine *e) {
     seed_kernel<<<grid_for(n, threads), threads, 0, e->cs>>>(e->seeds.p, n, e->dim, S.px.p, S.py.p, S.pz.p,
                                                              S.status.p, S.id.p,
                                                              e->has_life ? e->life_src.p : nullptr, S.life.p);
-    seed_record_kernel<<<grid_for(n, threads), threads, 0, e->cs>>>(e->seeds.p, n, e->dim, e->hpos.p, e->L);
+    seed_record_kernel<<<grid_for(n * e->dim, threads), threads, 0, e->cs>>>(e->seeds.p, n, e->dim, e->hpos.p);
     CK(cudaGetLastError());
     CK(cudaMemsetAsync(e->counters.p, 0, 4 * sizeof(unsigned long long), e->cs));
     if (e->compacting) *e->h_live = (int32_t)n;
@@ -1214,32 +1241,26 @@ int compact_pass(gr_engine *e, int32_t rec_now, int32_t k_end, bool graph) {
     return GR_OK;
 }
 
-// Records a retired particle would have written after it left the live set: its frozen
-// state, for records retire .. rec_end-1.
-// Position / volume / compute records [max(retire, rec_lo), rec_end) of every retired particle,
-// and with a table its per-step curvature records from its retirement on.  One warp per retired
-// particle: its records are contiguous in the particle-major history, so the lanes write
-// consecutive words (whole cache lines) instead of one particle's 12 bytes per thread.
+// Records [max(retire, rec_lo), rec_end) of every retired particle repeat its final state:
+// positions, volume / compute records, and with a table its per-step curvature records from its
+// retirement on.  One thread per retired particle, walking its records (rows of the record-major
+// history).
 __global__ void fill_forward_kernel(const __grid_constant__ KParams P, StateView R, const int32_t *n_ret,
                                     const int32_t *crec_of_rec, int32_t rec_lo, int32_t rec_end) {
     const int64_t nr = *n_ret;
-    const int lane = threadIdx.x & 31;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const int dim = P.dim;
-    for (int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nr; j += nwarps) {
+    const int64_t N = P.n_total;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nr; j += (int64_t)gridDim.x * blockDim.x) {
         const int64_t pid = R.id[j];
         const int32_t retire = R.retire[j];
         const int32_t r0 = max(retire, rec_lo);
         if (r0 < rec_end) {
             const float x = R.px[j], y = R.py[j], z = dim == 3 ? R.pz[j] : 0.f;
-            float *hp = P.hpos + (pid * P.L + r0) * dim;
-            const int64_t cnt = (int64_t)(rec_end - r0) * dim;
-            int c = dim == 3 ? lane % 3 : lane & 1;          // component of word e = lane + 32 k
-            const int step = dim == 3 ? 2 : 0;               // 32 mod dim
-            for (int64_t e = lane; e < cnt; e += 32) {
-                hp[e] = c == 0 ? x : (c == 1 ? y : z);
-                c += step;
-                if (c >= dim) c -= dim;
+            for (int32_t r = r0; r < rec_end; ++r) {
+                float *hp = P.hpos + ((int64_t)r * N + pid) * dim;
+                hp[0] = x;
+                hp[1] = y;
+                if (dim == 3) hp[2] = z;
             }
             // volume / expression record r - 1 belongs to position record r
             const int32_t i0 = max(r0 - 1, 0), i1 = rec_end - 1;
@@ -1247,21 +1268,19 @@ __global__ void fill_forward_kernel(const __grid_constant__ KParams P, StateView
                 if (P.volume_mode != 0)
                     for (int k = 0; k < P.nvol; ++k) {
                         const float val = R.volc[k * R.stride + j];
-                        float *hv = P.hvol + ((int64_t)k * P.n_total + pid) * P.Li;
-                        for (int32_t r = i0 + lane; r < i1; r += 32) hv[r] = val;
+                        for (int32_t r = i0; r < i1; ++r) P.hvol[((int64_t)k * P.Li + r) * N + pid] = val;
                     }
                 for (int k = 0; k < P.nexpr; ++k) {
                     const float val = R.cmpc[k * R.stride + j];
-                    float *hc = P.hcmp + ((int64_t)k * P.n_total + pid) * P.Li;
-                    for (int32_t r = i0 + lane; r < i1; r += 32) hc[r] = val;
+                    for (int32_t r = i0; r < i1; ++r) P.hcmp[((int64_t)k * P.Li + r) * N + pid] = val;
                 }
             }
         }
         if (crec_of_rec && P.curvature_mode == 3) {
             const float cv = R.curv[j];
-            for (int32_t r = retire + lane; r < rec_end; r += 32) {
+            for (int32_t r = retire; r < rec_end; ++r) {
                 const int32_t cr = crec_of_rec[r];
-                if (cr >= 0) P.hcurv[pid * P.Lc + cr] = cv;
+                if (cr >= 0) P.hcurv[(int64_t)cr * N + pid] = cv;
             }
         }
     }
@@ -1586,6 +1605,32 @@ int stream_begin(gr_engine *e, const RunPlan &R) {
     return GR_OK;
 }
 
+// Record-major history -> particle-major rows on the device: records [r0, r1) of particles
+// [p0, p1) of a quantity with D floats per particle (records_to_rows_kernel), on `st`.
+int launch_records_to_rows(gr_engine *e, cudaStream_t st, const float *src, int64_t n, int D, int32_t r0,
+                           int32_t r1, int64_t p0, int64_t p1, float *dst) {
+    constexpr int32_t kRowsPerLaunch = 32 * 65535;   // the grid's y extent
+    for (int32_t a = r0; a < r1; a += kRowsPerLaunch) {
+        const int32_t b = std::min(r1, a + kRowsPerLaunch);
+        // each launch covers records [a, b) of the destination rows sized for [r0, r1)
+        const dim3 grid((unsigned)((p1 - p0 + 31) / 32), (unsigned)((b - a + 31) / 32));
+        float *d = dst + (int64_t)(a - r0) * D;
+        const int32_t nr = r1 - r0;
+        if (D == 1) records_to_rows_kernel<1><<<grid, 256, 0, st>>>(src, n, a, b, p0, p1, d, nr);
+        else if (D == 2) records_to_rows_kernel<2><<<grid, 256, 0, st>>>(src, n, a, b, p0, p1, d, nr);
+        else records_to_rows_kernel<3><<<grid, 256, 0, st>>>(src, n, a, b, p0, p1, d, nr);
+        CK(cudaGetLastError());
+        e->stats.aux_launches++;
+    }
+    return GR_OK;
+}
+
+// Particles per staging chunk for particle-major rows of `row_floats` floats.
+int64_t stage_particles(int64_t n, int64_t row_floats) {
+    constexpr int64_t kStageBytes = int64_t(256) << 20;
+    return std::max<int64_t>(1, std::min<int64_t>(n, kStageBytes / std::max<int64_t>(1, row_floats * 4)));
+}
+
 // Copies records [e->streamed, r1) of every particle (and their volume / compute records) into
 // the destinations on the copy-out stream, behind everything already on the step stream.
 // Particles retired so far get those records filled first; particles still in the live set
@@ -1596,7 +1641,7 @@ int stream_records(RunCtx &r, int32_t r1) {
     if (r1 <= r0 || e->n == 0) return GR_OK;
     if (e->compacting) {
         const StateView Rv = view_of(e->ret, e->n);
-        fill_forward_kernel<<<grid_for(e->n * 32, 256), 256, 0, e->cs>>>(r.P, Rv, e->d_counts.p + 2, nullptr, r0, r1);
+        fill_forward_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(r.P, Rv, e->d_counts.p + 2, nullptr, r0, r1);
         CK(cudaGetLastError());
         e->stats.aux_launches++;
     }
@@ -1604,16 +1649,30 @@ int stream_records(RunCtx &r, int32_t r1) {
     CK(cudaStreamWaitEvent(e->ds, e->ds_ev, 0));
     const gr_result_destinations &d = e->dest;
     const int64_t n = e->n;
-    // rows of `width` floats, one pitched DMA
-    auto copy_rows = [&](float *dst, int64_t dpitch, const float *src, int64_t spitch, int64_t width) -> int {
-        CK(cudaMemcpy2DAsync(dst, (size_t)dpitch * sizeof(float), src, (size_t)spitch * sizeof(float),
-                             (size_t)width * sizeof(float), (size_t)n, cudaMemcpyDeviceToHost, e->ds));
-        e->stats.d2h_bytes += width * n * (int64_t)sizeof(float);
+    // records [a, b) of a record-major quantity (D floats per particle) into host rows of `dpitch`
+    // floats, from column a * D: chunks of particles transposed into the streaming stage, each
+    // followed by one pitched DMA (both on the copy-out stream, so a chunk's DMA ends before the
+    // next transpose reuses the stage)
+    auto stream_rows = [&](float *dst, int64_t dpitch, const float *src, int D, int32_t a, int32_t b) -> int {
+        const int64_t w = (int64_t)(b - a) * D;
+        const int64_t cp = stage_particles(n, w);
+        if ((size_t)(cp * w) > e->sstage.count) {
+            CK(cudaStreamSynchronize(e->ds));   // earlier DMAs may still read the old stage
+            CK(e->sstage.alloc((size_t)(cp * w)));
+        }
+        for (int64_t p0 = 0; p0 < n; p0 += cp) {
+            const int64_t p1 = std::min(n, p0 + cp);
+            const int rc = launch_records_to_rows(e, e->ds, src, n, D, a, b, p0, p1, e->sstage.p);
+            if (rc) return rc;
+            CK(cudaMemcpy2DAsync(dst + p0 * dpitch + (int64_t)a * D, (size_t)dpitch * sizeof(float), e->sstage.p,
+                                 (size_t)w * sizeof(float), (size_t)w * sizeof(float), (size_t)(p1 - p0),
+                                 cudaMemcpyDeviceToHost, e->ds));
+        }
+        e->stats.d2h_bytes += w * n * (int64_t)sizeof(float);
         return GR_OK;
     };
     if (d.positions) {
-        const int rc = copy_rows(d.positions + (size_t)r0 * e->dim, d.records_capacity * e->dim,
-                                 e->hpos.p + (size_t)r0 * e->dim, e->L * e->dim, (int64_t)(r1 - r0) * e->dim);
+        const int rc = stream_rows(d.positions, d.records_capacity * e->dim, e->hpos.p, e->dim, r0, r1);
         if (rc) return rc;
     }
     // info record i belongs to position record i + 1
@@ -1621,7 +1680,7 @@ int stream_records(RunCtx &r, int32_t r1) {
     if (i1 > i0) {
         auto copy_info = [&](float *dst, const float *src) -> int {
             if (!dst) return GR_OK;
-            return copy_rows(dst + i0, d.info_capacity, src + i0, e->Li, i1 - i0);
+            return stream_rows(dst, d.info_capacity, src, 1, i0, i1);
         };
         for (int k = 0; k < (e->s.volume_mode != 0 ? e->nvol : 0); ++k) {
             const int rc = copy_info(d.volume_info[k], e->hvol.p + (size_t)k * n * e->Li);
@@ -1695,7 +1754,7 @@ int run_tail(RunCtx &r, RecordCounts &c) {
             CK(cudaMemcpyAsync(e->crec_of_rec.p, t.data(), t.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e->cs));
         }
         const StateView Rv = view_of(e->ret, e->n);
-        fill_forward_kernel<<<grid_for(e->n * 32, 256), 256, 0, e->cs>>>(P, Rv, e->d_counts.p + 2, e->crec_of_rec.p,
+        fill_forward_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, Rv, e->d_counts.p + 2, e->crec_of_rec.p,
                                                                           e->streamed, (int32_t)c.rec);
         finalize_retired_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(Rv, e->d_counts.p + 2, s.abort_mode != 0,
                                                                          s.curvature_mode != 0, e->out_status.p,
@@ -1984,16 +2043,40 @@ static int fetch_rows(gr_engine *e, void *out, int64_t capacity, const void *src
     return GR_OK;
 }
 
+// Records [0, R) of a record-major quantity (D floats per particle) into particle-major host rows
+// of R * D floats: chunks of particles transposed on the device into the staging buffer, each
+// fetched like any device rows.
+static int fetch_records(gr_engine *e, float *out, int64_t cap, const float *src, int D, int64_t R) {
+    if (!e || !out) return USER_ERR("null argument >");
+    if (!e->have_result) return USER_ERR("No result: run() has not completed. >");
+    const int64_t n = e->n, w = R * D;
+    if (cap < n * w) return USER_ERR("Output buffer too small. >");
+    if (n == 0 || w == 0) return GR_OK;
+    int rc = set_device(e);
+    if (rc) return rc;
+    const int64_t cp = stage_particles(n, w);
+    CK(e->stage.alloc((size_t)(cp * w)));
+    for (int64_t p0 = 0; p0 < n; p0 += cp) {
+        const int64_t p1 = std::min(n, p0 + cp);
+        rc = launch_records_to_rows(e, e->cs, src, n, D, 0, (int32_t)R, p0, p1, e->stage.p);
+        if (rc) return rc;
+        CK(cudaStreamSynchronize(e->cs));
+        rc = fetch_rows(e, out + p0 * w, (p1 - p0) * w, e->stage.p, p1 - p0, w, w, sizeof(float));
+        if (rc) return rc;
+    }
+    return GR_OK;
+}
+
 int gr_fetch_positions(gr_engine *e, float *out, int64_t cap) {
     if (!e) return USER_ERR("null engine >");
-    return fetch_rows(e, out, cap, e->hpos.p, e->n, e->info.records * e->dim, e->L * e->dim, sizeof(float));
+    return fetch_records(e, out, cap, e->hpos.p, e->dim, e->info.records);
 }
 
 int gr_fetch_final_positions(gr_engine *e, float *out, int64_t cap) {
     if (!e) return USER_ERR("null engine >");
     if (!e->have_result) return USER_ERR("No result: run() has not completed. >");
-    const float *last = e->hpos.p + (e->info.records - 1) * e->dim;
-    return fetch_rows(e, out, cap, last, e->n, e->dim, e->L * e->dim, sizeof(float));
+    const float *last = e->hpos.p + (e->info.records - 1) * e->n * e->dim;   // the last record's row
+    return fetch_rows(e, out, cap, last, 1, e->n * e->dim, e->n * e->dim, sizeof(float));
 }
 
 int gr_fetch_status(gr_engine *e, int32_t *out, int64_t cap) {
@@ -2016,23 +2099,21 @@ int gr_fetch_total_curvature(gr_engine *e, float *out, int64_t cap) {
 int gr_fetch_curvatures(gr_engine *e, float *out, int64_t cap) {
     if (!e) return USER_ERR("null engine >");
     if (e->info.curvature_records == 0) return GR_OK;
-    return fetch_rows(e, out, cap, e->hcurv.p, e->n, e->info.curvature_records, e->Lc, sizeof(float));
+    return fetch_records(e, out, cap, e->hcurv.p, 1, e->info.curvature_records);
 }
 
 int gr_fetch_volume_info(gr_engine *e, int32_t index, float *out, int64_t cap) {
     if (!e) return USER_ERR("null engine >");
     if (index < 0 || index >= e->info.n_volumes) return USER_ERR("TrajectorySet: Volume with given key does not exist! >");
     if (e->info.info_records == 0) return GR_OK;
-    return fetch_rows(e, out, cap, e->hvol.p + (int64_t)index * e->n * e->Li, e->n, e->info.info_records, e->Li,
-                      sizeof(float));
+    return fetch_records(e, out, cap, e->hvol.p + (int64_t)index * e->n * e->Li, 1, e->info.info_records);
 }
 
 int gr_fetch_compute_info(gr_engine *e, int32_t index, float *out, int64_t cap) {
     if (!e) return USER_ERR("null engine >");
     if (index < 0 || index >= e->info.n_expressions) return USER_ERR("TrajectorySet: Volume with given id does not exist! >");
     if (e->info.info_records == 0) return GR_OK;
-    return fetch_rows(e, out, cap, e->hcmp.p + (int64_t)index * e->n * e->Li, e->n, e->info.info_records, e->Li,
-                      sizeof(float));
+    return fetch_records(e, out, cap, e->hcmp.p + (int64_t)index * e->n * e->Li, 1, e->info.info_records);
 }
 
 }  // extern "C"

@@ -82,11 +82,12 @@ struct KParams {
     int32_t grid_stride;          // 1: persistent grid striding over the live prefix
     int64_t n_state;              // stride of volc / cmpc
     int64_t n_total;              // original particle count (history / constants stride)
-    // history, particle-major
-    float *hpos;                  // [(id * L + rec) * dim + d]
-    float *hcurv;                 // [id * Lc + crec]
-    float *hvol;                  // [(k * n_total + id) * Li + irec]
-    float *hcmp;                  // [(e * n_total + id) * Li + irec]
+    // history, record-major: one row of n_total particles per record, so the rows a launch
+    // writes are whole in L2 before they reach DRAM (the fetch transposes them)
+    float *hpos;                  // [(rec * n_total + id) * dim + d]
+    float *hcurv;                 // [crec * n_total + id]
+    float *hvol;                  // [(k * Li + irec) * n_total + id]
+    float *hcmp;                  // [(e * Li + irec) * n_total + id]
     int64_t L, Lc, Li;
     // schedule
     const StepEntry *sched;
@@ -918,10 +919,10 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
         }
 
         if (valid && (E.flags & SF_SAVE)) {
-            float *hp = P.hpos + (pid * P.L + E.rec) * DIM;
+            float *hp = P.hpos + ((int64_t)E.rec * P.n_total + pid) * DIM;
             hp[0] = p.x; hp[1] = p.y;
             if (DIM == 3) hp[2] = p.z;
-            if (curvature_mode == 3 && (E.flags & SF_CURV_REC)) P.hcurv[pid * P.Lc + E.crec] = cv;
+            if (curvature_mode == 3 && (E.flags & SF_CURV_REC)) P.hcurv[(int64_t)E.crec * P.n_total + pid] = cv;
             if (extras) {
                 // volume / expression values: evaluated now if an alive step has passed since the
                 // last evaluation (and kept in the state arrays), else the state arrays' values
@@ -935,11 +936,11 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
                 if (P.volume_mode != 0) {
 #pragma unroll
                     for (int k = 0; k < GR_MAX_VOL; ++k)
-                        if (k < P.nvol) P.hvol[((int64_t)k * P.n_total + pid) * P.Li + E.irec] = vol[k];
+                        if (k < P.nvol) P.hvol[((int64_t)k * P.Li + E.irec) * P.n_total + pid] = vol[k];
                 }
 #pragma unroll
                 for (int e = 0; e < GR_MAX_EXPR; ++e)
-                    if (e < P.nexpr) P.hcmp[((int64_t)e * P.n_total + pid) * P.Li + E.irec] = cmp[e];
+                    if (e < P.nexpr) P.hcmp[((int64_t)e * P.Li + E.irec) * P.n_total + pid] = cmp[e];
                 // refill the sample cache for the next step's first sample (at p): the cached
                 // nodes are then dead while the values above are evaluated, which frees their
                 // registers there

@@ -185,10 +185,7 @@ def test_engine_reference_filter_matches_the_reference_kernel():
 # weights, so values drift apart by float rounding over the run.
 
 def options_fixture():
-    path = os.path.join(HERE, "options_reference.npz")
-    if not os.path.exists(path):
-        pytest.skip("options_reference.npz not generated")
-    return np.load(path)
+    return load("options_reference.npz")
 
 
 def option_fixture_case(f, name):
@@ -198,20 +195,23 @@ def option_fixture_case(f, name):
 
 def check_option_case(name, res, ref):
     """Abort codes, positions, lengths, curvature and expression values against the reference
-    kernel's.  Tolerances: abort codes equal for at least 97% of the particles (a particle at a
-    border or length threshold within float rounding may stop a step apart); positions of the
-    particles alive in both, in grid cells: median < 1e-4 after 5 steps and < 2e-3 after 60,
-    and below 0.05 for 90% of them; the rest: median relative difference < 1e-2."""
+    kernel's.  Tolerances (the reference interpolates in texture hardware; see the module
+    docstring): abort codes equal for at least 95% of the particles (a particle at a border or
+    length threshold within rounding may stop a step apart); positions of the particles alive in
+    both, in grid cells: median < 3e-4 after 5 steps and < 1e-2 after 60, 90th percentile < 0.5
+    after 60 (sphere coordinates with pole crossings amplify differences); lengths and
+    expression values: median relative difference < 2e-3; total and per-step curvature < 2e-2;
+    volume samples: median < 0.02 K."""
     settings = make_golden_settings(name)
     cell = np.asarray(settings["GridScale"], np.float64)
     assert res["trajectories"].shape == ref["trajectories"].shape, (res["trajectories"].shape, ref["trajectories"].shape)
     same = (res["status"] == ref["status"]).mean()
-    assert same >= 0.97, (name, same)
+    assert same >= 0.95, (name, same)
     both = (res["status"] == 0) & (ref["status"] == 0)
     e = cells(res["trajectories"][both], ref["trajectories"][both], cell)
     if e.size:
-        assert np.median(e[:, 1]) < 1e-4 and np.median(e[:, -1]) < 2e-3, (name, np.median(e[:, 1]), np.median(e[:, -1]))
-        assert np.percentile(e[:, -1], 90) < 0.05, (name, np.percentile(e[:, -1], 90))
+        assert np.median(e[:, 1]) < 3e-4 and np.median(e[:, -1]) < 1e-2, (name, np.median(e[:, 1]), np.median(e[:, -1]))
+        assert np.percentile(e[:, -1], 90) < 0.5, (name, np.percentile(e[:, -1], 90))
 
     def rel(a, b):
         a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
@@ -219,16 +219,16 @@ def check_option_case(name, res, ref):
         return np.median(np.abs(a[ok] - b[ok]) / np.abs(b[ok])) if ok.any() else 0.0
 
     if settings.get("AbortMode", 0):
-        assert rel(res["lengths"][both], ref["lengths"][both]) < 1e-2, name
+        assert rel(res["lengths"][both], ref["lengths"][both]) < 2e-3, name
     if settings.get("CurvatureMode", 0):
-        assert rel(res["total_curvature"][both], ref["total_curvature"][both]) < 1e-2, name
+        assert rel(res["total_curvature"][both], ref["total_curvature"][both]) < 2e-2, name
     if settings.get("CurvatureMode", 0) == 3:
         assert res["curvatures"].shape == ref["curvatures"].shape
-        assert rel(res["curvatures"][both], ref["curvatures"][both]) < 1e-2, name
+        assert rel(res["curvatures"][both], ref["curvatures"][both]) < 2e-2, name
     if settings.get("AdditionalCompute"):
-        assert rel(res["compute_info"][0][both], ref["compute_0"][both]) < 1e-2, name
+        assert rel(res["compute_info"][0][both], ref["compute_0"][both]) < 2e-3, name
     if settings.get("AdditionalVolumeMode", 0):
-        assert np.median(np.abs(res["volume_info"]["T"][both] - ref["volume_T"][both])) < 0.05, name
+        assert np.median(np.abs(res["volume_info"]["T"][both] - ref["volume_T"][both])) < 0.02, name
 
 
 def make_golden_settings(name):
