@@ -253,7 +253,8 @@ def plain_config(args, world):
     n_snap = args.sim_steps // 10 + 1
     return {"workload": WORKLOAD, "particles_per_gpu": args.particles, "sim_steps": args.sim_steps,
             "snapshots": n_snap, "grid": [192, 192, 64], "storage": args.storage,
-            "parallelism": f"replicas{world}", "l2": f"inputs larger than L2 ({n_snap} snapshots, 7.6 GB ring)",
+            "parallelism": f"replicas{world}",
+            "l2": f"inputs larger than L2 ({n_snap} snapshots, {n_snap * 192 * 192 * 64 * 16 / 1e9:.1f} GB ring)",
             "records_every": 10, "sort_interval": args.sort_interval, "steps_per_launch": args.steps_per_launch,
             "wind_layout": ["window-pair", "ring"][args.layout]}
 

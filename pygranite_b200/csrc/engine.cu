@@ -1337,19 +1337,19 @@ int pack_pair(gr_engine *e, int64_t w, cudaStream_t stream) {
     if (e->dim == 3) {
         const int32_t nx = (int32_t)e->nx, ny = (int32_t)e->ny, nz = (int32_t)e->nz;
         if (elem == 16)
-            pair_pack_padded_kernel<uint4><<<blocks, threads, 0, stream>>>((const uint4 *)back, (const uint4 *)front,
-                                                                          (uint4 *)e->pairbuf[b].p, nx, ny, nz);
+            pair_pack_padded_kernel<float><<<blocks, threads, 0, stream>>>((const float4 *)back, (const float4 *)front,
+                                                                          e->pairbuf[b].p, nx, ny, nz);
         else
-            pair_pack_padded_kernel<uint2><<<blocks, threads, 0, stream>>>((const uint2 *)back, (const uint2 *)front,
-                                                                          (uint2 *)e->pairbuf[b].p, nx, ny, nz);
+            pair_pack_padded_kernel<uint16_t><<<blocks, threads, 0, stream>>>((const uint2 *)back, (const uint2 *)front,
+                                                                             e->pairbuf[b].p, nx, ny, nz);
     } else {
         const int32_t nx = (int32_t)e->nx, ny = (int32_t)e->ny;
         if (elem == 8)
-            pair_pack_edge2_kernel<uint2><<<blocks, threads, 0, stream>>>((const uint2 *)back, (const uint2 *)front,
-                                                                         (uint2 *)e->pairbuf[b].p, nx, ny);
+            pair_pack_edge2_kernel<float><<<blocks, threads, 0, stream>>>((const float2 *)back, (const float2 *)front,
+                                                                         (float4 *)e->pairbuf[b].p, nx, ny);
         else
-            pair_pack_edge2_kernel<unsigned><<<blocks, threads, 0, stream>>>(
-                (const unsigned *)back, (const unsigned *)front, (unsigned *)e->pairbuf[b].p, nx, ny);
+            pair_pack_edge2_kernel<uint16_t><<<blocks, threads, 0, stream>>>(
+                (const unsigned *)back, (const unsigned *)front, (uint2 *)e->pairbuf[b].p, nx, ny);
     }
     CK(cudaGetLastError());
     e->pair_window[b] = w;

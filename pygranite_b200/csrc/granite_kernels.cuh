@@ -165,49 +165,46 @@ template <> struct Store<__half> {
     static constexpr int bytes3 = 8, bytes2 = 4;
 };
 
-// Window-pair layouts: node n holds the back snapshot's node followed by the front
-// snapshot's node, so one load returns both (32 bytes for float32 3D, 16 bytes for 16-bit 3D or
-// float32 2D, 8 bytes for 16-bit 2D).  Built per window from the ring (pack_kernels.cuh), with a
-// border (make_pcell, bil2p_padded).
+// Window-pair layouts: node n holds, component by component, the back snapshot's value followed
+// by the front snapshot's: {u_b, u_f, v_b, v_f, w_b, w_f, 0, 0} in 3D (32 bytes float32, 16 bytes
+// 16-bit), {u_b, u_f, v_b, v_f} in 2D (16 / 8 bytes).  One load returns both snapshots, and each
+// component arrives as a (back, front) pair that the paired float32 instructions of sm_100
+// (__ffma2_rn) interpolate in space at once.  Built per window from the ring (pack_kernels.cuh),
+// with a border (make_pcell, bil2p_padded).
 template <typename W> struct Pair {};
 
 template <typename W> struct IsPair { static constexpr bool value = false; };
 template <typename W> struct IsPair<Pair<W>> { static constexpr bool value = true; };
 
 template <> struct Store<Pair<float>> {
-    static __device__ __forceinline__ void load3p(const void *base, int32_t idx, float (&b)[3], float (&f)[3]) {
-        float r[8];   // {u_b, v_b, w_b, 0, u_f, v_f, w_f, 0}: one 256-bit load
+    // 3D node: (u_b, u_f), (v_b, v_f), (w_b, w_f), one 256-bit load
+    static __device__ __forceinline__ void load3p(const void *base, int32_t idx, float2 (&c)[3]) {
+        float r[8];
         const float *p = reinterpret_cast<const float *>(base) + (int64_t)idx * 8;
         asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                      : "=f"(r[0]), "=f"(r[1]), "=f"(r[2]), "=f"(r[3]), "=f"(r[4]), "=f"(r[5]), "=f"(r[6]), "=f"(r[7])
                      : "l"(p));
-        b[0] = r[0]; b[1] = r[1]; b[2] = r[2];
-        f[0] = r[4]; f[1] = r[5]; f[2] = r[6];
+        c[0] = make_float2(r[0], r[1]); c[1] = make_float2(r[2], r[3]); c[2] = make_float2(r[4], r[5]);
     }
-    static __device__ __forceinline__ void load2p(const void *base, int32_t idx, float (&b)[2], float (&f)[2]) {
+    // 2D node: (u_b, u_f), (v_b, v_f)
+    static __device__ __forceinline__ void load2p(const void *base, int32_t idx, float2 (&c)[2]) {
         const float4 q = __ldg(reinterpret_cast<const float4 *>(base) + idx);
-        b[0] = q.x; b[1] = q.y; f[0] = q.z; f[1] = q.w;
+        c[0] = make_float2(q.x, q.y); c[1] = make_float2(q.z, q.w);
     }
     static constexpr int bytes3 = 32, bytes2 = 16;
 };
 
 template <typename H> struct Store<Pair<H>> {
+    // one 32-bit word = (back, front) of one component, converted to a float pair
     static __device__ __forceinline__ float2 cvt(unsigned q) {
         if constexpr (sizeof(H) == 2 && std::is_same<H, __half>::value)
             return __half22float2(*reinterpret_cast<const __half2 *>(&q));
         else
             return __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&q));
     }
-    static __device__ __forceinline__ void load3p(const void *base, int32_t idx, float (&b)[3], float (&f)[3]) {
-        const uint4 q = __ldg(reinterpret_cast<const uint4 *>(base) + idx);
-        const float2 b01 = cvt(q.x), b2 = cvt(q.y), f01 = cvt(q.z), f2 = cvt(q.w);
-        b[0] = b01.x; b[1] = b01.y; b[2] = b2.x;
-        f[0] = f01.x; f[1] = f01.y; f[2] = f2.x;
-    }
-    static __device__ __forceinline__ void load2p(const void *base, int32_t idx, float (&b)[2], float (&f)[2]) {
+    static __device__ __forceinline__ void load2p(const void *base, int32_t idx, float2 (&c)[2]) {
         const uint2 q = __ldg(reinterpret_cast<const uint2 *>(base) + idx);
-        const float2 bb = cvt(q.x), ff = cvt(q.y);
-        b[0] = bb.x; b[1] = bb.y; f[0] = ff.x; f[1] = ff.y;
+        c[0] = cvt(q.x); c[1] = cvt(q.y);
     }
     static constexpr int bytes3 = 16, bytes2 = 8;
 };
@@ -264,23 +261,17 @@ __device__ __forceinline__ void tri3(const void *slot, const Cell3 &c, float &ou
     ow = lerp_(lerp_(a00, a10, c.fy), lerp_(a01, a11, c.fy), c.fz);
 }
 
-__device__ __forceinline__ float tri_corners(const float (&c)[8], const Cell3 &cl) {
-    const float a00 = lerp_(c[0], c[1], cl.fx), a10 = lerp_(c[2], c[3], cl.fx);
-    const float a01 = lerp_(c[4], c[5], cl.fx), a11 = lerp_(c[6], c[7], cl.fx);
-    return lerp_(lerp_(a00, a10, cl.fy), lerp_(a01, a11, cl.fy), cl.fz);
-}
-
 // Pair nodes of the last cell a particle sampled (window-pair layouts).  Consecutive samples of
 // one particle (its RK4 stages, its next step) mostly fall in the same cell, whose nodes then
 // need no new gathers; the values and the arithmetic are the same either way.  The cell is
 // identified by its first corner's index in the padded pair buffer (`base`); 3D 16-bit kernels
-// keep the raw nodes (32 registers), the float32 kernel the 48 floats (AdvBounds gives its launch
-// shape); 2D keeps the 4 corners as floats (16 registers).
+// keep the raw nodes (32 registers), the float32 kernel 24 (back, front) pairs (48 registers;
+// AdvBounds gives its launch shape); 2D keeps 8 pairs (16 registers).
 struct SampleCache {
     int32_t base;
     uint4 q[8];
-    float b2[4][2], f2[4][2];
-    float c32[6][8];   // float32 3D: u, v, w back and front of the 8 corners
+    float2 c2d[2][4];  // 2D: (back, front) of u and v at the 4 corners
+    float2 c2[3][8];   // float32 3D: (back, front) of u, v, w at the 8 corners
     __device__ __forceinline__ void reset() { base = -1; }
 };
 
@@ -319,14 +310,23 @@ __device__ __forceinline__ PCell make_pcell(const KParams &P, float ax, float ay
     return c;
 }
 
-__device__ __forceinline__ float tri8(const float (&c)[8], float fx, float fy, float fz) {
-    const float a00 = lerp_(c[0], c[1], fx), a10 = lerp_(c[2], c[3], fx);
-    const float a01 = lerp_(c[4], c[5], fx), a11 = lerp_(c[6], c[7], fx);
-    return lerp_(lerp_(a00, a10, fy), lerp_(a01, a11, fy), fz);
+// lerp_ on a (back, front) pair with one weight, as paired float32 instructions: b - a is formed
+// as fma(a, -1, b) (the product is exact, so it rounds like the subtraction), then fma(t, d, a);
+// each half equals lerp_ on that half bit for bit.
+__device__ __forceinline__ float2 lerp2_(float2 a, float2 b, float t) {
+    const float2 d = __ffma2_rn(a, make_float2(-1.f, -1.f), b);
+    return __ffma2_rn(make_float2(t, t), d, a);
 }
 
-// Loads the 8 padded corners of the cell at `base` into the sample cache: float32 as 48 floats
-// (back / front u, v, w per corner), 16-bit as the raw 16-byte pair nodes.
+// Trilinear interpolation of 8 corner pairs: x, then y, then z (the order of tri3).
+__device__ __forceinline__ float2 tri8p(const float2 (&c)[8], float fx, float fy, float fz) {
+    const float2 a00 = lerp2_(c[0], c[1], fx), a10 = lerp2_(c[2], c[3], fx);
+    const float2 a01 = lerp2_(c[4], c[5], fx), a11 = lerp2_(c[6], c[7], fx);
+    return lerp2_(lerp2_(a00, a10, fy), lerp2_(a01, a11, fy), fz);
+}
+
+// Loads the 8 padded corners of the cell at `base` into the sample cache: float32 as 24 (back,
+// front) pairs (u, v, w per corner), 16-bit as the raw 16-byte pair nodes.
 template <typename H>
 __device__ __forceinline__ void fill_padded(const KParams &P, const void *pairs, int32_t base, SampleCache &cc) {
     const int32_t sy = P.pnx, sz = P.pnxy;
@@ -334,10 +334,9 @@ __device__ __forceinline__ void fill_padded(const KParams &P, const void *pairs,
     for (int k = 0; k < 8; ++k) {
         const int32_t idx = base + ((k & 1) ? 1 : 0) + ((k & 2) ? sy : 0) + ((k & 4) ? sz : 0);
         if constexpr (std::is_same<H, float>::value) {
-            float b[3], f[3];
-            Store<Pair<float>>::load3p(pairs, idx, b, f);
-            cc.c32[0][k] = b[0]; cc.c32[1][k] = b[1]; cc.c32[2][k] = b[2];
-            cc.c32[3][k] = f[0]; cc.c32[4][k] = f[1]; cc.c32[5][k] = f[2];
+            float2 c[3];
+            Store<Pair<float>>::load3p(pairs, idx, c);
+            cc.c2[0][k] = c[0]; cc.c2[1][k] = c[1]; cc.c2[2][k] = c[2];
         } else {
             cc.q[k] = __ldg(reinterpret_cast<const uint4 *>(pairs) + idx);
         }
@@ -345,30 +344,31 @@ __device__ __forceinline__ void fill_padded(const KParams &P, const void *pairs,
     cc.base = base;
 }
 
-// float32: the 8 padded corners' back / front values as 48 floats, reloaded when the cell changes.
+// float32: the cached corner pairs, reloaded when the cell changes; out[c] = (back, front) value
+// of component c at the sample.
 __device__ __forceinline__ void tri3p_padded32(const KParams &P, const void *pairs, const PCell &c, SampleCache &cc,
-                                               float (&ob)[3], float (&of)[3]) {
+                                               float2 (&out)[3]) {
     if (c.base != cc.base) fill_padded<float>(P, pairs, c.base, cc);
-    ob[0] = tri8(cc.c32[0], c.fx, c.fy, c.fz); ob[1] = tri8(cc.c32[1], c.fx, c.fy, c.fz);
-    ob[2] = tri8(cc.c32[2], c.fx, c.fy, c.fz);
-    of[0] = tri8(cc.c32[3], c.fx, c.fy, c.fz); of[1] = tri8(cc.c32[4], c.fx, c.fy, c.fz);
-    of[2] = tri8(cc.c32[5], c.fx, c.fy, c.fz);
+    out[0] = tri8p(cc.c2[0], c.fx, c.fy, c.fz);
+    out[1] = tri8p(cc.c2[1], c.fx, c.fy, c.fz);
+    out[2] = tri8p(cc.c2[2], c.fx, c.fy, c.fz);
 }
 
-// 16-bit: the 8 padded corners as raw 16-byte pair nodes, converted per sample.
+// 16-bit: the 8 raw pair nodes, each word converted to a (back, front) pair per sample.
 template <typename H>
 __device__ __forceinline__ void tri3p_padded16(const KParams &P, const void *pairs, const PCell &c, SampleCache &cc,
-                                               float (&ob)[3], float (&of)[3]) {
+                                               float2 (&out)[3]) {
     if (c.base != cc.base) fill_padded<H>(P, pairs, c.base, cc);
-    float u[8], v[8], w[8], uf[8], vf[8], wf[8];
+    float2 u[8], v[8], w[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-        const float2 b01 = Store<Pair<H>>::cvt(cc.q[k].x), b2 = Store<Pair<H>>::cvt(cc.q[k].y);
-        const float2 f01 = Store<Pair<H>>::cvt(cc.q[k].z), f2 = Store<Pair<H>>::cvt(cc.q[k].w);
-        u[k] = b01.x; v[k] = b01.y; w[k] = b2.x; uf[k] = f01.x; vf[k] = f01.y; wf[k] = f2.x;
+        u[k] = Store<Pair<H>>::cvt(cc.q[k].x);
+        v[k] = Store<Pair<H>>::cvt(cc.q[k].y);
+        w[k] = Store<Pair<H>>::cvt(cc.q[k].z);
     }
-    ob[0] = tri8(u, c.fx, c.fy, c.fz); ob[1] = tri8(v, c.fx, c.fy, c.fz); ob[2] = tri8(w, c.fx, c.fy, c.fz);
-    of[0] = tri8(uf, c.fx, c.fy, c.fz); of[1] = tri8(vf, c.fx, c.fy, c.fz); of[2] = tri8(wf, c.fx, c.fy, c.fz);
+    out[0] = tri8p(u, c.fx, c.fy, c.fz);
+    out[1] = tri8p(v, c.fx, c.fy, c.fz);
+    out[2] = tri8p(w, c.fx, c.fy, c.fz);
 }
 
 template <typename W> struct PairElem { using type = void; };
@@ -427,24 +427,26 @@ __device__ __forceinline__ void bil2(const void *slot, const Cell2 &c, float &ou
 // The cache keeps the 4 corners as floats (16 registers), keyed by the first corner's index.
 template <typename W>
 __device__ __forceinline__ void bil2p_padded(const KParams &P, const void *pairs, float ax, float ay, SampleCache &cc,
-                                             float (&ob)[2], float (&of)[2]) {
+                                             float2 (&out)[2]) {
     int ix, iy;
     float fx, fy;
     pcell1(ax, P.nx, P.filter_weights, ix, fx);
     pcell1(ay, P.ny, P.filter_weights, iy, fy);
     const int32_t base = (iy + 1) * P.pnx + (ix + 1);
     if (base != cc.base) {
-        Store<W>::load2p(pairs, base, cc.b2[0], cc.f2[0]);
-        Store<W>::load2p(pairs, base + 1, cc.b2[1], cc.f2[1]);
-        Store<W>::load2p(pairs, base + P.pnx, cc.b2[2], cc.f2[2]);
-        Store<W>::load2p(pairs, base + P.pnx + 1, cc.b2[3], cc.f2[3]);
+        const int32_t idx[4] = {base, base + 1, base + P.pnx, base + P.pnx + 1};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float2 c[2];
+            Store<W>::load2p(pairs, idx[k], c);
+            cc.c2d[0][k] = c[0];
+            cc.c2d[1][k] = c[1];
+        }
         cc.base = base;
     }
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        ob[k] = lerp_(lerp_(cc.b2[0][k], cc.b2[1][k], fx), lerp_(cc.b2[2][k], cc.b2[3][k], fx), fy);
-        of[k] = lerp_(lerp_(cc.f2[0][k], cc.f2[1][k], fx), lerp_(cc.f2[2][k], cc.f2[3][k], fx), fy);
-    }
+    for (int k = 0; k < 2; ++k)
+        out[k] = lerp2_(lerp2_(cc.c2d[k][0], cc.c2d[k][1], fx), lerp2_(cc.c2d[k][2], cc.c2d[k][3], fx), fy);
 }
 
 
@@ -476,17 +478,17 @@ __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, co
         if (DIM == 3) {
             const float az = (p.z - P.off[2]) * P.inv_scale[2];
             const PCell c = make_pcell(P, ax, ay, az);
-            float b[3], f[3];
+            float2 bf[3];
             using H = typename PairElem<W>::type;
             if constexpr (std::is_same<H, float>::value)
-                tri3p_padded32(P, wb, c, cc, b, f);
+                tri3p_padded32(P, wb, c, cc, bf);
             else
-                tri3p_padded16<H>(P, wb, c, cc, b, f);
-            r.x = lerp_(b[0], f[0], t); r.y = lerp_(b[1], f[1], t); r.z = lerp_(b[2], f[2], t);
+                tri3p_padded16<H>(P, wb, c, cc, bf);
+            r.x = lerp_(bf[0].x, bf[0].y, t); r.y = lerp_(bf[1].x, bf[1].y, t); r.z = lerp_(bf[2].x, bf[2].y, t);
         } else {
-            float b[2], f[2];
-            bil2p_padded<W>(P, wb, ax, ay, cc, b, f);
-            r.x = lerp_(b[0], f[0], t); r.y = lerp_(b[1], f[1], t);
+            float2 bf[2];
+            bil2p_padded<W>(P, wb, ax, ay, cc, bf);
+            r.x = lerp_(bf[0].x, bf[0].y, t); r.y = lerp_(bf[1].x, bf[1].y, t);
         }
         return r;
     } else {

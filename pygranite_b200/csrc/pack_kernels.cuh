@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 namespace granite_b200 {
 
@@ -60,44 +61,79 @@ __global__ void pack_wind_kernel<__half>(const float *__restrict__ u, const floa
     }
 }
 
+// The window pair interleaves the two snapshots component by component (granite_kernels.cuh,
+// Store<Pair<...>>): from ring nodes b (back) and f (front) of storage type S to one pair node.
+// float32: ring nodes float4 {u, v, w, 0} / float2 {u, v}; 16-bit: uint2 {(u, v), (w, 0)} /
+// one word (u, v), each word two 16-bit values (low half first).
+template <typename S> struct PairNode;
+
+template <> struct PairNode<float> {
+    using Ring3 = float4;
+    using Ring2 = float2;
+    using Out3 = uint4;   // written as two of these: 32 bytes
+    using Out2 = float4;
+    static __device__ __forceinline__ void pack3(const float4 &b, const float4 &f, float4 *o) {
+        o[0] = make_float4(b.x, f.x, b.y, f.y);
+        o[1] = make_float4(b.z, f.z, 0.f, 0.f);
+    }
+    static __device__ __forceinline__ float4 pack2(const float2 &b, const float2 &f) { return make_float4(b.x, f.x, b.y, f.y); }
+};
+
+template <> struct PairNode<uint16_t> {
+    using Ring3 = uint2;
+    using Ring2 = unsigned;
+    using Out2 = uint2;
+    // __byte_perm(x, y, 0x5410): the low halves of x and y; 0x7632: their high halves
+    static __device__ __forceinline__ uint4 pack3(const uint2 &b, const uint2 &f) {
+        return make_uint4(__byte_perm(b.x, f.x, 0x5410), __byte_perm(b.x, f.x, 0x7632), __byte_perm(b.y, f.y, 0x5410), 0u);
+    }
+    static __device__ __forceinline__ uint2 pack2(unsigned b, unsigned f) {
+        return make_uint2(__byte_perm(b, f, 0x5410), __byte_perm(b, f, 0x7632));
+    }
+};
+
 // 2D window pair with replicated edges: padded node (x, y), x in [-1, nx + 1], y in [-1, ny + 1],
-// of a (nx + 3) x (ny + 3) buffer holds the back slot's node (clamp(x), clamp(y)) followed by the
-// front slot's (the step kernel's clamp addressing).  T is one packed node (8 bytes float32, 4
-// bytes 16-bit); every padded node is written.
-template <typename T>
-static __global__ void pair_pack_edge2_kernel(const T *__restrict__ back, const T *__restrict__ front, T *out,
-                                              int32_t nx, int32_t ny) {
+// of a (nx + 3) x (ny + 3) buffer holds the pair of ring nodes (clamp(x), clamp(y)) (the step
+// kernel's clamp addressing).  Every padded node is written.
+template <typename S>
+static __global__ void pair_pack_edge2_kernel(const typename PairNode<S>::Ring2 *__restrict__ back,
+                                              const typename PairNode<S>::Ring2 *__restrict__ front,
+                                              typename PairNode<S>::Out2 *out, int32_t nx, int32_t ny) {
     const int32_t pnx = nx + 3;
     const int32_t total = pnx * (ny + 3);
     for (int32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < total; o += gridDim.x * blockDim.x) {
         const int32_t x = min(max(o % pnx - 1, 0), nx - 1), y = min(max(o / pnx - 1, 0), ny - 1);
         const int64_t i = (int64_t)y * nx + x;
-        out[2 * (int64_t)o] = back[i];
-        out[2 * (int64_t)o + 1] = front[i];
+        out[o] = PairNode<S>::pack2(back[i], front[i]);
     }
 }
 
-// 3D window pair with a zero border: padded node (x, y, z), x in [-1, nx + 1] and likewise y,
-// z, of a (nx + 3) x (ny + 3) x (nz + 3) buffer holds the back slot's node (x, y, z) followed by
-// the front slot's, or zeros outside the grid (the step kernel's border addressing).  T is one
-// packed node (16 bytes float32, 8 bytes 16-bit); every padded node is written, so the buffer
-// needs no clearing.  The padded node count must stay below 2^31.
-template <typename T>
-static __global__ void pair_pack_padded_kernel(const T *__restrict__ back, const T *__restrict__ front, T *out,
+// 3D window pair with a zero border: padded node (x, y, z), x in [-1, nx + 1] and likewise y, z,
+// of a (nx + 3) x (ny + 3) x (nz + 3) buffer holds the pair of ring nodes (x, y, z), or zeros
+// outside the grid (the step kernel's border addressing).  Every padded node is written, so the
+// buffer needs no clearing.  The padded node count must stay below 2^31.
+template <typename S>
+static __global__ void pair_pack_padded_kernel(const typename PairNode<S>::Ring3 *__restrict__ back,
+                                               const typename PairNode<S>::Ring3 *__restrict__ front, void *out,
                                                int32_t nx, int32_t ny, int32_t nz) {
     const int32_t pnx = nx + 3, pny = ny + 3;
     const int32_t total = pnx * pny * (nz + 3);
     for (int32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < total; o += gridDim.x * blockDim.x) {
         const int32_t x = o % pnx - 1, r = o / pnx;
         const int32_t y = r % pny - 1, z = r / pny - 1;
-        T b{}, f{};
-        if ((unsigned)x < (unsigned)nx && (unsigned)y < (unsigned)ny && (unsigned)z < (unsigned)nz) {
-            const int64_t i = ((int64_t)z * ny + y) * nx + x;
-            b = back[i];
-            f = front[i];
+        const bool in = (unsigned)x < (unsigned)nx && (unsigned)y < (unsigned)ny && (unsigned)z < (unsigned)nz;
+        const int64_t i = in ? ((int64_t)z * ny + y) * nx + x : 0;
+        if constexpr (std::is_same<S, float>::value) {
+            float4 *po = reinterpret_cast<float4 *>(out) + 2 * (int64_t)o;
+            if (in) {
+                PairNode<float>::pack3(back[i], front[i], po);
+            } else {
+                po[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+                po[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        } else {
+            reinterpret_cast<uint4 *>(out)[o] = in ? PairNode<uint16_t>::pack3(back[i], front[i]) : make_uint4(0u, 0u, 0u, 0u);
         }
-        out[2 * (int64_t)o] = b;
-        out[2 * (int64_t)o + 1] = f;
     }
 }
 

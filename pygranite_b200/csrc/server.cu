@@ -244,11 +244,11 @@ __global__ void planar_pack_kernel(const float *__restrict__ u, const float *__r
     }
 }
 
-// Two planar slots -> the window-pair layout the step kernel reads: per node
-// {u_b, v_b, w_b, 0, u_f, v_f, w_f, 0} (3D) or {u_b, v_b, u_f, v_f} (2D), vector stores.
-// 3D pairs carry the zero border of pair_pack_padded_kernel (pack_kernels.cuh): every padded
-// node (nx + 3) x (ny + 3) x (nz + 3) is written, zeros outside the grid; 2D pairs replicate the
-// edge nodes.
+// Two planar slots -> the window-pair layout the step kernel reads (granite_kernels.cuh,
+// Store<Pair<...>>): per node, component by component, back then front: {u_b, u_f, v_b, v_f,
+// w_b, w_f, 0, 0} (3D) or {u_b, u_f, v_b, v_f} (2D), vector stores.  3D pairs carry the zero
+// border of pair_pack_padded_kernel (pack_kernels.cuh): every padded node (nx + 3) x (ny + 3) x
+// (nz + 3) is written, zeros outside the grid; 2D pairs replicate the edge nodes.
 template <typename T>
 __global__ void planar_pair_kernel(const T *__restrict__ b, const T *__restrict__ f, T *__restrict__ out,
                                    int64_t nodes, int dim, int32_t nx, int32_t ny, int32_t nz) {
@@ -264,8 +264,8 @@ __global__ void planar_pair_kernel(const T *__restrict__ b, const T *__restrict_
             alignas(sizeof(V)) T hi[4] = {zero, zero, zero, zero};
             if ((unsigned)x < (unsigned)nx && (unsigned)y < (unsigned)ny && (unsigned)z < (unsigned)nz) {
                 const int64_t i = ((int64_t)z * ny + y) * nx + x;
-                lo[0] = b[i]; lo[1] = b[nodes + i]; lo[2] = b[2 * nodes + i];
-                hi[0] = f[i]; hi[1] = f[nodes + i]; hi[2] = f[2 * nodes + i];
+                lo[0] = b[i]; lo[1] = f[i]; lo[2] = b[nodes + i]; lo[3] = f[nodes + i];
+                hi[0] = b[2 * nodes + i]; hi[1] = f[2 * nodes + i];
             }
             V *po = reinterpret_cast<V *>(out + 8 * (int64_t)o);
             po[0] = *reinterpret_cast<const V *>(lo);
@@ -279,7 +279,7 @@ __global__ void planar_pair_kernel(const T *__restrict__ b, const T *__restrict_
     for (int32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < total; o += gridDim.x * blockDim.x) {
         const int32_t x = min(max(o % pnx - 1, 0), nx - 1), y = min(max(o / pnx - 1, 0), ny - 1);
         const int64_t i = (int64_t)y * nx + x;
-        alignas(sizeof(V)) T q[4] = {b[i], b[nodes + i], f[i], f[nodes + i]};
+        alignas(sizeof(V)) T q[4] = {b[i], f[i], b[nodes + i], f[nodes + i]};
         *reinterpret_cast<V *>(out + 4 * (int64_t)o) = *reinterpret_cast<const V *>(q);
     }
 }
