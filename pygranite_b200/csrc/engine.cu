@@ -91,21 +91,41 @@ __global__ void seed_record_kernel(const float *__restrict__ seeds, int64_t n, i
         hpos[i] = seeds[i];
 }
 
+// Records of particles that left the live set (retired at compaction) are not written after
+// their retirement: they repeat the particle's frozen state, which is substituted when the rows
+// are read.  ret[pid] = the first position record not written for pid (a large value for
+// particles never retired), frz[pid * D + d] = its frozen value; history row x of the quantity
+// belongs to position record rec_of_row ? rec_of_row[x] : x + rec_offset.
+struct RowFill {
+    const int32_t *ret;
+    const float *frz;
+    int32_t rec_offset;
+    const int32_t *rec_of_row;
+};
+
 // Record-major history rows -> particle-major rows: records [r0, r1) of particles [p0, p1), D
 // floats each, from src[(r * n + p) * D + d] to dst[((p - p0) * nr + r - r0) * D + d], rows of nr
-// records (the layout of TrajectorySet's accessors, TrajectorySet.cpp:110-160).  A 32-record x 32-particle
-// tile through shared memory: reads run along a record row, writes along a particle's records,
-// both coalesced.
+// records (the layout of TrajectorySet's accessors, TrajectorySet.cpp:110-160), with the frozen
+// values of retired particles substituted (RowFill).  A 32-record x 32-particle tile through
+// shared memory: reads run along a record row, writes along a particle's records, both coalesced.
 template <int D>
 __global__ void __launch_bounds__(256) records_to_rows_kernel(const float *__restrict__ src, int64_t n, int32_t r0,
                                                               int32_t r1, int64_t p0, int64_t p1,
-                                                              float *__restrict__ dst, int32_t nr) {
+                                                              float *__restrict__ dst, int32_t nr, RowFill fill) {
     __shared__ float tile[32][32 * D + 1];
+    __shared__ int32_t ret[32];
     const int32_t rt = r0 + (int32_t)blockIdx.y * 32;
     const int64_t pt = p0 + (int64_t)blockIdx.x * 32;
+    if (threadIdx.x < 32) ret[threadIdx.x] = (fill.ret && pt + threadIdx.x < p1) ? fill.ret[pt + threadIdx.x] : 0x7fffffff;
+    __syncthreads();
     for (int idx = threadIdx.x; idx < 32 * 32 * D; idx += blockDim.x) {
         const int rr = idx / (32 * D), f = idx - rr * (32 * D);
-        if (rt + rr < r1 && pt + f / D < p1) tile[rr][f] = src[((int64_t)(rt + rr) * n + pt) * D + f];
+        const int q = f / D;
+        if (rt + rr < r1 && pt + q < p1) {
+            const int32_t r = rt + rr;
+            const int32_t rec = fill.rec_of_row ? fill.rec_of_row[r] : r + fill.rec_offset;
+            tile[rr][f] = rec >= ret[q] ? fill.frz[(pt + q) * D + (f - q * D)] : src[((int64_t)r * n + pt) * D + f];
+        }
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < 32 * 32 * D; idx += blockDim.x) {
@@ -113,6 +133,25 @@ __global__ void __launch_bounds__(256) records_to_rows_kernel(const float *__res
         const int rr = g / D, d = g - rr * D;
         if (rt + rr < r1 && pt + q < p1)
             dst[((pt + q - p0) * nr + (rt + rr - r0)) * D + d] = tile[rr][q * D + d];
+    }
+}
+
+// Per-particle retirement of the retired store so far: the first position record the particle
+// did not write (its retirement record) and its frozen position, volume / expression values and
+// per-step curvature, for RowFill.  Idempotent: runs before each read of the history.
+__global__ void note_retired_kernel(StateView R, const int32_t *n_ret, int dim, int nvol, int nexpr, int curv,
+                                    int64_t n, int32_t *ret, float *frz_pos, float *frz_vol, float *frz_cmp,
+                                    float *frz_curv) {
+    const int64_t nr = *n_ret;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nr; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pid = R.id[j];
+        ret[pid] = R.retire[j];
+        frz_pos[pid * dim] = R.px[j];
+        frz_pos[pid * dim + 1] = R.py[j];
+        if (dim == 3) frz_pos[pid * dim + 2] = R.pz[j];
+        for (int k = 0; k < nvol; ++k) frz_vol[k * n + pid] = R.volc[k * R.stride + j];
+        for (int k = 0; k < nexpr; ++k) frz_cmp[k * n + pid] = R.cmpc[k * R.stride + j];
+        if (curv) frz_curv[pid] = R.curv[j];
     }
 }
 
@@ -213,9 +252,12 @@ struct gr_engine {
     cudaEvent_t live_ready = nullptr;
     DevBuf<int32_t> c_key, c_hist, c_bintab, c_chunk, c_perm;
     int bx = 4, by = 4, bz = 2, nbx = 0, nby = 0, nbz = 0, nbins = 0;
-    DevBuf<int32_t> crec_of_rec;
+
     DevBuf<float> hpos, hcurv, hvol, hcmp;   // record-major (KParams)
     DevBuf<float> stage, sstage;             // particle-major chunks for the fetch / the streaming
+    DevBuf<int32_t> ret_rec;                 // retirement record per particle (RowFill)
+    DevBuf<float> frz_pos, frz_vol, frz_cmp, frz_curv;   // frozen values of retired particles
+    DevBuf<int32_t> rec_of_crec;             // position record of each curvature record
     DevBuf<int32_t> out_status;
     DevBuf<float> out_length, out_tc;
     DevBuf<unsigned long long> counters;
@@ -904,6 +946,7 @@ int reset_state(gr_engine *e) {
                                                              e->has_life ? e->life_src.p : nullptr, S.life.p);
     seed_record_kernel<<<grid_for(n * e->dim, threads), threads, 0, e->cs>>>(e->seeds.p, n, e->dim, e->hpos.p);
     CK(cudaGetLastError());
+    if (e->ret_rec.p) CK(cudaMemsetAsync(e->ret_rec.p, 0x7f, (size_t)n * sizeof(int32_t), e->cs));   // never retired
     CK(cudaMemsetAsync(e->counters.p, 0, 4 * sizeof(unsigned long long), e->cs));
     if (e->compacting) *e->h_live = (int32_t)n;
     e->stats.aux_launches += 3;
@@ -961,15 +1004,17 @@ void truncate_schedule(Schedule &sc, int64_t steps) {
 }
 
 // Channel-record index of each position record, for records written in steps [0, executed).
-std::vector<int32_t> crec_table(const gr_engine *e, const RunPlan &R, int64_t executed) {
-    std::vector<int32_t> t((size_t)e->L + 1, -1);
+// Position record of each curvature record (curvature records are written at position records
+// whose step had data.Time > 0, tpp:997-1012), for RowFill; unused entries hold a large value.
+std::vector<int32_t> rec_of_crec_table(const gr_engine *e, const RunPlan &R, int64_t executed) {
+    std::vector<int32_t> t((size_t)std::max<int64_t>(1, e->Lc), 0x7fffffff);
     int64_t rr = 1, cc = 0;
     for (int64_t k = 0; k < executed; ++k)
         if (R.sched.steps[k].save) {
-            if (R.sched.steps[k].time_pos) t[rr] = (int32_t)cc++;
+            if (R.sched.steps[k].time_pos && cc < (int64_t)t.size()) t[(size_t)cc++] = (int32_t)rr;
             ++rr;
         }
-    if (e->s.save_interval == 0 && executed > 0) t[rr] = (int32_t)cc;   // the final record
+    if (e->s.save_interval == 0 && executed > 0 && cc < (int64_t)t.size()) t[(size_t)cc] = (int32_t)rr;   // the final record
     return t;
 }
 
@@ -1092,6 +1137,12 @@ int run_prepare(gr_engine *e, RunPlan &R, bool graph) {
     if (e->Lc > 0) CK(e->hcurv.alloc(N * e->Lc));
     if (e->nvol > 0 && s.volume_mode != 0 && e->Li > 0) CK(e->hvol.alloc(N * e->Li * e->nvol));
     if (e->nexpr > 0 && e->Li > 0) CK(e->hcmp.alloc(N * e->Li * e->nexpr));
+    // retirement records and frozen values of retired particles (RowFill)
+    CK(e->ret_rec.alloc(N));
+    CK(e->frz_pos.alloc(N * e->dim));
+    if (e->hvol.p) CK(e->frz_vol.alloc(N * e->nvol));
+    if (e->hcmp.p) CK(e->frz_cmp.alloc(N * e->nexpr));
+    if (e->Lc > 0) CK(e->frz_curv.alloc(N));
 
     R.rec_before.assign((size_t)R.nsteps + 1, 1);
     for (int64_t k = 0; k < R.nsteps; ++k) R.rec_before[k + 1] = R.rec_before[k] + (R.sched.steps[k].save ? 1 : 0);
@@ -1110,10 +1161,10 @@ int run_prepare(gr_engine *e, RunPlan &R, bool graph) {
     if (graph) {
         if (e->use_pair)
             for (int b = 0; b < 2; ++b) CK(e->pairbuf[b].alloc(pair_bytes(e)));
-        // the fill-forward table of the full run, uploaded before the capture
-        const std::vector<int32_t> t = crec_table(e, R, R.nsteps);
-        CK(e->crec_of_rec.alloc(t.size()));
-        CK(cudaMemcpyAsync(e->crec_of_rec.p, t.data(), t.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e->cs));
+        // the curvature-record table of the full run, uploaded before the capture
+        const std::vector<int32_t> t = rec_of_crec_table(e, R, R.nsteps);
+        CK(e->rec_of_crec.alloc(t.size()));
+        CK(cudaMemcpyAsync(e->rec_of_crec.p, t.data(), t.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e->cs));
         CK(cudaStreamSynchronize(e->cs));
         CK(cudaStreamSynchronize(e->xs));   // snapshot uploads done: the graph waits on nothing outside
     }
@@ -1239,51 +1290,6 @@ int compact_pass(gr_engine *e, int32_t rec_now, int32_t k_end, bool graph) {
     e->cur = 1 - e->cur;
     e->stats.aux_launches += 6;
     return GR_OK;
-}
-
-// Records [max(retire, rec_lo), rec_end) of every retired particle repeat its final state:
-// positions, volume / compute records, and with a table its per-step curvature records from its
-// retirement on.  One thread per retired particle, walking its records (rows of the record-major
-// history).
-__global__ void fill_forward_kernel(const __grid_constant__ KParams P, StateView R, const int32_t *n_ret,
-                                    const int32_t *crec_of_rec, int32_t rec_lo, int32_t rec_end) {
-    const int64_t nr = *n_ret;
-    const int dim = P.dim;
-    const int64_t N = P.n_total;
-    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nr; j += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t pid = R.id[j];
-        const int32_t retire = R.retire[j];
-        const int32_t r0 = max(retire, rec_lo);
-        if (r0 < rec_end) {
-            const float x = R.px[j], y = R.py[j], z = dim == 3 ? R.pz[j] : 0.f;
-            for (int32_t r = r0; r < rec_end; ++r) {
-                float *hp = P.hpos + ((int64_t)r * N + pid) * dim;
-                hp[0] = x;
-                hp[1] = y;
-                if (dim == 3) hp[2] = z;
-            }
-            // volume / expression record r - 1 belongs to position record r
-            const int32_t i0 = max(r0 - 1, 0), i1 = rec_end - 1;
-            if (i1 > i0) {
-                if (P.volume_mode != 0)
-                    for (int k = 0; k < P.nvol; ++k) {
-                        const float val = R.volc[k * R.stride + j];
-                        for (int32_t r = i0; r < i1; ++r) P.hvol[((int64_t)k * P.Li + r) * N + pid] = val;
-                    }
-                for (int k = 0; k < P.nexpr; ++k) {
-                    const float val = R.cmpc[k * R.stride + j];
-                    for (int32_t r = i0; r < i1; ++r) P.hcmp[((int64_t)k * P.Li + r) * N + pid] = val;
-                }
-            }
-        }
-        if (crec_of_rec && P.curvature_mode == 3) {
-            const float cv = R.curv[j];
-            for (int32_t r = retire; r < rec_end; ++r) {
-                const int32_t cr = crec_of_rec[r];
-                if (cr >= 0) P.hcurv[(int64_t)cr * N + pid] = cv;
-            }
-        }
-    }
 }
 
 // Final per-particle outputs of the retired store.
@@ -1605,10 +1611,35 @@ int stream_begin(gr_engine *e, const RunPlan &R) {
     return GR_OK;
 }
 
+// Retirement records and frozen values of the retired store so far, on the step stream.
+int note_retired(gr_engine *e) {
+    const StateView Rv = view_of(e->ret, e->n);
+    const int nvol = e->hvol.p ? e->nvol : 0, nexpr = e->hcmp.p ? e->nexpr : 0;
+    note_retired_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(Rv, e->d_counts.p + 2, e->dim, nvol, nexpr,
+                                                               e->Lc > 0 ? 1 : 0, e->n, e->ret_rec.p, e->frz_pos.p,
+                                                               e->frz_vol.p, e->frz_cmp.p, e->frz_curv.p);
+    CK(cudaGetLastError());
+    e->stats.aux_launches++;
+    return GR_OK;
+}
+
+// The RowFill of a record-major quantity whose frozen values are frz (no substitution without a
+// retired store).
+RowFill row_fill(const gr_engine *e, const float *frz, int32_t rec_offset, const int32_t *rec_of_row) {
+    RowFill f{};
+    if (e->compacting && e->ret_rec.p) {
+        f.ret = e->ret_rec.p;
+        f.frz = frz;
+        f.rec_offset = rec_offset;
+        f.rec_of_row = rec_of_row;
+    }
+    return f;
+}
+
 // Record-major history -> particle-major rows on the device: records [r0, r1) of particles
 // [p0, p1) of a quantity with D floats per particle (records_to_rows_kernel), on `st`.
 int launch_records_to_rows(gr_engine *e, cudaStream_t st, const float *src, int64_t n, int D, int32_t r0,
-                           int32_t r1, int64_t p0, int64_t p1, float *dst) {
+                           int32_t r1, int64_t p0, int64_t p1, float *dst, const RowFill &fill) {
     constexpr int32_t kRowsPerLaunch = 32 * 65535;   // the grid's y extent
     for (int32_t a = r0; a < r1; a += kRowsPerLaunch) {
         const int32_t b = std::min(r1, a + kRowsPerLaunch);
@@ -1616,9 +1647,9 @@ int launch_records_to_rows(gr_engine *e, cudaStream_t st, const float *src, int6
         const dim3 grid((unsigned)((p1 - p0 + 31) / 32), (unsigned)((b - a + 31) / 32));
         float *d = dst + (int64_t)(a - r0) * D;
         const int32_t nr = r1 - r0;
-        if (D == 1) records_to_rows_kernel<1><<<grid, 256, 0, st>>>(src, n, a, b, p0, p1, d, nr);
-        else if (D == 2) records_to_rows_kernel<2><<<grid, 256, 0, st>>>(src, n, a, b, p0, p1, d, nr);
-        else records_to_rows_kernel<3><<<grid, 256, 0, st>>>(src, n, a, b, p0, p1, d, nr);
+        if (D == 1) records_to_rows_kernel<1><<<grid, 256, 0, st>>>(src, n, a, b, p0, p1, d, nr, fill);
+        else if (D == 2) records_to_rows_kernel<2><<<grid, 256, 0, st>>>(src, n, a, b, p0, p1, d, nr, fill);
+        else records_to_rows_kernel<3><<<grid, 256, 0, st>>>(src, n, a, b, p0, p1, d, nr, fill);
         CK(cudaGetLastError());
         e->stats.aux_launches++;
     }
@@ -1640,10 +1671,8 @@ int stream_records(RunCtx &r, int32_t r1) {
     const int32_t r0 = e->streamed;
     if (r1 <= r0 || e->n == 0) return GR_OK;
     if (e->compacting) {
-        const StateView Rv = view_of(e->ret, e->n);
-        fill_forward_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(r.P, Rv, e->d_counts.p + 2, nullptr, r0, r1);
-        CK(cudaGetLastError());
-        e->stats.aux_launches++;
+        const int rc = note_retired(e);
+        if (rc) return rc;
     }
     CK(cudaEventRecord(e->ds_ev, e->cs));
     CK(cudaStreamWaitEvent(e->ds, e->ds_ev, 0));
@@ -1653,7 +1682,8 @@ int stream_records(RunCtx &r, int32_t r1) {
     // floats, from column a * D: chunks of particles transposed into the streaming stage, each
     // followed by one pitched DMA (both on the copy-out stream, so a chunk's DMA ends before the
     // next transpose reuses the stage)
-    auto stream_rows = [&](float *dst, int64_t dpitch, const float *src, int D, int32_t a, int32_t b) -> int {
+    auto stream_rows = [&](float *dst, int64_t dpitch, const float *src, int D, int32_t a, int32_t b,
+                           const RowFill &fill) -> int {
         const int64_t w = (int64_t)(b - a) * D;
         const int64_t cp = stage_particles(n, w);
         if ((size_t)(cp * w) > e->sstage.count) {
@@ -1662,7 +1692,7 @@ int stream_records(RunCtx &r, int32_t r1) {
         }
         for (int64_t p0 = 0; p0 < n; p0 += cp) {
             const int64_t p1 = std::min(n, p0 + cp);
-            const int rc = launch_records_to_rows(e, e->ds, src, n, D, a, b, p0, p1, e->sstage.p);
+            const int rc = launch_records_to_rows(e, e->ds, src, n, D, a, b, p0, p1, e->sstage.p, fill);
             if (rc) return rc;
             CK(cudaMemcpy2DAsync(dst + p0 * dpitch + (int64_t)a * D, (size_t)dpitch * sizeof(float), e->sstage.p,
                                  (size_t)w * sizeof(float), (size_t)w * sizeof(float), (size_t)(p1 - p0),
@@ -1672,22 +1702,24 @@ int stream_records(RunCtx &r, int32_t r1) {
         return GR_OK;
     };
     if (d.positions) {
-        const int rc = stream_rows(d.positions, d.records_capacity * e->dim, e->hpos.p, e->dim, r0, r1);
+        const int rc = stream_rows(d.positions, d.records_capacity * e->dim, e->hpos.p, e->dim, r0, r1,
+                                   row_fill(e, e->frz_pos.p, 0, nullptr));
         if (rc) return rc;
     }
     // info record i belongs to position record i + 1
     const int32_t i0 = std::max(r0 - 1, 0), i1 = r1 - 1;
     if (i1 > i0) {
-        auto copy_info = [&](float *dst, const float *src) -> int {
+        // info record i belongs to position record i + 1
+        auto copy_info = [&](float *dst, const float *src, const float *frz) -> int {
             if (!dst) return GR_OK;
-            return stream_rows(dst, d.info_capacity, src, 1, i0, i1);
+            return stream_rows(dst, d.info_capacity, src, 1, i0, i1, row_fill(e, frz, 1, nullptr));
         };
         for (int k = 0; k < (e->s.volume_mode != 0 ? e->nvol : 0); ++k) {
-            const int rc = copy_info(d.volume_info[k], e->hvol.p + (size_t)k * n * e->Li);
+            const int rc = copy_info(d.volume_info[k], e->hvol.p + (size_t)k * n * e->Li, e->frz_vol.p + (size_t)k * n);
             if (rc) return rc;
         }
         for (int k = 0; k < e->nexpr; ++k) {
-            const int rc = copy_info(d.compute_info[k], e->hcmp.p + (size_t)k * n * e->Li);
+            const int rc = copy_info(d.compute_info[k], e->hcmp.p + (size_t)k * n * e->Li, e->frz_cmp.p + (size_t)k * n);
             if (rc) return rc;
         }
     }
@@ -1746,22 +1778,23 @@ int run_tail(RunCtx &r, RecordCounts &c) {
     CK(cudaGetLastError());
     e->stats.aux_launches++;
     if (e->compacting) {
-        // retired particles: their later records repeat the frozen state
+        // retired particles: their later records repeat the frozen state, substituted when the
+        // history is read (RowFill)
         std::vector<int32_t> t;
         if (!R.graph) {
-            t = crec_table(e, R, executed);
-            CK(e->crec_of_rec.alloc(t.size()));
-            CK(cudaMemcpyAsync(e->crec_of_rec.p, t.data(), t.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e->cs));
+            t = rec_of_crec_table(e, R, executed);
+            CK(e->rec_of_crec.alloc(t.size()));
+            CK(cudaMemcpyAsync(e->rec_of_crec.p, t.data(), t.size() * sizeof(int32_t), cudaMemcpyHostToDevice, e->cs));
         }
+        const int rc = note_retired(e);
+        if (rc) return rc;
         const StateView Rv = view_of(e->ret, e->n);
-        fill_forward_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(P, Rv, e->d_counts.p + 2, e->crec_of_rec.p,
-                                                                          e->streamed, (int32_t)c.rec);
         finalize_retired_kernel<<<grid_for(e->n, 256), 256, 0, e->cs>>>(Rv, e->d_counts.p + 2, s.abort_mode != 0,
                                                                          s.curvature_mode != 0, e->out_status.p,
                                                                          e->out_length.p, e->out_tc.p);
         CK(cudaGetLastError());
         if (!R.graph) CK(cudaStreamSynchronize(e->cs));   // the host table t is read by the copy above
-        e->stats.aux_launches += 2;
+        e->stats.aux_launches++;
     }
     return GR_OK;
 }
@@ -2043,13 +2076,15 @@ static int fetch_rows(gr_engine *e, void *out, int64_t capacity, const void *src
     return GR_OK;
 }
 
-// Records [0, R) of a record-major quantity (D floats per particle) into particle-major host rows
-// of R * D floats: chunks of particles transposed on the device into the staging buffer, each
-// fetched like any device rows.
-static int fetch_records(gr_engine *e, float *out, int64_t cap, const float *src, int D, int64_t R) {
+// Records [r0, r1) of a record-major quantity (D floats per particle) into particle-major host
+// rows of (r1 - r0) * D floats: chunks of particles transposed on the device into the staging
+// buffer (retired particles' frozen values substituted, RowFill), each fetched like any device
+// rows.
+static int fetch_records(gr_engine *e, float *out, int64_t cap, const float *src, int D, int64_t r0, int64_t r1,
+                         const RowFill &fill) {
     if (!e || !out) return USER_ERR("null argument >");
     if (!e->have_result) return USER_ERR("No result: run() has not completed. >");
-    const int64_t n = e->n, w = R * D;
+    const int64_t n = e->n, w = (r1 - r0) * D;
     if (cap < n * w) return USER_ERR("Output buffer too small. >");
     if (n == 0 || w == 0) return GR_OK;
     int rc = set_device(e);
@@ -2058,7 +2093,7 @@ static int fetch_records(gr_engine *e, float *out, int64_t cap, const float *src
     CK(e->stage.alloc((size_t)(cp * w)));
     for (int64_t p0 = 0; p0 < n; p0 += cp) {
         const int64_t p1 = std::min(n, p0 + cp);
-        rc = launch_records_to_rows(e, e->cs, src, n, D, 0, (int32_t)R, p0, p1, e->stage.p);
+        rc = launch_records_to_rows(e, e->cs, src, n, D, (int32_t)r0, (int32_t)r1, p0, p1, e->stage.p, fill);
         if (rc) return rc;
         CK(cudaStreamSynchronize(e->cs));
         rc = fetch_rows(e, out + p0 * w, (p1 - p0) * w, e->stage.p, p1 - p0, w, w, sizeof(float));
@@ -2069,14 +2104,15 @@ static int fetch_records(gr_engine *e, float *out, int64_t cap, const float *src
 
 int gr_fetch_positions(gr_engine *e, float *out, int64_t cap) {
     if (!e) return USER_ERR("null engine >");
-    return fetch_records(e, out, cap, e->hpos.p, e->dim, e->info.records);
+    return fetch_records(e, out, cap, e->hpos.p, e->dim, 0, e->info.records, row_fill(e, e->frz_pos.p, 0, nullptr));
 }
 
 int gr_fetch_final_positions(gr_engine *e, float *out, int64_t cap) {
     if (!e) return USER_ERR("null engine >");
     if (!e->have_result) return USER_ERR("No result: run() has not completed. >");
-    const float *last = e->hpos.p + (e->info.records - 1) * e->n * e->dim;   // the last record's row
-    return fetch_rows(e, out, cap, last, 1, e->n * e->dim, e->n * e->dim, sizeof(float));
+    // the last record's row
+    return fetch_records(e, out, cap, e->hpos.p, e->dim, e->info.records - 1, e->info.records,
+                         row_fill(e, e->frz_pos.p, 0, nullptr));
 }
 
 int gr_fetch_status(gr_engine *e, int32_t *out, int64_t cap) {
@@ -2099,21 +2135,24 @@ int gr_fetch_total_curvature(gr_engine *e, float *out, int64_t cap) {
 int gr_fetch_curvatures(gr_engine *e, float *out, int64_t cap) {
     if (!e) return USER_ERR("null engine >");
     if (e->info.curvature_records == 0) return GR_OK;
-    return fetch_records(e, out, cap, e->hcurv.p, 1, e->info.curvature_records);
+    return fetch_records(e, out, cap, e->hcurv.p, 1, 0, e->info.curvature_records,
+                         row_fill(e, e->frz_curv.p, 0, e->rec_of_crec.p));
 }
 
 int gr_fetch_volume_info(gr_engine *e, int32_t index, float *out, int64_t cap) {
     if (!e) return USER_ERR("null engine >");
     if (index < 0 || index >= e->info.n_volumes) return USER_ERR("TrajectorySet: Volume with given key does not exist! >");
     if (e->info.info_records == 0) return GR_OK;
-    return fetch_records(e, out, cap, e->hvol.p + (int64_t)index * e->n * e->Li, 1, e->info.info_records);
+    return fetch_records(e, out, cap, e->hvol.p + (int64_t)index * e->n * e->Li, 1, 0, e->info.info_records,
+                         row_fill(e, e->frz_vol.p + (int64_t)index * e->n, 1, nullptr));
 }
 
 int gr_fetch_compute_info(gr_engine *e, int32_t index, float *out, int64_t cap) {
     if (!e) return USER_ERR("null engine >");
     if (index < 0 || index >= e->info.n_expressions) return USER_ERR("TrajectorySet: Volume with given id does not exist! >");
     if (e->info.info_records == 0) return GR_OK;
-    return fetch_records(e, out, cap, e->hcmp.p + (int64_t)index * e->n * e->Li, 1, e->info.info_records);
+    return fetch_records(e, out, cap, e->hcmp.p + (int64_t)index * e->n * e->Li, 1, 0, e->info.info_records,
+                         row_fill(e, e->frz_cmp.p + (int64_t)index * e->n, 1, nullptr));
 }
 
 }  // extern "C"
