@@ -11,10 +11,11 @@ using AdvanceFn = void (*)(const KParams);
 // The feature set (FT_* in granite_kernels.cuh) a launch with parameters P may use: a lean
 // variant when every option it leaves out is off in P (window-pair layouts only), else generic.
 inline int kernel_features(const KParams &P, bool pair) {
-    if (!pair || P.compensated || P.uplift_mode != 0 || P.abort_mode != 0 || P.topography || P.sphere ||
-        P.border_mode != 0 || P.alive_at != nullptr || (P.curvature_mode != 0 && P.curvature_mode != 1))
+    if (!pair || P.uplift_mode != 0 || P.abort_mode != 0 || P.topography || P.sphere || P.border_mode != 0 ||
+        P.alive_at != nullptr || (P.curvature_mode != 0 && P.curvature_mode != 1))
         return FT_GENERIC;
     const bool extras = (P.volume_mode != 0 && P.nvol > 0) || P.nexpr > 0;
+    if (P.compensated) return (P.curvature_mode == 0 && !extras) ? (FT_LEAN | FT_COMP) : FT_GENERIC;
     return FT_LEAN | (P.curvature_mode == 1 ? FT_CURV : 0) | (extras ? FT_EXTRAS : 0);
 }
 

@@ -29,11 +29,12 @@ constexpr int GR_MAX_CON = 4;
 
 // Compile-time feature sets of the step kernel.  FT_GENERIC honours every runtime option.  A
 // lean variant (FT_LEAN) is picked by the host (kernel_features in advance.h) when the launch has
-// no Kahan positions, uplift, length abort, topography, sphere coordinates, loop borders or
-// per-step alive counts, and curvature Off or Total; FT_CURV / FT_EXTRAS say whether it keeps
-// total curvature and volume / expression values.  The lean variants drop the dead state from
-// registers; their arithmetic is the generic variant's.
-constexpr int FT_GENERIC = 0, FT_LEAN = 1, FT_CURV = 2, FT_EXTRAS = 4;
+// no uplift, length abort, topography, sphere coordinates, loop borders or per-step alive counts,
+// and curvature Off or Total; FT_CURV / FT_EXTRAS say whether it keeps total curvature and volume
+// / expression values, FT_COMP Kahan-compensated positions (instantiated alone: the precision
+// form).  The lean variants drop the dead state from registers; their arithmetic is the generic
+// variant's.
+constexpr int FT_GENERIC = 0, FT_LEAN = 1, FT_CURV = 2, FT_EXTRAS = 4, FT_COMP = 8;
 
 // Step-schedule flags.
 constexpr int SF_SAVE = 1;       // position / info record after this step
@@ -691,7 +692,7 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
     const int curvature_mode = LEAN ? ((FT & FT_CURV) ? 1 : 0) : P.curvature_mode;
     const int abort_mode = LEAN ? 0 : P.abort_mode;
     const int uplift_mode = LEAN ? 0 : P.uplift_mode;
-    const bool compensated = LEAN ? false : P.compensated != 0;
+    const bool compensated = LEAN ? (FT & FT_COMP) != 0 : P.compensated != 0;
     const bool topography = LEAN ? false : P.topography != 0;
     const int border_mode = LEAN ? 0 : P.border_mode;
     unsigned *const alive_at = LEAN ? nullptr : P.alive_at;
