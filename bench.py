@@ -826,17 +826,136 @@ def run_serve(args, world, rank, local, pg_dist):
     }
 
 
+GYRE_WORKLOAD = "gyre-2d-euler-1e4x1000"
+
+
+def run_gyre(args, world, rank, local, pg_dist):
+    """The 2D configuration: double gyre on 256 x 128 nodes, 10,000 particles, 1,000 Euler steps
+    of 0.01, a record after every step.  Device-resident (16-slot ring, engine events) and
+    through the pygranite API (constructor, Python loader, every record copied out), each run
+    checked against the float32 oracle."""
+    import torch
+    import pygranite_b200 as pg
+    from oracle import oracle as orc
+    from pygranite_b200 import capi
+    from pygranite_b200 import workloads as W
+
+    settings, src, seeds = W.config1()
+    n_snap = len(src.wind)
+    eng = capi.Engine(capi.settings_from_reference(settings, ring_slots=n_snap, device=local))
+    eng.set_seeds(seeds)
+    for k, snap in enumerate(src.wind):
+        eng.load_windfield(k, snap)
+    resident = lambda k: 1 if k < n_snap else 0  # noqa: E731
+    for _ in range(max(1, args.warmup)):
+        eng.run(resident)
+    ms = ps = 0.0
+    for _ in range(args.steps):
+        eng.run(resident)
+        st = eng.stats()
+        ms += st.run_ms
+        ps += st.particle_steps
+    res = eng.results(volumes=False, compute=False)
+    eng.close()
+    ref = orc.run(orc.settings(**settings), orc.Inputs(wind=src.wind, seeds=seeds), precision="f32",
+                  threads=os.cpu_count() or 1)
+    device_exact = bool(np.array_equal(res["trajectories"], ref["trajectories"]) and
+                        np.array_equal(res["status"], ref["status"]))
+    enums = dict(Space=pg.Space, Integrator=pg.Integrator, WindfieldMode=pg.WindfieldMode, BorderMode=pg.BorderMode,
+                 CurvatureMode=pg.CurvatureMode)
+    api_s, api_ps, api_exact = 0.0, 0, None
+    for k in range(1 + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s_ = W.apply_settings(pg.IntegratorSettings(), settings, enums)
+        s_.Device = local
+        out = pg.TrajectoryIntegrator(s_, W.make_loader(pg.DataLoader, src), pg.TrajectorySet(seeds)).compute()
+        traj = out.trajectories()
+        dt = time.perf_counter() - t0
+        if k >= 1:
+            api_s += dt
+            api_ps += out.particleSteps()
+        if k == args.steps:
+            api_exact = bool(np.array_equal(traj, ref["trajectories"]))
+    return {"metric": "particle-steps/s", "unit": "particle-steps/s", "dtype": "f32",
+            "config": {"workload": GYRE_WORKLOAD, "grid": [256, 128], "snapshots": n_snap, "particles": len(seeds),
+                       "steps": 1000, "records": int(res["trajectories"].shape[1])},
+            "value": ps / (ms / 1e3), "ms_per_step": ms / args.steps, "f32_bitexact": device_exact,
+            "e2e": {"value": api_ps / api_s, "ms_per_step": 1e3 * api_s / args.steps, "f32_bitexact": api_exact,
+                    "path": "TrajectoryIntegrator(settings, loader, TrajectorySet(seeds)).compute().trajectories()"}}
+
+
+# option combinations timed on the benchmark field (device-resident, 1e6 particles x 200 steps)
+OPTION_SETS = {
+    "rk4_plain": dict(CurvatureMode=0, AdditionalVolumeMode=0, AdditionalCompute=[]),
+    "rk4_benchmark_options": dict(),
+    "rk4_individual_curvature_length": dict(CurvatureMode=3, AbortMode=1, MaximumLength=60000.0,
+                                            AdditionalVolumeMode=0, AdditionalCompute=[]),
+    "rk4_fast_total_curvature_reverse": dict(CurvatureMode=2, Reverse=True, AdditionalVolumeMode=0,
+                                             AdditionalCompute=[]),
+    "euler_fitlength_uplift_topography": dict(Integrator=0, CurvatureMode=0, AbortMode=2, MaximumLength=60000.0,
+                                              UpLiftMode=1, AdditionalVolumeMode=0, AdditionalCompute=[]),
+    "rk4_kahan": dict(CurvatureMode=0, AdditionalVolumeMode=0, AdditionalCompute=[]),
+}
+
+
+def run_options(args, world, rank, local, pg_dist):
+    """Throughput of option combinations beside the benchmark's own, on its field and seeds
+    (1e6 particles, 200 steps, records every 10): which kernel variant each runs (lean or
+    generic) and its particle-steps/s, device-resident."""
+    from pygranite_b200 import capi
+    from pygranite_b200 import workloads as W
+
+    steps = 200
+    settings, src, seeds = W.config2(n_particles=1_000_000, n_snapshots=steps // 10 + 1, steps=steps, seed=rank)
+    n_snap = len(src.wind)
+    n = seeds.shape[0]
+    rng = np.random.default_rng(3)
+    lift = (rng.standard_normal((n, 3)) * np.array([5.0, 5.0, 1.0])).astype(np.float32)
+    topo = np.zeros((192, 192), np.float32)
+    topo[:, 150:] = 2000.0
+    out = {}
+    for name, over in OPTION_SETS.items():
+        st = dict(settings, **over)
+        extra = dict(compensated=1) if name == "rk4_kahan" else {}
+        eng = capi.Engine(capi.settings_from_reference(st, ring_slots=n_snap, device=local, **extra))
+        eng.set_seeds(seeds)
+        for k, snap in enumerate(src.wind):
+            eng.load_windfield(k, snap)
+        if st.get("AdditionalVolumeMode", 0):
+            eng.load_volume(0, 0, src.volumes[0]["T"])
+        for e_, code in enumerate(st.get("AdditionalCompute", [])):
+            eng.compile_expression(e_, code, ["T"], [])
+        if st.get("UpLiftMode", 0):
+            eng.load_uplift(0, lift)
+            eng.set_topography(topo)
+        resident = lambda k: 1 if k < n_snap else 0  # noqa: E731
+        eng.run(resident)
+        ms = ps = 0.0
+        for _ in range(3):
+            eng.run(resident)
+            s_ = eng.stats()
+            ms += s_.run_ms
+            ps += s_.particle_steps
+        out[name] = {"value": ps / (ms / 1e3), "ms_per_run": ms / 3, "settings": {k: v for k, v in over.items()}}
+        eng.close()
+    return {"metric": "particle-steps/s", "unit": "particle-steps/s", "dtype": "f32",
+            "config": {"workload": "options-3d-1e6x200", "grid": [192, 192, 64], "steps": steps, "records_every": 10},
+            "per_option_set": out}
+
+
 def run_forms(args, world, rank, local):
-    """The three forms beside the plain kernel, on one GPU, each its own phase after the plain
-    measurement: batching (BF16 and FP16 graphs against one plain FP32 run per set), serving
-    (the Poisson request stream) and precision (the 4e6-particle, 5,000-step configuration per
-    storage).  A form that fails reports its error instead of a figure."""
+    """The other configurations and the three forms beside the plain kernel, on one GPU, each its
+    own phase after the plain measurement: the 2D double gyre, option combinations, batching
+    (BF16 and FP16 graphs against one plain FP32 run per set), serving (the Poisson request
+    stream) and precision (the 4e6-particle, 5,000-step configuration per storage).  A phase
+    that fails reports its error instead of a figure."""
     import copy
     import traceback
     import torch
     forms = {}
-    for name, fn, kw in (("precision", run_precision, {}), ("batch", run_batch, {"storages": ["bf16", "f16"]}),
-                         ("serve", run_serve, {})):
+    for name, fn, kw in (("gyre", run_gyre, {}), ("options", run_options, {}), ("precision", run_precision, {}),
+                         ("batch", run_batch, {"storages": ["bf16", "f16"]}), ("serve", run_serve, {})):
         a = copy.copy(args)
         a.steps, a.warmup = min(args.steps, 5), min(args.warmup, 2)
         t0 = time.perf_counter()
