@@ -15,7 +15,7 @@ inline int kernel_features(const KParams &P, bool pair) {
         P.alive_at != nullptr || (P.curvature_mode != 0 && P.curvature_mode != 1))
         return FT_GENERIC;
     const bool extras = (P.volume_mode != 0 && P.nvol > 0) || P.nexpr > 0;
-    if (P.compensated) return (P.curvature_mode == 0 && !extras) ? (FT_LEAN | FT_COMP) : FT_GENERIC;
+    if (P.compensated) return extras ? FT_GENERIC : (FT_LEAN | FT_COMP | (P.curvature_mode == 1 ? FT_CURV : 0));
     return FT_LEAN | (P.curvature_mode == 1 ? FT_CURV : 0) | (extras ? FT_EXTRAS : 0);
 }
 

@@ -4,7 +4,7 @@
 // brick they sit in (4x4x2 nodes in 3D, 4x4 in 2D), so a warp samples neighbouring cells
 // and the gathers of one warp share cache lines.  Aborted particles go to a separate
 // retired store and are never launched again; the records they would have written later
-// are filled from their frozen state at the end of the run.  Per-particle arithmetic does
+// repeat their frozen state, substituted when the history is read (RowFill, engine.cu).  Per-particle arithmetic does
 // not depend on the order, so results stay bit-identical.
 //
 // Kernels are static: every translation unit that includes this header owns its instances.

@@ -31,8 +31,8 @@ constexpr int GR_MAX_CON = 4;
 // lean variant (FT_LEAN) is picked by the host (kernel_features in advance.h) when the launch has
 // no uplift, length abort, topography, sphere coordinates, loop borders or per-step alive counts,
 // and curvature Off or Total; FT_CURV / FT_EXTRAS say whether it keeps total curvature and volume
-// / expression values, FT_COMP Kahan-compensated positions (instantiated alone: the precision
-// form).  The lean variants drop the dead state from registers; their arithmetic is the generic
+// / expression values, FT_COMP Kahan-compensated positions (instantiated without extras: the
+// precision form).  The lean variants drop the dead state from registers; their arithmetic is the generic
 // variant's.
 constexpr int FT_GENERIC = 0, FT_LEAN = 1, FT_CURV = 2, FT_EXTRAS = 4, FT_COMP = 8;
 
@@ -265,14 +265,13 @@ __device__ __forceinline__ void tri3(const void *slot, const Cell3 &c, float &ou
 // Pair nodes of the last cell a particle sampled (window-pair layouts).  Consecutive samples of
 // one particle (its RK4 stages, its next step) mostly fall in the same cell, whose nodes then
 // need no new gathers; the values and the arithmetic are the same either way.  The cell is
-// identified by its first corner's index in the padded pair buffer (`base`); 3D 16-bit kernels
-// keep the raw nodes (32 registers), the float32 kernel 24 (back, front) pairs (48 registers;
-// AdvBounds gives its launch shape); 2D keeps 8 pairs (16 registers).
+// identified by its first corner's index in the padded pair buffer (`base`); 3D keeps 24 (back,
+// front) float pairs (48 registers; 16-bit nodes converted when loaded; AdvBounds gives the
+// launch shape), 2D 8 pairs (16 registers).
 struct SampleCache {
     int32_t base;
-    uint4 q[8];
     float2 c2d[2][4];  // 2D: (back, front) of u and v at the 4 corners
-    float2 c2[3][8];   // float32 3D: (back, front) of u, v, w at the 8 corners
+    float2 c2[3][8];   // 3D: (back, front) of u, v, w at the 8 corners
     __device__ __forceinline__ void reset() { base = -1; }
 };
 
@@ -326,8 +325,8 @@ __device__ __forceinline__ float2 tri8p(const float2 (&c)[8], float fx, float fy
     return lerp2_(lerp2_(a00, a10, fy), lerp2_(a01, a11, fy), fz);
 }
 
-// Loads the 8 padded corners of the cell at `base` into the sample cache: float32 as 24 (back,
-// front) pairs (u, v, w per corner), 16-bit as the raw 16-byte pair nodes.
+// Loads the 8 padded corners of the cell at `base` into the sample cache as 24 (back, front)
+// float pairs (u, v, w per corner); 16-bit nodes are converted once here, not per sample.
 template <typename H>
 __device__ __forceinline__ void fill_padded(const KParams &P, const void *pairs, int32_t base, SampleCache &cc) {
     const int32_t sy = P.pnx, sz = P.pnxy;
@@ -339,37 +338,24 @@ __device__ __forceinline__ void fill_padded(const KParams &P, const void *pairs,
             Store<Pair<float>>::load3p(pairs, idx, c);
             cc.c2[0][k] = c[0]; cc.c2[1][k] = c[1]; cc.c2[2][k] = c[2];
         } else {
-            cc.q[k] = __ldg(reinterpret_cast<const uint4 *>(pairs) + idx);
+            const uint4 q = __ldg(reinterpret_cast<const uint4 *>(pairs) + idx);
+            cc.c2[0][k] = Store<Pair<H>>::cvt(q.x);
+            cc.c2[1][k] = Store<Pair<H>>::cvt(q.y);
+            cc.c2[2][k] = Store<Pair<H>>::cvt(q.z);
         }
     }
     cc.base = base;
 }
 
-// float32: the cached corner pairs, reloaded when the cell changes; out[c] = (back, front) value
-// of component c at the sample.
-__device__ __forceinline__ void tri3p_padded32(const KParams &P, const void *pairs, const PCell &c, SampleCache &cc,
-                                               float2 (&out)[3]) {
-    if (c.base != cc.base) fill_padded<float>(P, pairs, c.base, cc);
+// The cached corner pairs, reloaded when the cell changes; out[c] = (back, front) value of
+// component c at the sample.  H: the pair's element type (float, bf16 or fp16).
+template <typename H>
+__device__ __forceinline__ void tri3p_padded(const KParams &P, const void *pairs, const PCell &c, SampleCache &cc,
+                                             float2 (&out)[3]) {
+    if (c.base != cc.base) fill_padded<H>(P, pairs, c.base, cc);
     out[0] = tri8p(cc.c2[0], c.fx, c.fy, c.fz);
     out[1] = tri8p(cc.c2[1], c.fx, c.fy, c.fz);
     out[2] = tri8p(cc.c2[2], c.fx, c.fy, c.fz);
-}
-
-// 16-bit: the 8 raw pair nodes, each word converted to a (back, front) pair per sample.
-template <typename H>
-__device__ __forceinline__ void tri3p_padded16(const KParams &P, const void *pairs, const PCell &c, SampleCache &cc,
-                                               float2 (&out)[3]) {
-    if (c.base != cc.base) fill_padded<H>(P, pairs, c.base, cc);
-    float2 u[8], v[8], w[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        u[k] = Store<Pair<H>>::cvt(cc.q[k].x);
-        v[k] = Store<Pair<H>>::cvt(cc.q[k].y);
-        w[k] = Store<Pair<H>>::cvt(cc.q[k].z);
-    }
-    out[0] = tri8p(u, c.fx, c.fy, c.fz);
-    out[1] = tri8p(v, c.fx, c.fy, c.fz);
-    out[2] = tri8p(w, c.fx, c.fy, c.fz);
 }
 
 template <typename W> struct PairElem { using type = void; };
@@ -481,10 +467,7 @@ __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, co
             const PCell c = make_pcell(P, ax, ay, az);
             float2 bf[3];
             using H = typename PairElem<W>::type;
-            if constexpr (std::is_same<H, float>::value)
-                tri3p_padded32(P, wb, c, cc, bf);
-            else
-                tri3p_padded16<H>(P, wb, c, cc, bf);
+            tri3p_padded<H>(P, wb, c, cc, bf);
             r.x = lerp_(bf[0].x, bf[0].y, t); r.y = lerp_(bf[1].x, bf[1].y, t); r.z = lerp_(bf[2].x, bf[2].y, t);
         } else {
             float2 bf[2];
