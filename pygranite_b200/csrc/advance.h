@@ -12,7 +12,7 @@ using AdvanceFn = void (*)(const KParams);
 // variant when every option it leaves out is off in P (window-pair layouts only), else generic.
 inline int kernel_features(const KParams &P, bool pair) {
     if (!pair || P.uplift_mode != 0 || P.abort_mode != 0 || P.topography || P.sphere || P.border_mode != 0 ||
-        P.alive_at != nullptr || (P.curvature_mode != 0 && P.curvature_mode != 1))
+        P.alive_at != nullptr || P.filter_weights || (P.curvature_mode != 0 && P.curvature_mode != 1))
         return FT_GENERIC;
     const bool extras = (P.volume_mode != 0 && P.nvol > 0) || P.nexpr > 0;
     if (P.compensated) return extras ? FT_GENERIC : (FT_LEAN | FT_COMP | (P.curvature_mode == 1 ? FT_CURV : 0));

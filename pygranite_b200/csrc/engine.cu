@@ -1191,6 +1191,7 @@ KParams make_params(gr_engine *e) {
         P.scale[d] = e->scale[d];
     }
     P.nx = (int32_t)e->nx; P.ny = (int32_t)e->ny; P.nz = (int32_t)e->nz; P.dim = e->dim;
+    P.fn[0] = (float)e->nx; P.fn[1] = (float)e->ny; P.fn[2] = (float)e->nz;
     P.pnx = (int32_t)(e->nx + 3); P.pnxy = (int32_t)((e->nx + 3) * (e->ny + 3));
     P.wind = e->wind.p; P.wind_stride = e->wind_stride;
     P.vol = e->vol.p; P.vol_plane = e->nodes;
@@ -1211,6 +1212,8 @@ KParams make_params(gr_engine *e) {
     P.h = s.delta_t;
     P.hh = 0.5f * s.delta_t;
     P.sixth = 1.0f / 6;
+    P.inv_2h = 1.0f / (2.0f * s.delta_t);
+    P.inv_hh = 1.0f / (s.delta_t * s.delta_t);
     P.max_length = s.maximum_length;
     P.sphere_radius = s.sphere_radius;
     P.wind_dynamic = e->wind_dynamic;

@@ -29,8 +29,8 @@ constexpr int GR_MAX_CON = 4;
 
 // Compile-time feature sets of the step kernel.  FT_GENERIC honours every runtime option.  A
 // lean variant (FT_LEAN) is picked by the host (kernel_features in advance.h) when the launch has
-// no uplift, length abort, topography, sphere coordinates, loop borders or per-step alive counts,
-// and curvature Off or Total; FT_CURV / FT_EXTRAS say whether it keeps total curvature and volume
+// no uplift, length abort, topography, sphere coordinates, loop borders, per-step alive counts
+// or 1/256 filter weights, and curvature Off or Total; FT_CURV / FT_EXTRAS say whether it keeps total curvature and volume
 // / expression values, FT_COMP Kahan-compensated positions (instantiated without extras: the
 // precision form).  The lean variants drop the dead state from registers; their arithmetic is the generic
 // variant's.
@@ -53,6 +53,7 @@ struct KParams {
     // geometry (TrajectoryIntegrator.tpp:521-574)
     float inv_scale[3], off[3], dom[3], scale[3];
     int32_t nx, ny, nz, dim;
+    float fn[3];                  // nx, ny, nz as floats (the upper clamp of the window pair's cells)
     // ring buffers: slot s of quantity q starts at base + s * stride
     const void *wind;
     int64_t wind_stride;          // bytes per slot
@@ -95,6 +96,7 @@ struct KParams {
     int32_t s0, s1;
     // options (runtime-uniform)
     float h, hh, sixth, max_length, sphere_radius;
+    float inv_2h, inv_hh;         // 1 / (2 h) and 1 / (h h), rounded to float (curvature differences)
     int32_t wind_dynamic, dyn_any, border_mode, curvature_mode, abort_mode, uplift_mode;
     int32_t constants_mode, volume_mode, reverse, sphere, topography, compensated;
     int32_t nvol, ncon, nexpr;
@@ -268,10 +270,13 @@ __device__ __forceinline__ void tri3(const void *slot, const Cell3 &c, float &ou
 // identified by its first corner's index in the padded pair buffer (`base`); 3D keeps 24 (back,
 // front) float pairs (48 registers; 16-bit nodes converted when loaded; AdvBounds gives the
 // launch shape), 2D 8 pairs (16 registers).
+// Corner k + 1 of each x pair (k even) is kept as its difference from corner k, formed once when
+// the cell is loaded: the x lerps of every later sample are then one paired FMA each, with the
+// difference lerp2_ would form (same instruction, same rounding).
 struct SampleCache {
     int32_t base;
-    float2 c2d[2][4];  // 2D: (back, front) of u and v at the 4 corners
-    float2 c2[3][8];   // 3D: (back, front) of u, v, w at the 8 corners
+    float2 c2d[2][4];  // 2D: (back, front) of u and v at corners 0, 2 and differences 1 - 0, 3 - 2
+    float2 c2[3][8];   // 3D: (back, front) of u, v, w at even corners, differences at odd ones
     __device__ __forceinline__ void reset() { base = -1; }
 };
 
@@ -292,21 +297,30 @@ struct PCell {
     float fx, fy, fz;
 };
 
-__device__ __forceinline__ void pcell1(float a, int n, int fw, int &i, float &f) {
-    a = fminf(fmaxf(a, -1.0f), (float)n);
-    const float fl = floorf(a);
-    i = (int)fl;
-    f = a - fl;
+// Cell of a padded-axis coordinate without the conversion unit.  a is clamped to [-1, n]
+// (n < 2^22); a + 1.5 * 2^23 rounded toward -infinity lies in [2^23, 2^24), where the floats
+// are the integers, so it is floor(a) + 1.5 * 2^23 exactly and its bit pattern is
+// PCELL_BITS + floor(a).  The fraction a + (1.5 * 2^23 - t) equals a - floorf(a) bit for bit,
+// the sign of a zero fraction included (an exact integer is subtracted either way).
+constexpr uint32_t PCELL_BITS = 0x4B400000u;   // bit pattern of 1.5 * 2^23
+__device__ __forceinline__ uint32_t pcell1(float a, float n, int fw, float &f) {
+    a = fminf(fmaxf(a, -1.0f), n);
+    const float t = __fadd_rd(a, 12582912.0f);
+    f = a + (12582912.0f - t);
     if (fw) f = floorf(f * 256.0f + 0.5f) * (1.0f / 256.0f);
+    return __float_as_uint(t);   // PCELL_BITS + floor(a)
 }
 
-__device__ __forceinline__ PCell make_pcell(const KParams &P, float ax, float ay, float az) {
-    int ix, iy, iz;
+// fw: the launch's filter_weights (0 where the variant has it off at compile time).  The
+// index (iz + 1) pnxy + (iy + 1) pnx + (ix + 1) is formed from the bit patterns of pcell1 in
+// wrapping 32-bit arithmetic, with the patterns' offset removed by one loop-invariant term.
+__device__ __forceinline__ PCell make_pcell(const KParams &P, float ax, float ay, float az, int fw) {
     PCell c;
-    pcell1(ax, P.nx, P.filter_weights, ix, c.fx);
-    pcell1(ay, P.ny, P.filter_weights, iy, c.fy);
-    pcell1(az, P.nz, P.filter_weights, iz, c.fz);
-    c.base = (iz + 1) * P.pnxy + (iy + 1) * P.pnx + (ix + 1);
+    const uint32_t bx = pcell1(ax, P.fn[0], fw, c.fx);
+    const uint32_t by = pcell1(ay, P.fn[1], fw, c.fy);
+    const uint32_t bz = pcell1(az, P.fn[2], fw, c.fz);
+    const uint32_t sy = (uint32_t)P.pnx, sz = (uint32_t)P.pnxy;
+    c.base = (int32_t)(bz * sz + by * sy + bx - (PCELL_BITS - 1u) * (sz + sy + 1u));
     return c;
 }
 
@@ -318,10 +332,15 @@ __device__ __forceinline__ float2 lerp2_(float2 a, float2 b, float t) {
     return __ffma2_rn(make_float2(t, t), d, a);
 }
 
-// Trilinear interpolation of 8 corner pairs: x, then y, then z (the order of tri3).
+// b - a of lerp2_, formed alone (the sample cache stores it for the x pairs).
+__device__ __forceinline__ float2 diff2_(float2 a, float2 b) { return __ffma2_rn(a, make_float2(-1.f, -1.f), b); }
+
+// Trilinear interpolation of 8 corner pairs (odd entries: differences, SampleCache): x, then y,
+// then z (the order of tri3).
 __device__ __forceinline__ float2 tri8p(const float2 (&c)[8], float fx, float fy, float fz) {
-    const float2 a00 = lerp2_(c[0], c[1], fx), a10 = lerp2_(c[2], c[3], fx);
-    const float2 a01 = lerp2_(c[4], c[5], fx), a11 = lerp2_(c[6], c[7], fx);
+    const float2 tx = make_float2(fx, fx);
+    const float2 a00 = __ffma2_rn(tx, c[1], c[0]), a10 = __ffma2_rn(tx, c[3], c[2]);
+    const float2 a01 = __ffma2_rn(tx, c[5], c[4]), a11 = __ffma2_rn(tx, c[7], c[6]);
     return lerp2_(lerp2_(a00, a10, fy), lerp2_(a01, a11, fy), fz);
 }
 
@@ -333,15 +352,21 @@ __device__ __forceinline__ void fill_padded(const KParams &P, const void *pairs,
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const int32_t idx = base + ((k & 1) ? 1 : 0) + ((k & 2) ? sy : 0) + ((k & 4) ? sz : 0);
+        float2 c[3];
         if constexpr (std::is_same<H, float>::value) {
-            float2 c[3];
             Store<Pair<float>>::load3p(pairs, idx, c);
-            cc.c2[0][k] = c[0]; cc.c2[1][k] = c[1]; cc.c2[2][k] = c[2];
         } else {
             const uint4 q = __ldg(reinterpret_cast<const uint4 *>(pairs) + idx);
-            cc.c2[0][k] = Store<Pair<H>>::cvt(q.x);
-            cc.c2[1][k] = Store<Pair<H>>::cvt(q.y);
-            cc.c2[2][k] = Store<Pair<H>>::cvt(q.z);
+            c[0] = Store<Pair<H>>::cvt(q.x);
+            c[1] = Store<Pair<H>>::cvt(q.y);
+            c[2] = Store<Pair<H>>::cvt(q.z);
+        }
+        if (k & 1) {
+            cc.c2[0][k] = diff2_(cc.c2[0][k - 1], c[0]);
+            cc.c2[1][k] = diff2_(cc.c2[1][k - 1], c[1]);
+            cc.c2[2][k] = diff2_(cc.c2[2][k - 1], c[2]);
+        } else {
+            cc.c2[0][k] = c[0]; cc.c2[1][k] = c[1]; cc.c2[2][k] = c[2];
         }
     }
     cc.base = base;
@@ -413,27 +438,28 @@ __device__ __forceinline__ void bil2(const void *slot, const Cell2 &c, float &ou
 // axis are the same edge node, interpolated with any fraction to that node's value exactly.
 // The cache keeps the 4 corners as floats (16 registers), keyed by the first corner's index.
 template <typename W>
-__device__ __forceinline__ void bil2p_padded(const KParams &P, const void *pairs, float ax, float ay, SampleCache &cc,
-                                             float2 (&out)[2]) {
-    int ix, iy;
+__device__ __forceinline__ void bil2p_padded(const KParams &P, const void *pairs, float ax, float ay, int fw,
+                                             SampleCache &cc, float2 (&out)[2]) {
     float fx, fy;
-    pcell1(ax, P.nx, P.filter_weights, ix, fx);
-    pcell1(ay, P.ny, P.filter_weights, iy, fy);
-    const int32_t base = (iy + 1) * P.pnx + (ix + 1);
+    const uint32_t bx = pcell1(ax, P.fn[0], fw, fx);
+    const uint32_t by = pcell1(ay, P.fn[1], fw, fy);
+    const uint32_t sy = (uint32_t)P.pnx;
+    const int32_t base = (int32_t)(by * sy + bx - (PCELL_BITS - 1u) * (sy + 1u));   // (iy + 1) pnx + (ix + 1)
     if (base != cc.base) {
         const int32_t idx[4] = {base, base + 1, base + P.pnx, base + P.pnx + 1};
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             float2 c[2];
             Store<W>::load2p(pairs, idx[k], c);
-            cc.c2d[0][k] = c[0];
-            cc.c2d[1][k] = c[1];
+            cc.c2d[0][k] = (k & 1) ? diff2_(cc.c2d[0][k - 1], c[0]) : c[0];
+            cc.c2d[1][k] = (k & 1) ? diff2_(cc.c2d[1][k - 1], c[1]) : c[1];
         }
         cc.base = base;
     }
 #pragma unroll
     for (int k = 0; k < 2; ++k)
-        out[k] = lerp2_(lerp2_(cc.c2d[k][0], cc.c2d[k][1], fx), lerp2_(cc.c2d[k][2], cc.c2d[k][3], fx), fy);
+        out[k] = lerp2_(__ffma2_rn(make_float2(fx, fx), cc.c2d[k][1], cc.c2d[k][0]),
+                        __ffma2_rn(make_float2(fx, fx), cc.c2d[k][3], cc.c2d[k][2]), fy);
 }
 
 
@@ -454,24 +480,26 @@ __device__ __forceinline__ float dot3(const V3 &a, const V3 &b, int dim) {
 }
 
 // Wind at world position p, time weight t: interpolate() of TrajectoryIntegrator.icc:42-110.
-template <int DIM, typename W>
+// FT: the step kernel's feature set; lean variants run with filter_weights off (kernel_features).
+template <int DIM, typename W, int FT = FT_GENERIC>
 __device__ __forceinline__ V3 wind_at(const KParams &P, const V3 &p, float t, const void *wb, const void *wf,
                                       SampleCache &cc) {
     V3 r{0.f, 0.f, 0.f};
+    const int fw = (FT & FT_LEAN) ? 0 : P.filter_weights;
     const float ax = (p.x - P.off[0]) * P.inv_scale[0];
     const float ay = (p.y - P.off[1]) * P.inv_scale[1];
     if constexpr (IsPair<W>::value) {
         // window-pair layout (dynamic wind only): wb points at the pair buffer
         if (DIM == 3) {
             const float az = (p.z - P.off[2]) * P.inv_scale[2];
-            const PCell c = make_pcell(P, ax, ay, az);
+            const PCell c = make_pcell(P, ax, ay, az, fw);
             float2 bf[3];
             using H = typename PairElem<W>::type;
             tri3p_padded<H>(P, wb, c, cc, bf);
             r.x = lerp_(bf[0].x, bf[0].y, t); r.y = lerp_(bf[1].x, bf[1].y, t); r.z = lerp_(bf[2].x, bf[2].y, t);
         } else {
             float2 bf[2];
-            bil2p_padded<W>(P, wb, ax, ay, cc, bf);
+            bil2p_padded<W>(P, wb, ax, ay, fw, cc, bf);
             r.x = lerp_(bf[0].x, bf[0].y, t); r.y = lerp_(bf[1].x, bf[1].y, t);
         }
         return r;
@@ -661,6 +689,31 @@ __device__ __forceinline__ void store_extras(const KParams &P, int64_t i, const 
 
 // ------------------------------------------------------------------ the step kernel
 
+// Volume / expression values at a record or at the end of a launch (tpp:363-435): evaluated if
+// an alive step has passed since the last evaluation (`dirty`, then kept in the state arrays),
+// else the state arrays' values; written to the record's rows when irec >= 0.  Not inlined: it
+// runs once per record, and its register peak (the expression stack, the volume samples) then
+// stays out of the step loop's allocation; the caller's live registers are saved around the call.
+template <int DIM>
+__device__ __noinline__ void record_extras(const KParams &P, int64_t i, int64_t pid, bool dirty, int last_s,
+                                           V3 p, V3 vc_last, float cv, int32_t irec) {
+    float vol[GR_MAX_VOL], cmp[GR_MAX_EXPR];
+    load_extras(P, i, dirty, vol, cmp);
+    if (dirty) {
+        eval_extras<DIM>(P, P.sched[last_s], pid, p, vc_last, cv, vol, cmp);
+        store_extras(P, i, vol, cmp);
+    }
+    if (irec < 0) return;
+    if (P.volume_mode != 0) {
+#pragma unroll
+        for (int k = 0; k < GR_MAX_VOL; ++k)
+            if (k < P.nvol) P.hvol[((int64_t)k * P.Li + irec) * P.n_total + pid] = vol[k];
+    }
+#pragma unroll
+    for (int e = 0; e < GR_MAX_EXPR; ++e)
+        if (e < P.nexpr) P.hcmp[((int64_t)e * P.Li + irec) * P.n_total + pid] = cmp[e];
+}
+
 #ifndef GR_ADV_MIN_BLOCKS
 #define GR_ADV_MIN_BLOCKS 2
 #endif
@@ -688,10 +741,15 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
     float len = 0.f, tc = 0.f, cv = 0.f;
 
     const bool curv_prev = curvature_mode == 1 || curvature_mode == 3;
+    float seg = 0.f;   // |p - q| (curvature's ds): carried from the step that formed it
     if (valid) {
         p.x = P.px[i]; p.y = P.py[i];
         if (DIM == 3) p.z = P.pz[i];
-        if (curv_prev) { q.x = P.qx[i]; q.y = P.qy[i]; if (DIM == 3) q.z = P.qz[i]; }
+        if (curv_prev) {
+            q.x = P.qx[i]; q.y = P.qy[i]; if (DIM == 3) q.z = P.qz[i];
+            const V3 a{p.x - q.x, p.y - q.y, p.z - q.z};
+            seg = sqrtf(dot3(a, a, DIM));
+        }
         if (compensated) { comp.x = P.kx[i]; comp.y = P.ky[i]; if (DIM == 3) comp.z = P.kz[i]; }
         if (curvature_mode == 2) { ld.x = P.lx[i]; ld.y = P.ly[i]; if (DIM == 3) ld.z = P.lz[i]; }
         if (abort_mode != 0) len = P.length[i];
@@ -729,7 +787,7 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
 #pragma unroll 1
                 for (int stage = 0; stage < 4; ++stage) {
                     const float tw = stage == 0 ? t0 : (stage == 3 ? E.t2 : E.t1);
-                    const V3 kc = wind_at<DIM, W>(P, a, tw, wb, wf, cc);
+                    const V3 kc = wind_at<DIM, W, FT>(P, a, tw, wb, wf, cc);
                     const V3 k = sph ? sphere_(P, a.y, kc) : kc;
                     if (stage == 0) {
                         acc = k;
@@ -753,7 +811,7 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
                     vc = v;
                 }
             } else {
-                vc = wind_at<DIM, W>(P, p, t0, wb, wf, cc);
+                vc = wind_at<DIM, W, FT>(P, p, t0, wb, wf, cc);
                 v = sph ? sphere_(P, p.y, vc) : vc;
             }
 
@@ -876,21 +934,27 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
                         if (!isnan(k)) tc += k;
                     }
                     ld = u;
-                } else if (curv_prev && (E.flags & SF_TIME_POS)) {
-                    float k = 0.f;
-                    if (DIM == 3) {
-                        const float two_dt = 2.f * P.h, dt2 = P.h * P.h;
-                        const V3 d1{(np.x - q.x) / two_dt, (np.y - q.y) / two_dt, (np.z - q.z) / two_dt};
-                        const V3 d2{((q.x + np.x) - 2.f * p.x) / dt2, ((q.y + np.y) - 2.f * p.y) / dt2,
-                                    ((q.z + np.z) - 2.f * p.z) / dt2};
-                        const V3 x{d1.y * d2.z - d1.z * d2.y, d1.z * d2.x - d1.x * d2.z, d1.x * d2.y - d1.y * d2.x};
-                        const float l = sqrtf(dot3(d1, d1, 3));
-                        k = fabsf(sqrtf(dot3(x, x, 3)) / (l * l * l));
+                } else if (curv_prev) {
+                    // |np - p|: this segment's length, the next step's |p - q|
+                    const V3 b{np.x - p.x, np.y - p.y, np.z - p.z};
+                    const float nseg = sqrtf(dot3(b, b, DIM));
+                    if (E.flags & SF_TIME_POS) {
+                        float k = 0.f;
+                        if (DIM == 3) {
+                            // central differences scaled by the float reciprocals of 2 h and h h
+                            // (the reference divides, icc:151-154: within one rounding of these)
+                            const V3 d1{(np.x - q.x) * P.inv_2h, (np.y - q.y) * P.inv_2h, (np.z - q.z) * P.inv_2h};
+                            const V3 d2{((q.x + np.x) - 2.f * p.x) * P.inv_hh, ((q.y + np.y) - 2.f * p.y) * P.inv_hh,
+                                        ((q.z + np.z) - 2.f * p.z) * P.inv_hh};
+                            const V3 x{d1.y * d2.z - d1.z * d2.y, d1.z * d2.x - d1.x * d2.z, d1.x * d2.y - d1.y * d2.x};
+                            const float l = sqrtf(dot3(d1, d1, 3));
+                            k = fabsf(sqrtf(dot3(x, x, 3)) / (l * l * l));
+                        }
+                        const float ds = 0.5f * (seg + nseg);
+                        if (curvature_mode == 3) cv = k;
+                        if (!isnan(k)) tc += k * ds;
                     }
-                    const V3 a{p.x - q.x, p.y - q.y, p.z - q.z}, b{np.x - p.x, np.y - p.y, np.z - p.z};
-                    const float ds = 0.5f * (sqrtf(dot3(a, a, DIM)) + sqrtf(dot3(b, b, DIM)));
-                    if (curvature_mode == 3) cv = k;
-                    if (!isnan(k)) tc += k * ds;
+                    seg = nseg;
                 }
 
                 // volumes and expressions are evaluated lazily (eval_extras)
@@ -910,29 +974,14 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
             if (DIM == 3) hp[2] = p.z;
             if (curvature_mode == 3 && (E.flags & SF_CURV_REC)) P.hcurv[(int64_t)E.crec * P.n_total + pid] = cv;
             if (extras) {
-                // volume / expression values: evaluated now if an alive step has passed since the
-                // last evaluation (and kept in the state arrays), else the state arrays' values
-                float vol[GR_MAX_VOL], cmp[GR_MAX_EXPR];
-                load_extras(P, i, dirty, vol, cmp);
-                if (dirty) {
-                    eval_extras<DIM>(P, P.sched[last_s], pid, p, vc_last, cv, vol, cmp);
-                    store_extras(P, i, vol, cmp);
-                    dirty = false;
-                }
-                if (P.volume_mode != 0) {
-#pragma unroll
-                    for (int k = 0; k < GR_MAX_VOL; ++k)
-                        if (k < P.nvol) P.hvol[((int64_t)k * P.Li + E.irec) * P.n_total + pid] = vol[k];
-                }
-#pragma unroll
-                for (int e = 0; e < GR_MAX_EXPR; ++e)
-                    if (e < P.nexpr) P.hcmp[((int64_t)e * P.Li + E.irec) * P.n_total + pid] = cmp[e];
+                record_extras<DIM>(P, i, pid, dirty, last_s, p, vc_last, cv, E.irec);
+                dirty = false;
                 // refill the sample cache for the next step's first sample (at p): the cached
                 // nodes are then dead while the values above are evaluated, which frees their
                 // registers there
                 if constexpr (IsPair<W>::value && DIM == 3) {
                     const PCell c = make_pcell(P, (p.x - P.off[0]) * P.inv_scale[0], (p.y - P.off[1]) * P.inv_scale[1],
-                                               (p.z - P.off[2]) * P.inv_scale[2]);
+                                               (p.z - P.off[2]) * P.inv_scale[2], LEAN ? 0 : P.filter_weights);
                     fill_padded<typename PairElem<W>::type>(P, P.pair, c.base, cc);
                 }
             }
@@ -948,12 +997,7 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
     }
 
     if (valid && was_alive) {
-        if (extras && dirty) {
-            float vol[GR_MAX_VOL], cmp[GR_MAX_EXPR];
-            load_extras(P, i, true, vol, cmp);
-            eval_extras<DIM>(P, P.sched[last_s], pid, p, vc_last, cv, vol, cmp);
-            store_extras(P, i, vol, cmp);
-        }
+        if (extras && dirty) record_extras<DIM>(P, i, pid, true, last_s, p, vc_last, cv, -1);
         P.status[i] = st;
         P.px[i] = p.x; P.py[i] = p.y;
         if (DIM == 3) P.pz[i] = p.z;
@@ -972,13 +1016,24 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
 // One thread per particle, or (P.grid_stride) a persistent grid striding over the live
 // prefix, whose size is read on the device: the launch shape then stays fixed while the live
 // count shrinks, as a captured CUDA graph needs.
-// Launch bounds: 256 threads, 2 blocks per SM (128 registers); the float32 3D pair kernel keeps
-// 48 cached floats and runs 128-thread blocks, 3 per SM (up to 170 registers).
+// Launch bounds: 256 threads, 2 blocks per SM (128 registers).  The float32 3D pair kernel keeps
+// 48 cached floats in 128-thread blocks: 4 per SM (128 registers) in the generic variant and the
+// lean ones with volume / expression values or with both Kahan positions and curvature, 5 per SM
+// (96 registers, 20 warps) in the other lean ones, whose state fits there without spills; the
+// extra warps hide more of the sampling and curvature latency.  The 16-bit kernels keep 256 x 2
+// (measured faster than 128 x 5 there).
 template <int DIM, typename W, int FT> struct AdvBounds { static constexpr int threads = 256, blocks = GR_ADV_MIN_BLOCKS; };
 #ifndef GR_F32_PAIR_BLOCKS
 #define GR_F32_PAIR_BLOCKS 4
 #endif
-template <int FT> struct AdvBounds<3, Pair<float>, FT> { static constexpr int threads = 128, blocks = GR_F32_PAIR_BLOCKS; };
+#ifndef GR_F32_LIGHT_BLOCKS
+#define GR_F32_LIGHT_BLOCKS 5
+#endif
+template <int FT> struct AdvBounds<3, Pair<float>, FT> {
+    static constexpr bool light = (FT & FT_LEAN) != 0 && (FT & FT_EXTRAS) == 0 &&
+                                  (FT & (FT_COMP | FT_CURV)) != (FT_COMP | FT_CURV);
+    static constexpr int threads = 128, blocks = light ? GR_F32_LIGHT_BLOCKS : GR_F32_PAIR_BLOCKS;
+};
 
 template <int DIM, bool RK4, typename W, int FT>
 __global__ void __launch_bounds__(AdvBounds<DIM, W, FT>::threads, AdvBounds<DIM, W, FT>::blocks)

@@ -245,6 +245,7 @@ extern "C" int gr_advance_noalloc(const gr_settings *s, int64_t nz, int64_t ny, 
         P.dom[d] = g[d] * scale[d];
     }
     P.nx = (int32_t)nx; P.ny = (int32_t)ny; P.nz = (int32_t)(dim == 3 ? nz : 1); P.dim = dim;
+    P.fn[0] = (float)P.nx; P.fn[1] = (float)P.ny; P.fn[2] = (float)P.nz;
     P.wind = wind_back;
     P.wind_stride = reinterpret_cast<const char *>(wind_front) - reinterpret_cast<const char *>(wind_back);
     P.px = px; P.py = py; P.pz = pz; P.status = status;
@@ -254,6 +255,8 @@ extern "C" int gr_advance_noalloc(const gr_settings *s, int64_t nz, int64_t ny, 
     P.h = h;
     P.hh = 0.5f * h;
     P.sixth = 1.0f / 6;
+    P.inv_2h = 1.0f / (2.0f * h);
+    P.inv_hh = 1.0f / (h * h);
     P.sphere_radius = s->sphere_radius;
     P.filter_weights = s->filter_weights ? 1 : 0;
     P.wind_dynamic = 1;

@@ -378,8 +378,9 @@ int allocate(gr_server *S, int64_t budget) {
         P.threads = 256;
         const int st = S->s.storage;
         // positions only (no curvature, volumes, constants, uplift, length abort, compensation):
-        // the lean variant unless 2D loop borders or sphere coordinates are on
-        const bool lean = !(S->dim == 2 && (S->s.border_mode != 0 || S->s.sphere_radius > 0.f));
+        // the lean variant unless 2D loop borders, sphere coordinates or 1/256 filter weights are on
+        const bool lean = !(S->dim == 2 && (S->s.border_mode != 0 || S->s.sphere_radius > 0.f)) &&
+                          !S->s.filter_weights;
         const int ft = lean ? FT_LEAN : FT_GENERIC;
         P.fn = st == GR_STORE_BF16 ? advance_bf16(S->dim, p == 1, true, ft)
              : st == GR_STORE_F16 ? advance_f16(S->dim, p == 1, true, ft) : advance_f32(S->dim, p == 1, true, ft);
@@ -412,6 +413,7 @@ KParams pool_params(gr_server *S, Pool &P) {
         K.scale[d] = S->scale[d];
     }
     K.nx = (int32_t)S->nx; K.ny = (int32_t)S->ny; K.nz = (int32_t)S->nz; K.dim = S->dim;
+    K.fn[0] = (float)S->nx; K.fn[1] = (float)S->ny; K.fn[2] = (float)S->nz;
     K.wind = S->ring.p;
     K.wind_stride = S->slot_stride;
     K.pair = S->pair.p;
@@ -427,6 +429,8 @@ KParams pool_params(gr_server *S, Pool &P) {
     K.h = s.delta_t;
     K.hh = 0.5f * s.delta_t;
     K.sixth = 1.0f / 6;
+    K.inv_2h = 1.0f / (2.0f * s.delta_t);
+    K.inv_hh = 1.0f / (s.delta_t * s.delta_t);
     K.sphere_radius = s.sphere_radius;
     K.wind_dynamic = 1;
     K.dyn_any = 1;
