@@ -1,6 +1,6 @@
 // advance.cu — instantiates the step kernel (granite_kernels.cuh) for one wind storage type,
 // chosen by the build: GR_ADVANCE_F32, GR_ADVANCE_BF16 or GR_ADVANCE_F16.  Ring layouts get the
-// generic variant only; window-pair layouts also the six lean ones (advance.h).
+// generic variant only; window-pair layouts also the eight lean ones (advance.h).
 #include "advance.h"
 
 namespace granite_b200 {
@@ -16,6 +16,8 @@ AdvanceFn pick_pair(int ft) {
         case FT_LEAN | FT_CURV | FT_EXTRAS: return advance_kernel<DIM, RK4, Pair<T>, FT_LEAN | FT_CURV | FT_EXTRAS>;
         case FT_LEAN | FT_COMP: return advance_kernel<DIM, RK4, Pair<T>, FT_LEAN | FT_COMP>;
         case FT_LEAN | FT_COMP | FT_CURV: return advance_kernel<DIM, RK4, Pair<T>, FT_LEAN | FT_COMP | FT_CURV>;
+        case FT_LEAN | FT_DEFER: return advance_kernel<DIM, RK4, Pair<T>, FT_LEAN | FT_DEFER>;
+        case FT_LEAN | FT_CURV | FT_DEFER: return advance_kernel<DIM, RK4, Pair<T>, FT_LEAN | FT_CURV | FT_DEFER>;
         default: return advance_kernel<DIM, RK4, Pair<T>, FT_GENERIC>;
     }
 }

@@ -25,6 +25,7 @@ constexpr int SCAN_CHUNK = 1024;   // bins per block of the first scan level
 struct StateView {
     float *px, *py, *pz, *qx, *qy, *qz, *kx, *ky, *kz, *lx, *ly, *lz;
     float *length, *tc, *curv, *volc, *cmpc;
+    float4 *vlast;    // deferred volume / expression inputs (KParams::vlast), or null
     int32_t *status, *id, *retire, *life, *birth;
     int64_t stride;   // per-array stride of volc / cmpc
 };
@@ -166,6 +167,7 @@ __device__ __forceinline__ void move_live(const CompactParams &C, int64_t i, int
     if (C.curv_ind) D.curv[d] = S.curv[i];
     for (int k = 0; k < C.nvol; ++k) D.volc[k * D.stride + d] = S.volc[k * S.stride + i];
     for (int k = 0; k < C.nexpr; ++k) D.cmpc[k * D.stride + d] = S.cmpc[k * S.stride + i];
+    if (S.vlast) D.vlast[d] = S.vlast[i];
     D.status[d] = S.status[i];
     D.id[d] = S.id[i];
     if (S.life) D.life[d] = S.life[i];

@@ -238,11 +238,13 @@ struct gr_engine {
     DevBuf<float> seeds;               // AoS n x dim
     struct State {
         DevBuf<float> px, py, pz, qx, qy, qz, kx, ky, kz, lx, ly, lz, length, tc, curv, volc, cmpc;
+        DevBuf<float4> vlast;          // inputs of deferred volume / expression values
         DevBuf<int32_t> status, id, retire, life;
     };
     State st[2];                       // double-buffered live state (compaction swaps)
     State ret;                         // retired particles (frozen state)
     State ck;                          // MinimumAliveParticles: state before the current launch
+    DevBuf<float4> vrec;               // inputs of a record's deferred volume / expression values
     DevBuf<unsigned> alive_at;         // per-step alive counts of a launch, 32 shards per step
     std::vector<unsigned> h_alive;
     int cur = 0;
@@ -833,6 +835,7 @@ struct RunPlan {
     Schedule sched;
     int64_t nsteps = 0, nwin = 0;
     std::vector<int32_t> rec_before;   // records written before step k: 1 + saves in [0, k)
+    std::vector<int64_t> save_next;    // first save step >= k (nsteps if none)
     int64_t spl = 0;                   // steps per launch
     bool graph = false;                // fixed launch shapes and no host reads (graph capture)
 };
@@ -853,6 +856,8 @@ int alloc_set(gr_engine *e, gr_engine::State &S, bool retired) {
     CK(S.length.alloc(N)); CK(S.tc.alloc(N)); CK(S.curv.alloc(N));
     const int nv = std::max(1, e->nvol), ne = std::max(1, e->nexpr);
     CK(S.volc.alloc(N * nv)); CK(S.cmpc.alloc(N * ne));
+    const bool extras = (e->s.volume_mode != 0 && e->nvol > 0) || e->nexpr > 0;
+    if (!retired && extras) CK(S.vlast.alloc(N));
     return GR_OK;
 }
 
@@ -861,6 +866,7 @@ int alloc_state(gr_engine *e) {
     const size_t N = (size_t)e->n;
     int rc = alloc_set(e, e->st[0], false);
     if (rc) return rc;
+    if (e->st[0].vlast.p) CK(e->vrec.alloc(N));
     CK(e->out_status.alloc(N)); CK(e->out_length.alloc(N)); CK(e->out_tc.alloc(N));
     e->compacting = e->s.sort_interval > 0;
     CK(e->d_counts.alloc(4));
@@ -939,6 +945,7 @@ int reset_state(gr_engine *e) {
     const int nv = std::max(1, e->nvol), ne = std::max(1, e->nexpr);
     CK(cudaMemsetAsync(S.volc.p, 0, N * nv * 4, e->cs));
     CK(cudaMemsetAsync(S.cmpc.p, 0, N * ne * 4, e->cs));
+    if (S.vlast.p) CK(cudaMemsetAsync(S.vlast.p, 0xff, N * sizeof(float4), e->cs));   // step index -1
     init_counts_kernel<<<1, 1, 0, e->cs>>>(e->d_counts.p, (int32_t)n);
     const int threads = 256;
     seed_kernel<<<grid_for(n, threads), threads, 0, e->cs>>>(e->seeds.p, n, e->dim, S.px.p, S.py.p, S.pz.p,
@@ -1146,6 +1153,8 @@ int run_prepare(gr_engine *e, RunPlan &R, bool graph) {
 
     R.rec_before.assign((size_t)R.nsteps + 1, 1);
     for (int64_t k = 0; k < R.nsteps; ++k) R.rec_before[k + 1] = R.rec_before[k] + (R.sched.steps[k].save ? 1 : 0);
+    R.save_next.assign((size_t)R.nsteps + 1, R.nsteps);
+    for (int64_t k = R.nsteps - 1; k >= 0; --k) R.save_next[k] = R.sched.steps[k].save ? k : R.save_next[k + 1];
     R.spl = s.steps_per_launch > 0 ? s.steps_per_launch : (int64_t)1 << 40;
     if (e->compacting && s.steps_per_launch <= 0 && R.nwin > 0)
         R.spl = std::max<int64_t>(1, R.sched.window_begin[1] - R.sched.window_begin[0]);   // one window per launch
@@ -1176,6 +1185,7 @@ StateView view_of(gr_engine::State &S, int64_t stride) {
     v.px = S.px.p; v.py = S.py.p; v.pz = S.pz.p; v.qx = S.qx.p; v.qy = S.qy.p; v.qz = S.qz.p;
     v.kx = S.kx.p; v.ky = S.ky.p; v.kz = S.kz.p; v.lx = S.lx.p; v.ly = S.ly.p; v.lz = S.lz.p;
     v.length = S.length.p; v.tc = S.tc.p; v.curv = S.curv.p; v.volc = S.volc.p; v.cmpc = S.cmpc.p;
+    v.vlast = S.vlast.p;
     v.status = S.status.p; v.id = S.id.p; v.retire = S.retire.p; v.life = S.life.p; v.birth = nullptr;
     v.stride = stride;
     return v;
@@ -1202,7 +1212,7 @@ KParams make_params(gr_engine *e) {
     P.kx = S.kx.p; P.ky = S.ky.p; P.kz = S.kz.p;
     P.lx = S.lx.p; P.ly = S.ly.p; P.lz = S.lz.p;
     P.status = S.status.p; P.length = S.length.p; P.tc = S.tc.p; P.curv = S.curv.p;
-    P.volc = S.volc.p; P.cmpc = S.cmpc.p; P.id = S.id.p; P.life = e->has_life ? S.life.p : nullptr;
+    P.volc = S.volc.p; P.cmpc = S.cmpc.p; P.vlast = S.vlast.p; P.vrec = e->vrec.p; P.id = S.id.p; P.life = e->has_life ? S.life.p : nullptr;
     P.n = e->n; P.n_state = e->n; P.n_total = e->n;
     P.n_dev = e->compacting ? e->d_counts.p : nullptr;
     P.hpos = e->hpos.p; P.hcurv = e->hcurv.p; P.hvol = e->hvol.p; P.hcmp = e->hcmp.p;
@@ -1309,10 +1319,10 @@ __global__ void finalize_retired_kernel(StateView R, const int32_t *n_ret, int a
 
 using KernelFn = void (*)(const KParams);
 
-KernelFn pick_kernel(const gr_engine *e, const KParams &P) {
+KernelFn pick_kernel(const gr_engine *e, const KParams &P, bool defer) {
     const bool rk4 = e->s.integrator == 1;
     const int st = e->s.storage;
-    const int ft = kernel_features(P, e->use_pair);
+    const int ft = kernel_features(P, e->use_pair, defer);
     return st == GR_STORE_BF16 ? advance_bf16(e->dim, rk4, e->use_pair, ft)
          : st == GR_STORE_F16 ? advance_f16(e->dim, rk4, e->use_pair, ft) : advance_f32(e->dim, rk4, e->use_pair, ft);
 }
@@ -1420,6 +1430,8 @@ struct RunCtx {
     int64_t since_sort = 0;    // launches since the last compaction
     int64_t alive_known = -1;  // particles alive before the next step (-1: all of them)
     unsigned long long ps_known = 0;   // particle-steps counted before the next launch
+    bool defer = false;        // volume / expression values by deferred_extras_kernel after each
+                               // launch (at most one save step per launch)
 };
 
 int make_ctx(gr_engine *e, RunPlan &R, RunCtx &r) {
@@ -1427,7 +1439,10 @@ int make_ctx(gr_engine *e, RunPlan &R, RunCtx &r) {
     r.e = e;
     r.R = &R;
     r.P = make_params(e);
-    r.fn = pick_kernel(e, r.P);
+    // deferred volume / expression values: not in graph runs (fixed launch shapes) and only
+    // where a lean variant applies
+    r.defer = !R.graph && r.P.vlast != nullptr && (kernel_features(r.P, e->use_pair, true) & FT_DEFER) != 0;
+    r.fn = pick_kernel(e, r.P, r.defer);
     r.threads = block_size_for(e);
     // some step kernels are built for smaller blocks (their launch bounds)
     cudaFuncAttributes fa{};
@@ -1478,6 +1493,24 @@ int launch_steps(RunCtx &r, int64_t s0, int64_t s1, int64_t window) {
     return GR_OK;
 }
 
+// Volume / expression values of a FT_DEFER run (deferred_extras_kernel): save_step >= 0 after
+// the launch that ran that save step (the record's rows); else the slots with pending inputs,
+// all of them or (all = false) those that retire at the compaction after step k_end.
+int launch_deferred_extras(RunCtx &r, int64_t save_step, int64_t k_end, bool all) {
+    gr_engine *e = r.e;
+    const RunPlan &R = *r.R;
+    const int32_t rec = save_step >= 0 ? R.rec_before[save_step] : -1;
+    const int threads = 256;
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((r.P.n + threads - 1) / threads, 148 * 8));
+    if (e->dim == 3)
+        deferred_extras_kernel<3><<<(unsigned)blocks, threads, 0, e->cs>>>(r.P, rec, rec - 1, (int32_t)k_end, all);
+    else
+        deferred_extras_kernel<2><<<(unsigned)blocks, threads, 0, e->cs>>>(r.P, rec, rec - 1, (int32_t)k_end, all);
+    CK(cudaGetLastError());
+    e->stats.aux_launches++;
+    return GR_OK;
+}
+
 // After a launch that ended before step k_end: maybe retire / re-sort (compact.cuh).
 int after_launch(RunCtx &r, int64_t k_end) {
     gr_engine *e = r.e;
@@ -1485,6 +1518,10 @@ int after_launch(RunCtx &r, int64_t k_end) {
     if (!e->compacting || k_end >= R.nsteps) return 0;
     if (++r.since_sort < e->s.sort_interval) return 0;
     r.since_sort = 0;
+    if (r.defer) {   // retiring particles take their final values along
+        const int q = launch_deferred_extras(r, -1, k_end, false);
+        if (q) return q;
+    }
     int q = compact_pass(e, R.rec_before[k_end], (int32_t)k_end, R.graph);
     if (q) return q;
     const int32_t gs = r.P.grid_stride;
@@ -1560,8 +1597,14 @@ int launch_range(RunCtx &r, int64_t b, int64_t t) {
         int64_t k1 = std::min(t, k + R.spl);
         const int64_t w = R.sched.steps[k].window;
         if (e->use_pair) k1 = std::min(k1, R.sched.window_begin[w + 1]);   // one window per launch
+        if (r.defer && R.save_next[k] < R.nsteps)
+            k1 = std::min(k1, R.save_next[R.save_next[k] + 1]);            // and one save step
         int q = launch_steps(r, k, k1, w);
         if (q) return q;
+        if (r.defer && R.save_next[k] < k1) {
+            q = launch_deferred_extras(r, R.save_next[k], 0, false);
+            if (q) return q;
+        }
         q = after_launch(r, k1);
         if (q) return q;
         k = k1;
@@ -1765,6 +1808,10 @@ int run_tail(RunCtx &r, RecordCounts &c) {
     const int64_t executed = r.executed;
     c = count_records(R, executed);
     KParams P = r.P;
+    if (r.defer) {   // pending volume / expression values into the state arrays
+        const int q = launch_deferred_extras(r, -1, executed, true);
+        if (q) return q;
+    }
     if (s.save_interval == 0) {
         const bool tpos = executed > 0;   // data.Time > 0 after at least one step
         if (e->dim == 3)

@@ -32,9 +32,11 @@ constexpr int GR_MAX_CON = 4;
 // no uplift, length abort, topography, sphere coordinates, loop borders, per-step alive counts
 // or 1/256 filter weights, and curvature Off or Total; FT_CURV / FT_EXTRAS say whether it keeps total curvature and volume
 // / expression values, FT_COMP Kahan-compensated positions (instantiated without extras: the
-// precision form).  The lean variants drop the dead state from registers; their arithmetic is the generic
-// variant's.
-constexpr int FT_GENERIC = 0, FT_LEAN = 1, FT_CURV = 2, FT_EXTRAS = 4, FT_COMP = 8;
+// precision form).  FT_DEFER (with FT_LEAN, instead of FT_EXTRAS) leaves the volume / expression
+// values to deferred_extras_kernel after the launch: the step kernel only stores each moved step's
+// stage-averaged velocity and step index, and hands them to the record at a save step.  The lean
+// variants drop the dead state from registers; their arithmetic is the generic variant's.
+constexpr int FT_GENERIC = 0, FT_LEAN = 1, FT_CURV = 2, FT_EXTRAS = 4, FT_COMP = 8, FT_DEFER = 16;
 
 // Step-schedule flags.
 constexpr int SF_SAVE = 1;       // position / info record after this step
@@ -76,6 +78,10 @@ struct KParams {
     float *length, *tc, *curv;
     float *volc;                  // [8][n_state]
     float *cmpc;                  // [4][n_state]
+    float4 *vlast;                // FT_DEFER: (stage-averaged velocity, step index as int bits) of
+                                  // each slot's last moved step; index -1: no step since the values
+                                  // were last evaluated (or handed to a record)
+    float4 *vrec;                 // FT_DEFER: vlast as of the launch's save step, for its record
     const int32_t *id;            // original particle index
     int64_t n;                    // particles in this launch (prefix of the state arrays)
     const int32_t *n_dev;         // if set: live prefix length on the device (<= n)
@@ -714,6 +720,39 @@ __device__ __noinline__ void record_extras(const KParams &P, int64_t i, int64_t 
         if (e < P.nexpr) P.hcmp[((int64_t)e * P.Li + irec) * P.n_total + pid] = cmp[e];
 }
 
+// Volume / expression values after a FT_DEFER step launch (tpp:363-435), from the inputs of a
+// slot's last moved step: its position (a particle keeps it once it stops), the stored
+// velocity and that step's schedule entry.  Same values as the in-kernel evaluation.
+//  - rec >= 0: the launch saved record rec (info record irec) at one step: every slot of the live
+//    prefix writes the record's rows, evaluating first if it moved since its last evaluation
+//    (inputs in vrec, position in the record's row).
+//  - rec < 0: slots with pending inputs (vlast) are evaluated into the state arrays: all of them
+//    (all = 1, the end of a run) or those about to retire (aborted, or lifetime over by k_end).
+template <int DIM>
+__global__ void __launch_bounds__(256) deferred_extras_kernel(const __grid_constant__ KParams P, int32_t rec,
+                                                              int32_t irec, int32_t k_end, int32_t all) {
+    const int64_t n = P.n_dev ? (int64_t)*P.n_dev : P.n;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pid = P.id[i];
+        const float cv = P.curvature_mode == 3 ? P.curv[i] : 0.f;
+        if (rec >= 0) {
+            const float4 v = P.vrec[i];
+            const int32_t last_s = __float_as_int(v.w);
+            const float *hp = P.hpos + ((int64_t)rec * P.n_total + pid) * DIM;
+            const V3 p{hp[0], hp[1], DIM == 3 ? hp[2] : 0.f};
+            record_extras<DIM>(P, i, pid, last_s >= 0, last_s < 0 ? 0 : last_s, p, V3{v.x, v.y, v.z}, cv, irec);
+        } else {
+            const float4 v = P.vlast[i];
+            const int32_t last_s = __float_as_int(v.w);
+            if (last_s < 0) continue;
+            if (!all && P.status[i] == 0 && !(P.life && P.life[i] <= k_end)) continue;
+            const V3 p{P.px[i], P.py[i], DIM == 3 ? P.pz[i] : 0.f};
+            record_extras<DIM>(P, i, pid, true, last_s, p, V3{v.x, v.y, v.z}, cv, -1);
+            reinterpret_cast<int32_t *>(P.vlast + i)[3] = -1;
+        }
+    }
+}
+
 #ifndef GR_ADV_MIN_BLOCKS
 #define GR_ADV_MIN_BLOCKS 2
 #endif
@@ -957,7 +996,10 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
                     seg = nseg;
                 }
 
-                // volumes and expressions are evaluated lazily (eval_extras)
+                // volumes and expressions are evaluated lazily (eval_extras), or after the launch
+                // from the stored inputs (FT_DEFER, deferred_extras_kernel)
+                if constexpr ((FT & FT_DEFER) != 0)
+                    P.vlast[i] = make_float4(vc.x, vc.y, DIM == 3 ? vc.z : 0.f, __int_as_float(s));
                 vc_last = vc;
                 last_s = s;
                 dirty = true;
@@ -973,6 +1015,12 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
             hp[0] = p.x; hp[1] = p.y;
             if (DIM == 3) hp[2] = p.z;
             if (curvature_mode == 3 && (E.flags & SF_CURV_REC)) P.hcurv[(int64_t)E.crec * P.n_total + pid] = cv;
+            if constexpr ((FT & FT_DEFER) != 0) {
+                // the record's inputs: the last moved step's (if any since the last evaluation)
+                const float4 v = P.vlast[i];
+                P.vrec[i] = v;
+                if (__float_as_int(v.w) >= 0) reinterpret_cast<int32_t *>(P.vlast + i)[3] = -1;
+            }
             if (extras) {
                 record_extras<DIM>(P, i, pid, dirty, last_s, p, vc_last, cv, E.irec);
                 dirty = false;

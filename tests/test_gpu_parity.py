@@ -283,8 +283,11 @@ def test_launch_shape_does_not_change_results(extra):
     particles change nothing: every output stays bit-identical to the float32 oracle."""
     base, wind, seeds = problem3d(seed=2)
     vols = [{"temp": np.random.default_rng(4).standard_normal((12, 20, 24)).astype(np.float32)} for _ in wind]
+    # the lean variants defer volume / expression values to a kernel after each launch (records
+    # every 3 steps: several per window, launches split to one save step each)
     for extra_settings, exprs in ((dict(CurvatureMode=3, SaveInterval=2), ["x + cv*2", "temp - z"]),
-                                  (dict(CurvatureMode=1, SaveInterval=0), ["x*2", "temp - z"])):
+                                  (dict(CurvatureMode=1, SaveInterval=0), ["x*2", "temp - z"]),
+                                  (dict(CurvatureMode=1, SaveInterval=3), ["x*2", "temp - z + u*v"])):
         settings = dict(base, AdditionalVolumeMode=1, AdditionalCompute=exprs, **extra_settings)
         ref = H.run_oracle(settings, wind, seeds, volumes=vols, precision="f32")
         eng = H.run_engine(settings, wind, seeds, volumes=vols, **extra)
