@@ -866,7 +866,7 @@ int alloc_state(gr_engine *e) {
     const size_t N = (size_t)e->n;
     int rc = alloc_set(e, e->st[0], false);
     if (rc) return rc;
-    if (e->st[0].vlast.p) CK(e->vrec.alloc(N));
+    if (e->st[0].vlast.p) CK(e->vrec.alloc(2 * N));
     CK(e->out_status.alloc(N)); CK(e->out_length.alloc(N)); CK(e->out_tc.alloc(N));
     e->compacting = e->s.sort_interval > 0;
     CK(e->d_counts.alloc(4));
@@ -1500,12 +1500,27 @@ int launch_deferred_extras(RunCtx &r, int64_t save_step, int64_t k_end, bool all
     gr_engine *e = r.e;
     const RunPlan &R = *r.R;
     const int32_t rec = save_step >= 0 ? R.rec_before[save_step] : -1;
+    // the expression programs travel in the kernel's parameters when they fit
+    ExprSet X;
+    std::memset(&X, 0, sizeof X);
+    int32_t total = 0;
+    for (int k = 0; k < e->nexpr; ++k) total += e->progs[k].len;
+    if (total <= GR_EXPR_PARAM_CODE) {
+        X.in_params = 1;
+        int32_t at = 0;
+        for (int k = 0; k < e->nexpr; ++k) {
+            X.start[k] = at;
+            X.len[k] = e->progs[k].len;
+            std::memcpy(X.code + at, e->progs[k].code, sizeof(Instr) * (size_t)e->progs[k].len);
+            at += e->progs[k].len;
+        }
+    }
     const int threads = 256;
     const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((r.P.n + threads - 1) / threads, 148 * 8));
     if (e->dim == 3)
-        deferred_extras_kernel<3><<<(unsigned)blocks, threads, 0, e->cs>>>(r.P, rec, rec - 1, (int32_t)k_end, all);
+        deferred_extras_kernel<3><<<(unsigned)blocks, threads, 0, e->cs>>>(r.P, X, rec, rec - 1, (int32_t)k_end, all);
     else
-        deferred_extras_kernel<2><<<(unsigned)blocks, threads, 0, e->cs>>>(r.P, rec, rec - 1, (int32_t)k_end, all);
+        deferred_extras_kernel<2><<<(unsigned)blocks, threads, 0, e->cs>>>(r.P, X, rec, rec - 1, (int32_t)k_end, all);
     CK(cudaGetLastError());
     e->stats.aux_launches++;
     return GR_OK;
@@ -1602,7 +1617,7 @@ int launch_range(RunCtx &r, int64_t b, int64_t t) {
         int q = launch_steps(r, k, k1, w);
         if (q) return q;
         if (r.defer && R.save_next[k] < k1) {
-            q = launch_deferred_extras(r, R.save_next[k], 0, false);
+            q = launch_deferred_extras(r, R.save_next[k], k1, false);
             if (q) return q;
         }
         q = after_launch(r, k1);

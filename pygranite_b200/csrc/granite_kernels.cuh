@@ -81,7 +81,8 @@ struct KParams {
     float4 *vlast;                // FT_DEFER: (stage-averaged velocity, step index as int bits) of
                                   // each slot's last moved step; index -1: no step since the values
                                   // were last evaluated (or handed to a record)
-    float4 *vrec;                 // FT_DEFER: vlast as of the launch's save step, for its record
+    float4 *vrec;                 // FT_DEFER: [2 i] position, [2 i + 1] vlast as of the launch's
+                                  // save step, for its record
     const int32_t *id;            // original particle index
     int64_t n;                    // particles in this launch (prefix of the state arrays)
     const int32_t *n_dev;         // if set: live prefix length on the device (<= n)
@@ -564,13 +565,37 @@ __device__ __forceinline__ float ref_at(const float (&ref)[19], int i) {
     }
 }
 
+// Expression programs in kernel parameter space (deferred_extras_kernel): read through the
+// constant cache at a warp-uniform index, so the dispatch below branches on uniform values and
+// no global load sits on the evaluation's critical path.  Programs longer in total than
+// GR_EXPR_PARAM_CODE are read from global memory (KParams::prog) instead.
+constexpr int GR_EXPR_PARAM_CODE = 512;
+struct ExprSet {
+    int32_t in_params;                 // 1: code[] holds the programs
+    int32_t start[GR_MAX_EXPR], len[GR_MAX_EXPR];
+    Instr code[GR_EXPR_PARAM_CODE];
+};
+
+// Program sources of eval_program: expression e's length and instruction k.
+struct GlobalCode {
+    const Program *prog;
+    __device__ __forceinline__ int len(int e) const { return prog[e].len; }
+    __device__ __forceinline__ Instr at(int e, int k) const { return prog[e].code[k]; }
+};
+struct ParamCode {
+    const ExprSet &X;
+    __device__ __forceinline__ int len(int e) const { return X.len[e]; }
+    __device__ __forceinline__ Instr at(int e, int k) const { return X.code[X.start[e] + k]; }
+};
+
 // Postfix evaluation with an 8-register rotating stack (s0 = top); the program is uniform
 // across the grid, so every branch here is uniform.
-__device__ __forceinline__ float eval_program(const Program *prog, const float (&ref)[19]) {
+template <typename Code>
+__device__ __forceinline__ float eval_program(const Code &code, int e, const float (&ref)[19]) {
     float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f, s4 = 0.f, s5 = 0.f, s6 = 0.f, s7 = 0.f;
-    const int len = prog->len;
+    const int len = code.len(e);
     for (int k = 0; k < len; ++k) {
-        const Instr in = prog->code[k];
+        const Instr in = code.at(e, k);
         float r;
         bool binary = false, push = false;
         switch (in.op) {
@@ -611,9 +636,9 @@ __device__ __forceinline__ float eval_program(const Program *prog, const float (
 // and the step's time weight / ring slots (tpp:363-447).  The kernel calls this only when the
 // values become observable (a record, the end of a launch), which gives the same values as
 // evaluating after every alive step, as the reference does.
-template <int DIM>
-__device__ __forceinline__ void eval_extras(const KParams &P, const StepEntry &E, int64_t pid, const V3 &p,
-                                            const V3 &vc, float cv, float (&vol)[GR_MAX_VOL],
+template <int DIM, typename Code>
+__device__ __forceinline__ void eval_extras(const KParams &P, const Code &code, const StepEntry &E, int64_t pid,
+                                            const V3 &p, const V3 &vc, float cv, float (&vol)[GR_MAX_VOL],
                                             float (&cmp)[GR_MAX_EXPR]) {
     const float t0 = P.dyn_any ? E.t0 : 0.f;
     if (P.volume_mode != 0 && P.nvol > 0) {
@@ -667,7 +692,7 @@ __device__ __forceinline__ void eval_extras(const KParams &P, const StepEntry &E
         ref[16] = vc.x; ref[17] = vc.y; ref[18] = DIM == 3 ? vc.z : 0.f;
 #pragma unroll
         for (int e = 0; e < GR_MAX_EXPR; ++e)
-            if (e < P.nexpr) cmp[e] = eval_program(P.prog + e, ref);
+            if (e < P.nexpr) cmp[e] = eval_program(code, e, ref);
     }
 }
 
@@ -697,16 +722,14 @@ __device__ __forceinline__ void store_extras(const KParams &P, int64_t i, const 
 
 // Volume / expression values at a record or at the end of a launch (tpp:363-435): evaluated if
 // an alive step has passed since the last evaluation (`dirty`, then kept in the state arrays),
-// else the state arrays' values; written to the record's rows when irec >= 0.  Not inlined: it
-// runs once per record, and its register peak (the expression stack, the volume samples) then
-// stays out of the step loop's allocation; the caller's live registers are saved around the call.
-template <int DIM>
-__device__ __noinline__ void record_extras(const KParams &P, int64_t i, int64_t pid, bool dirty, int last_s,
-                                           V3 p, V3 vc_last, float cv, int32_t irec) {
+// else the state arrays' values; written to the record's rows when irec >= 0.
+template <int DIM, typename Code>
+__device__ __forceinline__ void extras_at(const KParams &P, const Code &code, int64_t i, int64_t pid, bool dirty,
+                                          int last_s, const V3 &p, const V3 &vc_last, float cv, int32_t irec) {
     float vol[GR_MAX_VOL], cmp[GR_MAX_EXPR];
     load_extras(P, i, dirty, vol, cmp);
     if (dirty) {
-        eval_extras<DIM>(P, P.sched[last_s], pid, p, vc_last, cv, vol, cmp);
+        eval_extras<DIM>(P, code, P.sched[last_s], pid, p, vc_last, cv, vol, cmp);
         store_extras(P, i, vol, cmp);
     }
     if (irec < 0) return;
@@ -720,37 +743,59 @@ __device__ __noinline__ void record_extras(const KParams &P, int64_t i, int64_t 
         if (e < P.nexpr) P.hcmp[((int64_t)e * P.Li + irec) * P.n_total + pid] = cmp[e];
 }
 
+// extras_at for the step kernel's in-kernel evaluation (FT_EXTRAS).  Not inlined: it runs once
+// per record, and its register peak (the expression stack, the volume samples) then stays out
+// of the step loop's allocation; the caller's live registers are saved around the call.
+template <int DIM>
+__device__ __noinline__ void record_extras(const KParams &P, int64_t i, int64_t pid, bool dirty, int last_s,
+                                           V3 p, V3 vc_last, float cv, int32_t irec) {
+    extras_at<DIM>(P, GlobalCode{P.prog}, i, pid, dirty, last_s, p, vc_last, cv, irec);
+}
+
 // Volume / expression values after a FT_DEFER step launch (tpp:363-435), from the inputs of a
 // slot's last moved step: its position (a particle keeps it once it stops), the stored
 // velocity and that step's schedule entry.  Same values as the in-kernel evaluation.
 //  - rec >= 0: the launch saved record rec (info record irec) at one step: every slot of the live
 //    prefix writes the record's rows, evaluating first if it moved since its last evaluation
-//    (inputs in vrec, position in the record's row).
+//    (inputs and position in vrec, as of the save step).
 //  - rec < 0: slots with pending inputs (vlast) are evaluated into the state arrays: all of them
-//    (all = 1, the end of a run) or those about to retire (aborted, or lifetime over by k_end).
-template <int DIM>
-__global__ void __launch_bounds__(256) deferred_extras_kernel(const __grid_constant__ KParams P, int32_t rec,
-                                                              int32_t irec, int32_t k_end, int32_t all) {
+//    (all = 1, the end of a run) or those about to retire (aborted, or lifetime over by k_end),
+//    whose values are final.  (Folding this pass into the record kernel measured slower: the
+//    second evaluation path doubles the kernel's code.)
+template <int DIM, typename Code>
+__device__ __forceinline__ void deferred_extras(const KParams &P, const Code &code, int32_t rec, int32_t irec,
+                                                int32_t k_end, int32_t all) {
     const int64_t n = P.n_dev ? (int64_t)*P.n_dev : P.n;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t pid = P.id[i];
-        const float cv = P.curvature_mode == 3 ? P.curv[i] : 0.f;
         if (rec >= 0) {
-            const float4 v = P.vrec[i];
+            const int64_t pid = P.id[i];
+            const float cv = P.curvature_mode == 3 ? P.curv[i] : 0.f;
+            const float4 a = P.vrec[2 * i], v = P.vrec[2 * i + 1];
             const int32_t last_s = __float_as_int(v.w);
-            const float *hp = P.hpos + ((int64_t)rec * P.n_total + pid) * DIM;
-            const V3 p{hp[0], hp[1], DIM == 3 ? hp[2] : 0.f};
-            record_extras<DIM>(P, i, pid, last_s >= 0, last_s < 0 ? 0 : last_s, p, V3{v.x, v.y, v.z}, cv, irec);
+            extras_at<DIM>(P, code, i, pid, last_s >= 0, last_s < 0 ? 0 : last_s, V3{a.x, a.y, a.z},
+                           V3{v.x, v.y, v.z}, cv, irec);
         } else {
+            if (!all && P.status[i] == 0 && !(P.life && P.life[i] <= k_end)) continue;
             const float4 v = P.vlast[i];
             const int32_t last_s = __float_as_int(v.w);
             if (last_s < 0) continue;
-            if (!all && P.status[i] == 0 && !(P.life && P.life[i] <= k_end)) continue;
+            const int64_t pid = P.id[i];
+            const float cv = P.curvature_mode == 3 ? P.curv[i] : 0.f;
             const V3 p{P.px[i], P.py[i], DIM == 3 ? P.pz[i] : 0.f};
-            record_extras<DIM>(P, i, pid, true, last_s, p, V3{v.x, v.y, v.z}, cv, -1);
+            extras_at<DIM>(P, code, i, pid, true, last_s, p, V3{v.x, v.y, v.z}, cv, -1);
             reinterpret_cast<int32_t *>(P.vlast + i)[3] = -1;
         }
     }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) deferred_extras_kernel(const __grid_constant__ KParams P,
+                                                              const __grid_constant__ ExprSet X, int32_t rec,
+                                                              int32_t irec, int32_t k_end, int32_t all) {
+    if (X.in_params)
+        deferred_extras<DIM>(P, ParamCode{X}, rec, irec, k_end, all);
+    else
+        deferred_extras<DIM>(P, GlobalCode{P.prog}, rec, irec, k_end, all);
 }
 
 #ifndef GR_ADV_MIN_BLOCKS
@@ -1016,9 +1061,11 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
             if (DIM == 3) hp[2] = p.z;
             if (curvature_mode == 3 && (E.flags & SF_CURV_REC)) P.hcurv[(int64_t)E.crec * P.n_total + pid] = cv;
             if constexpr ((FT & FT_DEFER) != 0) {
-                // the record's inputs: the last moved step's (if any since the last evaluation)
+                // the record's inputs: the position and the last moved step's (if any since the
+                // last evaluation)
                 const float4 v = P.vlast[i];
-                P.vrec[i] = v;
+                P.vrec[2 * i] = make_float4(p.x, p.y, DIM == 3 ? p.z : 0.f, 0.f);
+                P.vrec[2 * i + 1] = v;
                 if (__float_as_int(v.w) >= 0) reinterpret_cast<int32_t *>(P.vlast + i)[3] = -1;
             }
             if (extras) {
