@@ -123,6 +123,7 @@ typedef struct gr_stats {
     int64_t particle_steps;
     int64_t h2d_bytes;
     int64_t d2h_bytes;
+    int64_t jit_launches;        /* deferred volume / expression launches of run-time compiled code */
 } gr_stats;
 
 /* Step plan of a run whose loader never runs dry: counts and, if the arrays are non-null,

@@ -64,7 +64,7 @@ class ResultInfo(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("kernel_ms", ctypes.c_double), ("run_ms", ctypes.c_double), ("launches", ctypes.c_int64),
                 ("aux_launches", ctypes.c_int64), ("particle_steps", ctypes.c_int64),
-                ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64)]
+                ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64), ("jit_launches", ctypes.c_int64)]
 
 
 class PlanInfo(ctypes.Structure):

@@ -31,6 +31,7 @@
 #include "compact.cuh"
 #include "engine_graph.h"
 #include "granite_kernels.cuh"
+#include "jit.h"
 #include "schedule.h"
 
 using namespace granite_b200;
@@ -245,6 +246,8 @@ struct gr_engine {
     State ret;                         // retired particles (frozen state)
     State ck;                          // MinimumAliveParticles: state before the current launch
     DevBuf<float4> vrec;               // inputs of a record's deferred volume / expression values
+    cudaKernel_t jit_extras = nullptr; // run-time compiled deferred kernel of the expressions (jit.cu)
+    std::string jit_why;               // why there is none
     DevBuf<unsigned> alive_at;         // per-step alive counts of a launch, 32 shards per step
     std::vector<unsigned> h_alive;
     int cur = 0;
@@ -1442,6 +1445,8 @@ int make_ctx(gr_engine *e, RunPlan &R, RunCtx &r) {
     // deferred volume / expression values: not in graph runs (fixed launch shapes) and only
     // where a lean variant applies
     r.defer = !R.graph && r.P.vlast != nullptr && (kernel_features(r.P, e->use_pair, true) & FT_DEFER) != 0;
+    if (r.defer && e->nexpr > 0 && !e->jit_extras)
+        e->jit_extras = jit_deferred_kernel(e->progs, e->nexpr, e->dim, e->jit_why);
     r.fn = pick_kernel(e, r.P, r.defer);
     r.threads = block_size_for(e);
     // some step kernels are built for smaller blocks (their launch bounds)
@@ -1517,6 +1522,16 @@ int launch_deferred_extras(RunCtx &r, int64_t save_step, int64_t k_end, bool all
     }
     const int threads = 256;
     const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((r.P.n + threads - 1) / threads, 148 * 8));
+    if (e->jit_extras) {
+        KParams P = r.P;
+        int32_t a_rec = rec, a_irec = rec - 1, a_k = (int32_t)k_end, a_all = all ? 1 : 0;
+        void *args[] = {&P, &a_rec, &a_irec, &a_k, &a_all};
+        CK(cudaLaunchKernel(reinterpret_cast<const void *>(e->jit_extras), dim3((unsigned)blocks), dim3(threads), args, 0,
+                            e->cs));
+        e->stats.aux_launches++;
+        e->stats.jit_launches++;
+        return GR_OK;
+    }
     if (e->dim == 3)
         deferred_extras_kernel<3><<<(unsigned)blocks, threads, 0, e->cs>>>(r.P, X, rec, rec - 1, (int32_t)k_end, all);
     else

@@ -7,9 +7,11 @@
 // stack at most GR_EXPR_MAX_STACK deep, so the device keeps the whole stack in registers.
 #pragma once
 
+#ifndef __CUDACC_RTC__
 #include <cstdint>
 #include <string>
 #include <vector>
+#endif
 
 namespace granite_b200 {
 
@@ -43,6 +45,7 @@ struct Program {
     Instr code[GR_EXPR_MAX_CODE];
 };
 
+#ifndef __CUDACC_RTC__
 // Compiles `code`.  volume_names[k] -> f_k, constant_names[k] -> c_k.  On failure returns
 // false and sets `error` to the reference's message ("ERROR < USER INPUT | ... >").
 bool compile_expression(const std::string &code, const std::vector<std::string> &volume_names,
@@ -51,5 +54,6 @@ bool compile_expression(const std::string &code, const std::vector<std::string> 
 
 // Host evaluation of a compiled program (used by the engine's self-check and tests).
 float evaluate(const Program &p, const float *ref);
+#endif
 
 }  // namespace granite_b200

@@ -16,8 +16,24 @@
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#ifdef __CUDACC_RTC__
+// run-time compilation of the deferred volume / expression kernel (jit.cu): no host headers
+typedef signed char int8_t;
+typedef short int16_t;
+typedef int int32_t;
+typedef long long int64_t;
+typedef unsigned char uint8_t;
+typedef unsigned short uint16_t;
+typedef unsigned int uint32_t;
+typedef unsigned long long uint64_t;
+namespace std {
+template <class A, class B> struct is_same { static constexpr bool value = false; };
+template <class A> struct is_same<A, A> { static constexpr bool value = true; };
+}  // namespace std
+#else
 #include <cstdint>
 #include <type_traits>
+#endif
 
 #include "expr.h"
 
@@ -295,9 +311,11 @@ struct SampleCache {
 // fraction is 0 with the weighted-away corner finite, so the interpolation is +0 either way.
 // Padded node count of a window-pair buffer: (nx + 3) (ny + 3) (nz + 3) in 3D, (nx + 3) (ny + 3)
 // in 2D.
+#ifndef __CUDACC_RTC__
 inline int64_t padded_pair_nodes(int dim, int64_t nx, int64_t ny, int64_t nz) {
     return (nx + 3) * (ny + 3) * (dim == 3 ? nz + 3 : 1);
 }
+#endif
 
 struct PCell {
     int32_t base;        // padded node index of corner (ix, iy, iz)
@@ -576,16 +594,19 @@ struct ExprSet {
     Instr code[GR_EXPR_PARAM_CODE];
 };
 
-// Program sources of eval_program: expression e's length and instruction k.
+// Program sources of eval_program: expression e's length and instruction k; eval(e, ref) is the
+// value of expression e (the interpreter here, straight-line code in a run-time compiled JitCode).
 struct GlobalCode {
     const Program *prog;
     __device__ __forceinline__ int len(int e) const { return prog[e].len; }
     __device__ __forceinline__ Instr at(int e, int k) const { return prog[e].code[k]; }
+    __device__ __forceinline__ float eval(int e, const float (&ref)[19]) const;
 };
 struct ParamCode {
     const ExprSet &X;
     __device__ __forceinline__ int len(int e) const { return X.len[e]; }
     __device__ __forceinline__ Instr at(int e, int k) const { return X.code[X.start[e] + k]; }
+    __device__ __forceinline__ float eval(int e, const float (&ref)[19]) const;
 };
 
 // Postfix evaluation with an 8-register rotating stack (s0 = top); the program is uniform
@@ -630,6 +651,9 @@ __device__ __forceinline__ float eval_program(const Code &code, int e, const flo
     }
     return s0;
 }
+
+__device__ __forceinline__ float GlobalCode::eval(int e, const float (&ref)[19]) const { return eval_program(*this, e, ref); }
+__device__ __forceinline__ float ParamCode::eval(int e, const float (&ref)[19]) const { return eval_program(*this, e, ref); }
 
 // Volume samples and expression values of a particle, evaluated from the inputs of its last
 // alive step: position p (that step's new position), stage-averaged velocity vc, curvature cv
@@ -692,7 +716,7 @@ __device__ __forceinline__ void eval_extras(const KParams &P, const Code &code, 
         ref[16] = vc.x; ref[17] = vc.y; ref[18] = DIM == 3 ? vc.z : 0.f;
 #pragma unroll
         for (int e = 0; e < GR_MAX_EXPR; ++e)
-            if (e < P.nexpr) cmp[e] = eval_program(code, e, ref);
+            if (e < P.nexpr) cmp[e] = code.eval(e, ref);
     }
 }
 

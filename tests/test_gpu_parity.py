@@ -430,3 +430,36 @@ def test_edge_cases_bitexact(name, space):
     eng = H.run_engine(settings, wind, seeds)
     ref = H.run_oracle(settings, wind, seeds, precision="f32")
     H.assert_same(eng, ref)
+
+
+def test_compiled_expressions_equal_the_interpreter_and_the_oracle(monkeypatch):
+    """The lean kernels defer volume / expression values to a kernel after each launch, whose
+    expressions are compiled to straight-line code at run time (jit.cu); with GR_JIT=0 the
+    bytecode interpreter evaluates them instead.  Both give the float32 oracle's values; the
+    transcendental cases within the ulps of the interpreter test above."""
+    from pygranite_b200 import capi
+    base, wind, seeds = problem3d(seed=11)
+    temp = [np.random.default_rng(12 + k).standard_normal((12, 20, 24)).astype(np.float32) for k in range(len(wind))]
+    exprs = ["sqrt(u*u+v*v)*temp", "temp - z/3 + x*y - 1.25", "(u - v)/(w + 4) * -2"]
+    settings = dict(base, CurvatureMode=1, AdditionalVolumeMode=2, SaveInterval=3, AdditionalCompute=exprs)
+    ref = H.run_oracle(settings, wind, seeds, volumes=[{"temp": t} for t in temp], precision="f32")
+    runs = {}
+    for jit in ("1", "0"):
+        monkeypatch.setenv("GR_JIT", jit)
+        eng = capi.Engine(capi.settings_from_reference(settings, ring_slots=len(wind), sort_interval=2))
+        eng.set_seeds(seeds)
+        for k, snap in enumerate(wind):
+            eng.load_windfield(k, snap)
+            eng.load_volume(k, 0, temp[k])
+        for e, code in enumerate(exprs):
+            eng.compile_expression(e, code, ["temp"], [])
+        eng.run(lambda k: 1 if k < len(wind) else 0)
+        runs[jit] = (eng.results(), eng.stats().jit_launches)
+        eng.close()
+    assert runs["1"][1] > 0, "the run-time compiled kernel did not run"
+    assert runs["0"][1] == 0
+    for jit, (res, _) in runs.items():
+        H.assert_same(res, ref, ("trajectories", "status", "total_curvature"))
+        assert np.array_equal(res["volume_info"][0], ref["volume_info"]["temp"]), jit
+        for e in range(len(exprs)):
+            assert np.array_equal(res["compute_info"][e], ref["compute_info"][e]), (jit, e)
