@@ -1358,12 +1358,17 @@ int pack_pair(gr_engine *e, int64_t w, cudaStream_t stream) {
     const int threads = 256, blocks = grid_for(e->nodes, threads);
     if (e->dim == 3) {
         const int32_t nx = (int32_t)e->nx, ny = (int32_t)e->ny, nz = (int32_t)e->nz;
+        // beside the step launches (side stream): one block per SM; else the whole buffer at once
+        int sms = 148;
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->s.device));
+        const int b3 = stream == e->ps ? sms
+                                       : grid_for(padded_pair_nodes(3, nx, ny, nz) / PACK3_UNROLL, PACK3_THREADS);
         if (elem == 16)
-            pair_pack_padded_kernel<float><<<blocks, threads, 0, stream>>>((const float4 *)back, (const float4 *)front,
-                                                                          e->pairbuf[b].p, nx, ny, nz);
-        else
-            pair_pack_padded_kernel<uint16_t><<<blocks, threads, 0, stream>>>((const uint2 *)back, (const uint2 *)front,
+            pair_pack_padded_kernel<float><<<b3, PACK3_THREADS, 0, stream>>>((const float4 *)back, (const float4 *)front,
                                                                              e->pairbuf[b].p, nx, ny, nz);
+        else
+            pair_pack_padded_kernel<uint16_t><<<b3, PACK3_THREADS, 0, stream>>>((const uint2 *)back, (const uint2 *)front,
+                                                                                e->pairbuf[b].p, nx, ny, nz);
     } else {
         const int32_t nx = (int32_t)e->nx, ny = (int32_t)e->ny;
         if (elem == 8)
@@ -1521,7 +1526,7 @@ int launch_deferred_extras(RunCtx &r, int64_t save_step, int64_t k_end, bool all
         }
     }
     const int threads = 256;
-    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((r.P.n + threads - 1) / threads, 148 * 8));
+    const int blocks = grid_for(r.P.n, threads);
     if (e->jit_extras) {
         KParams P = r.P;
         int32_t a_rec = rec, a_irec = rec - 1, a_k = (int32_t)k_end, a_all = all ? 1 : 0;

@@ -813,7 +813,7 @@ __device__ __forceinline__ void deferred_extras(const KParams &P, const Code &co
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(256) deferred_extras_kernel(const __grid_constant__ KParams P,
+__global__ void __launch_bounds__(256, 3) deferred_extras_kernel(const __grid_constant__ KParams P,
                                                               const __grid_constant__ ExprSet X, int32_t rec,
                                                               int32_t irec, int32_t k_end, int32_t all) {
     if (X.in_params)

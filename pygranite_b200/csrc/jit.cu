@@ -185,7 +185,7 @@ std::string jit_source(const Program *progs, int nexpr, int dim) {
         src += "      }\n";
     }
     src += "      return 0.f;\n    }\n};\n}  // namespace granite_b200\n";
-    src += "extern \"C\" __global__ void __launch_bounds__(256) gr_jit_deferred_extras(\n"
+    src += "extern \"C\" __global__ void __launch_bounds__(256, 3) gr_jit_deferred_extras(\n"
            "    const __grid_constant__ granite_b200::KParams P, int rec, int irec, int k_end, int all) {\n";
     src += "    granite_b200::deferred_extras<" + std::to_string(dim) +
            ">(P, granite_b200::JitCode{}, rec, irec, k_end, all);\n}\n";

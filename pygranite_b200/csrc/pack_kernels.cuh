@@ -112,27 +112,38 @@ static __global__ void pair_pack_edge2_kernel(const typename PairNode<S>::Ring2 
 // of a (nx + 3) x (ny + 3) x (nz + 3) buffer holds the pair of ring nodes (x, y, z), or zeros
 // outside the grid (the step kernel's border addressing).  Every padded node is written, so the
 // buffer needs no clearing.  The padded node count must stay below 2^31.
+// 128-thread blocks of at most 32 registers (4 nodes in flight per thread): one block fits on an
+// SM beside the 3D float32 step kernel's five 96-register blocks, so a pack launched on a side
+// stream with one block per SM runs alongside the step launches instead of taking their slots.
+constexpr int PACK3_THREADS = 128, PACK3_UNROLL = 4;
 template <typename S>
-static __global__ void pair_pack_padded_kernel(const typename PairNode<S>::Ring3 *__restrict__ back,
-                                               const typename PairNode<S>::Ring3 *__restrict__ front, void *out,
-                                               int32_t nx, int32_t ny, int32_t nz) {
+static __global__ void __launch_bounds__(PACK3_THREADS, 16)
+    pair_pack_padded_kernel(const typename PairNode<S>::Ring3 *__restrict__ back,
+                            const typename PairNode<S>::Ring3 *__restrict__ front, void *__restrict__ out, int32_t nx,
+                            int32_t ny, int32_t nz) {
     const int32_t pnx = nx + 3, pny = ny + 3;
     const int32_t total = pnx * pny * (nz + 3);
-    for (int32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < total; o += gridDim.x * blockDim.x) {
-        const int32_t x = o % pnx - 1, r = o / pnx;
-        const int32_t y = r % pny - 1, z = r / pny - 1;
-        const bool in = (unsigned)x < (unsigned)nx && (unsigned)y < (unsigned)ny && (unsigned)z < (unsigned)nz;
-        const int64_t i = in ? ((int64_t)z * ny + y) * nx + x : 0;
-        if constexpr (std::is_same<S, float>::value) {
-            float4 *po = reinterpret_cast<float4 *>(out) + 2 * (int64_t)o;
-            if (in) {
-                PairNode<float>::pack3(back[i], front[i], po);
+    const int32_t chunk = PACK3_THREADS * PACK3_UNROLL;
+    for (int32_t o0 = blockIdx.x * chunk + threadIdx.x; o0 < total; o0 += gridDim.x * chunk) {
+#pragma unroll
+        for (int u = 0; u < PACK3_UNROLL; ++u) {
+            const int32_t o = o0 + u * PACK3_THREADS;
+            if (o >= total) break;
+            const int32_t x = o % pnx - 1, r = o / pnx;
+            const int32_t y = r % pny - 1, z = r / pny - 1;
+            const bool in = (unsigned)x < (unsigned)nx && (unsigned)y < (unsigned)ny && (unsigned)z < (unsigned)nz;
+            const int64_t i = in ? ((int64_t)z * ny + y) * nx + x : 0;
+            if constexpr (std::is_same<S, float>::value) {
+                float4 *po = reinterpret_cast<float4 *>(out) + 2 * (int64_t)o;
+                if (in) {
+                    PairNode<float>::pack3(back[i], front[i], po);
+                } else {
+                    po[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    po[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
             } else {
-                po[0] = make_float4(0.f, 0.f, 0.f, 0.f);
-                po[1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                reinterpret_cast<uint4 *>(out)[o] = in ? PairNode<uint16_t>::pack3(back[i], front[i]) : make_uint4(0u, 0u, 0u, 0u);
             }
-        } else {
-            reinterpret_cast<uint4 *>(out)[o] = in ? PairNode<uint16_t>::pack3(back[i], front[i]) : make_uint4(0u, 0u, 0u, 0u);
         }
     }
 }
