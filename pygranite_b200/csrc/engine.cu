@@ -1358,11 +1358,7 @@ int pack_pair(gr_engine *e, int64_t w, cudaStream_t stream) {
     const int threads = 256, blocks = grid_for(e->nodes, threads);
     if (e->dim == 3) {
         const int32_t nx = (int32_t)e->nx, ny = (int32_t)e->ny, nz = (int32_t)e->nz;
-        // beside the step launches (side stream): one block per SM; else the whole buffer at once
-        int sms = 148;
-        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->s.device));
-        const int b3 = stream == e->ps ? sms
-                                       : grid_for(padded_pair_nodes(3, nx, ny, nz) / PACK3_UNROLL, PACK3_THREADS);
+        const int b3 = grid_for(padded_pair_nodes(3, nx, ny, nz) / PACK3_UNROLL, PACK3_THREADS);
         if (elem == 16)
             pair_pack_padded_kernel<float><<<b3, PACK3_THREADS, 0, stream>>>((const float4 *)back, (const float4 *)front,
                                                                              e->pairbuf[b].p, nx, ny, nz);

@@ -112,9 +112,9 @@ static __global__ void pair_pack_edge2_kernel(const typename PairNode<S>::Ring2 
 // of a (nx + 3) x (ny + 3) x (nz + 3) buffer holds the pair of ring nodes (x, y, z), or zeros
 // outside the grid (the step kernel's border addressing).  Every padded node is written, so the
 // buffer needs no clearing.  The padded node count must stay below 2^31.
-// 128-thread blocks of at most 32 registers (4 nodes in flight per thread): one block fits on an
-// SM beside the 3D float32 step kernel's five 96-register blocks, so a pack launched on a side
-// stream with one block per SM runs alongside the step launches instead of taking their slots.
+// 128-thread blocks, 4 nodes in flight per thread.  (Run as one 32-register block per SM beside
+// the step launches, the pack measured slower overall: its stream through L2 displaced the
+// window pair the step kernel gathers from.)
 constexpr int PACK3_THREADS = 128, PACK3_UNROLL = 4;
 template <typename S>
 static __global__ void __launch_bounds__(PACK3_THREADS, 16)
