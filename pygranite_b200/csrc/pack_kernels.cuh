@@ -113,8 +113,8 @@ static __global__ void pair_pack_edge2_kernel(const typename PairNode<S>::Ring2 
 // outside the grid (the step kernel's border addressing).  Every padded node is written, so the
 // buffer needs no clearing.  The padded node count must stay below 2^31.
 // 128-thread blocks, 4 nodes in flight per thread.  (Run as one 32-register block per SM beside
-// the step launches, the pack measured slower overall: its stream through L2 displaced the
-// window pair the step kernel gathers from.)
+// the step launches, the pack measured 1% faster on the 3D benchmark configuration and 3-15%
+// slower on the other 3D configurations, so it covers the whole buffer at once.)
 constexpr int PACK3_THREADS = 128, PACK3_UNROLL = 4;
 template <typename S>
 static __global__ void __launch_bounds__(PACK3_THREADS, 16)
