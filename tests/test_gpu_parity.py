@@ -463,3 +463,52 @@ def test_compiled_expressions_equal_the_interpreter_and_the_oracle(monkeypatch):
         assert np.array_equal(res["volume_info"][0], ref["volume_info"]["temp"]), jit
         for e in range(len(exprs)):
             assert np.array_equal(res["compute_info"][e], ref["compute_info"][e]), (jit, e)
+
+
+def test_deferred_values_with_lifetimes_match_shorter_oracle_runs():
+    """Per-particle lifetimes with deferred volume / expression values, one plain run (the lean
+    kernel, compaction every 2 launches): a particle whose lifetime ends retires with its final
+    values, and its later records repeat its last state.  Set A lives 13 steps (its last step
+    saves record 5), set B the whole run; each equals the float32 oracle run of that set alone
+    with MaximumSimulationTime = lifetime * DeltaT."""
+    from pygranite_b200 import capi
+    base, wind, seeds = problem3d(seed=13)
+    temp = np.random.default_rng(14).standard_normal((12, 20, 24)).astype(np.float32)
+    exprs = ["sqrt(u*u+v*v)*temp", "temp - z*0.5 + x"]
+    settings = dict(base, CurvatureMode=1, AdditionalVolumeMode=1, SaveInterval=3, AdditionalCompute=exprs)
+    n = seeds.shape[0]
+    half = n // 2
+    life_a = 13
+    lifes = np.full(n, int(settings["MaximumSimulationTime"] / settings["DeltaT"]), np.int32)
+    lifes[:half] = life_a
+    eng = capi.Engine(capi.settings_from_reference(settings, ring_slots=len(wind), sort_interval=2))
+    eng.set_seeds(seeds)
+    eng.set_lifetimes(lifes)
+    for k, snap in enumerate(wind):
+        eng.load_windfield(k, snap)
+    eng.load_volume(0, 0, temp)
+    for e, code in enumerate(exprs):
+        eng.compile_expression(e, code, ["temp"], [])
+    eng.run(lambda k: 1 if k < len(wind) else 0)
+    res = eng.results()
+    eng.close()
+    vols = [{"temp": temp}]
+    ref_a = H.run_oracle(dict(settings, MaximumSimulationTime=life_a * settings["DeltaT"]), wind, seeds[:half],
+                         volumes=vols, precision="f32")
+    ref_b = H.run_oracle(settings, wind, seeds[half:], volumes=vols, precision="f32")
+    la = ref_a["trajectories"].shape[1]
+    assert la == 6
+    pos, vol, cmp = res["trajectories"], res["volume_info"][0], res["compute_info"]
+    assert np.array_equal(pos[:half, :la], ref_a["trajectories"])
+    assert np.array_equal(pos[:half, la:], np.repeat(ref_a["trajectories"][:, -1:], pos.shape[1] - la, axis=1))
+    assert np.array_equal(vol[:half, :la - 1], ref_a["volume_info"]["temp"])
+    assert np.array_equal(vol[:half, la - 1:], np.repeat(ref_a["volume_info"]["temp"][:, -1:], vol.shape[1] - la + 1, axis=1))
+    for e in range(len(exprs)):
+        assert np.array_equal(cmp[e][:half, :la - 1], ref_a["compute_info"][e])
+        assert np.array_equal(cmp[e][:half, la - 1:], np.repeat(ref_a["compute_info"][e][:, -1:], cmp[e].shape[1] - la + 1, axis=1))
+        assert np.array_equal(cmp[e][half:], ref_b["compute_info"][e])
+    assert np.array_equal(pos[half:], ref_b["trajectories"])
+    assert np.array_equal(vol[half:], ref_b["volume_info"]["temp"])
+    assert np.array_equal(res["status"][:half], ref_a["status"]) and np.array_equal(res["status"][half:], ref_b["status"])
+    assert np.array_equal(res["total_curvature"][:half], ref_a["total_curvature"])
+    assert np.array_equal(res["total_curvature"][half:], ref_b["total_curvature"])
