@@ -1446,8 +1446,14 @@ int make_ctx(gr_engine *e, RunPlan &R, RunCtx &r) {
     // deferred volume / expression values: not in graph runs (fixed launch shapes) and only
     // where a lean variant applies
     r.defer = !R.graph && r.P.vlast != nullptr && (kernel_features(r.P, e->use_pair, true) & FT_DEFER) != 0;
-    if (r.defer && e->nexpr > 0 && !e->jit_extras)
-        e->jit_extras = jit_deferred_kernel(e->progs, e->nexpr, e->dim, e->jit_why);
+    // resolved per run (a cache lookup after the first compile): expressions and settings may
+    // change between runs
+    e->jit_extras = nullptr;
+    if (r.defer && e->nexpr > 0)
+        e->jit_extras = jit_deferred_kernel(e->progs,
+                                            JitOptions{r.P.nvol, r.P.nexpr, r.P.ncon, r.P.volume_mode, r.P.constants_mode,
+                                                       r.P.curvature_mode, r.P.dyn_any},
+                                            e->dim, e->jit_why);
     r.fn = pick_kernel(e, r.P, r.defer);
     r.threads = block_size_for(e);
     // some step kernels are built for smaller blocks (their launch bounds)

@@ -655,6 +655,15 @@ __device__ __forceinline__ float eval_program(const Code &code, int e, const flo
 __device__ __forceinline__ float GlobalCode::eval(int e, const float (&ref)[19]) const { return eval_program(*this, e, ref); }
 __device__ __forceinline__ float ParamCode::eval(int e, const float (&ref)[19]) const { return eval_program(*this, e, ref); }
 
+// The run's volume / expression options as the code below reads them: the KParams fields, or
+// compile-time constants in the run-time compiled deferred kernel (jit.cu defines
+// GR_JIT_OPTIONS and GR_JIT_<field>), where the loops and branches a run does not use drop out.
+#ifdef GR_JIT_OPTIONS
+#define GR_OPT(P, name) (GR_JIT_##name)
+#else
+#define GR_OPT(P, name) ((P).name)
+#endif
+
 // Volume samples and expression values of a particle, evaluated from the inputs of its last
 // alive step: position p (that step's new position), stage-averaged velocity vc, curvature cv
 // and the step's time weight / ring slots (tpp:363-447).  The kernel calls this only when the
@@ -664,9 +673,9 @@ template <int DIM, typename Code>
 __device__ __forceinline__ void eval_extras(const KParams &P, const Code &code, const StepEntry &E, int64_t pid,
                                             const V3 &p, const V3 &vc, float cv, float (&vol)[GR_MAX_VOL],
                                             float (&cmp)[GR_MAX_EXPR]) {
-    const float t0 = P.dyn_any ? E.t0 : 0.f;
-    if (P.volume_mode != 0 && P.nvol > 0) {
-        const int vb = P.volume_mode == 2 ? E.slot_back : 0, vf = P.volume_mode == 2 ? E.slot_front : 0;
+    const float t0 = GR_OPT(P, dyn_any) ? E.t0 : 0.f;
+    if (GR_OPT(P, volume_mode) != 0 && GR_OPT(P, nvol) > 0) {
+        const int vb = GR_OPT(P, volume_mode) == 2 ? E.slot_back : 0, vf = GR_OPT(P, volume_mode) == 2 ? E.slot_front : 0;
         const float ax = (p.x - P.off[0]) * P.inv_scale[0];
         const float ay = (p.y - P.off[1]) * P.inv_scale[1];
         if (DIM == 3) {
@@ -674,9 +683,9 @@ __device__ __forceinline__ void eval_extras(const KParams &P, const Code &code, 
             const Cell3 c = make_cell3(P, ax, ay, az);
 #pragma unroll
             for (int k = 0; k < GR_MAX_VOL; ++k) {
-                if (k < P.nvol) {
+                if (k < GR_OPT(P, nvol)) {
                     const float b = tri1(P.vol + ((int64_t)vb * GR_MAX_VOL + k) * P.vol_plane, c);
-                    vol[k] = P.volume_mode == 2 ? lerp_(b, tri1(P.vol + ((int64_t)vf * GR_MAX_VOL + k) * P.vol_plane, c), t0)
+                    vol[k] = GR_OPT(P, volume_mode) == 2 ? lerp_(b, tri1(P.vol + ((int64_t)vf * GR_MAX_VOL + k) * P.vol_plane, c), t0)
                                                 : b;
                 }
             }
@@ -684,27 +693,27 @@ __device__ __forceinline__ void eval_extras(const KParams &P, const Code &code, 
             const Cell2 c = make_cell2(P.nx, P.ny, P.filter_weights, ax, ay);
 #pragma unroll
             for (int k = 0; k < GR_MAX_VOL; ++k) {
-                if (k < P.nvol) {
+                if (k < GR_OPT(P, nvol)) {
                     const float b = bil1(P.vol + ((int64_t)vb * GR_MAX_VOL + k) * P.vol_plane, c);
-                    vol[k] = P.volume_mode == 2 ? lerp_(b, bil1(P.vol + ((int64_t)vf * GR_MAX_VOL + k) * P.vol_plane, c), t0)
+                    vol[k] = GR_OPT(P, volume_mode) == 2 ? lerp_(b, bil1(P.vol + ((int64_t)vf * GR_MAX_VOL + k) * P.vol_plane, c), t0)
                                                 : b;
                 }
             }
         }
     }
-    if (P.nexpr > 0) {
+    if (GR_OPT(P, nexpr) > 0) {
         float ref[19];
         ref[0] = p.x; ref[1] = p.y; ref[2] = DIM == 3 ? p.z : 0.f;
-        ref[3] = P.curvature_mode == 3 ? cv : 0.f;
+        ref[3] = GR_OPT(P, curvature_mode) == 3 ? cv : 0.f;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) ref[4 + k] = k < P.nvol ? vol[k] : 0.f;
+        for (int k = 0; k < 8; ++k) ref[4 + k] = k < GR_OPT(P, nvol) ? vol[k] : 0.f;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             float c = 0.f;
-            if (k < P.ncon && P.constants_mode != 0) {
-                const int cb = P.constants_mode == 2 ? E.slot_back : 0;
+            if (k < GR_OPT(P, ncon) && GR_OPT(P, constants_mode) != 0) {
+                const int cb = GR_OPT(P, constants_mode) == 2 ? E.slot_back : 0;
                 const float b = __ldg(P.cons + ((int64_t)cb * GR_MAX_CON + k) * P.n_total + pid);
-                if (P.constants_mode == 2) {
+                if (GR_OPT(P, constants_mode) == 2) {
                     const float f = __ldg(P.cons + ((int64_t)E.slot_front * GR_MAX_CON + k) * P.n_total + pid);
                     c = lerp_(b, f, t0);
                 } else {
@@ -716,7 +725,7 @@ __device__ __forceinline__ void eval_extras(const KParams &P, const Code &code, 
         ref[16] = vc.x; ref[17] = vc.y; ref[18] = DIM == 3 ? vc.z : 0.f;
 #pragma unroll
         for (int e = 0; e < GR_MAX_EXPR; ++e)
-            if (e < P.nexpr) cmp[e] = code.eval(e, ref);
+            if (e < GR_OPT(P, nexpr)) cmp[e] = code.eval(e, ref);
     }
 }
 
@@ -725,21 +734,21 @@ __device__ __forceinline__ void eval_extras(const KParams &P, const Code &code, 
 // volumes when no volume is sampled (their stored values enter the expressions).
 __device__ __forceinline__ void load_extras(const KParams &P, int64_t i, bool evaluating, float (&vol)[GR_MAX_VOL],
                                             float (&cmp)[GR_MAX_EXPR]) {
-    const bool vols = !evaluating || P.volume_mode == 0;
+    const bool vols = !evaluating || GR_OPT(P, volume_mode) == 0;
 #pragma unroll
-    for (int k = 0; k < GR_MAX_VOL; ++k) vol[k] = (k < P.nvol && vols) ? P.volc[k * P.n_state + i] : 0.f;
+    for (int k = 0; k < GR_MAX_VOL; ++k) vol[k] = (k < GR_OPT(P, nvol) && vols) ? P.volc[k * P.n_state + i] : 0.f;
 #pragma unroll
-    for (int k = 0; k < GR_MAX_EXPR; ++k) cmp[k] = (k < P.nexpr && !evaluating) ? P.cmpc[k * P.n_state + i] : 0.f;
+    for (int k = 0; k < GR_MAX_EXPR; ++k) cmp[k] = (k < GR_OPT(P, nexpr) && !evaluating) ? P.cmpc[k * P.n_state + i] : 0.f;
 }
 
 __device__ __forceinline__ void store_extras(const KParams &P, int64_t i, const float (&vol)[GR_MAX_VOL],
                                              const float (&cmp)[GR_MAX_EXPR]) {
 #pragma unroll
     for (int k = 0; k < GR_MAX_VOL; ++k)
-        if (k < P.nvol) P.volc[k * P.n_state + i] = vol[k];
+        if (k < GR_OPT(P, nvol)) P.volc[k * P.n_state + i] = vol[k];
 #pragma unroll
     for (int k = 0; k < GR_MAX_EXPR; ++k)
-        if (k < P.nexpr) P.cmpc[k * P.n_state + i] = cmp[k];
+        if (k < GR_OPT(P, nexpr)) P.cmpc[k * P.n_state + i] = cmp[k];
 }
 
 // ------------------------------------------------------------------ the step kernel
@@ -757,14 +766,14 @@ __device__ __forceinline__ void extras_at(const KParams &P, const Code &code, in
         store_extras(P, i, vol, cmp);
     }
     if (irec < 0) return;
-    if (P.volume_mode != 0) {
+    if (GR_OPT(P, volume_mode) != 0) {
 #pragma unroll
         for (int k = 0; k < GR_MAX_VOL; ++k)
-            if (k < P.nvol) P.hvol[((int64_t)k * P.Li + irec) * P.n_total + pid] = vol[k];
+            if (k < GR_OPT(P, nvol)) P.hvol[((int64_t)k * P.Li + irec) * P.n_total + pid] = vol[k];
     }
 #pragma unroll
     for (int e = 0; e < GR_MAX_EXPR; ++e)
-        if (e < P.nexpr) P.hcmp[((int64_t)e * P.Li + irec) * P.n_total + pid] = cmp[e];
+        if (e < GR_OPT(P, nexpr)) P.hcmp[((int64_t)e * P.Li + irec) * P.n_total + pid] = cmp[e];
 }
 
 // extras_at for the step kernel's in-kernel evaluation (FT_EXTRAS).  Not inlined: it runs once
@@ -793,7 +802,7 @@ __device__ __forceinline__ void deferred_extras(const KParams &P, const Code &co
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         if (rec >= 0) {
             const int64_t pid = P.id[i];
-            const float cv = P.curvature_mode == 3 ? P.curv[i] : 0.f;
+            const float cv = GR_OPT(P, curvature_mode) == 3 ? P.curv[i] : 0.f;
             const float4 a = P.vrec[2 * i], v = P.vrec[2 * i + 1];
             const int32_t last_s = __float_as_int(v.w);
             extras_at<DIM>(P, code, i, pid, last_s >= 0, last_s < 0 ? 0 : last_s, V3{a.x, a.y, a.z},
@@ -804,7 +813,7 @@ __device__ __forceinline__ void deferred_extras(const KParams &P, const Code &co
             const int32_t last_s = __float_as_int(v.w);
             if (last_s < 0) continue;
             const int64_t pid = P.id[i];
-            const float cv = P.curvature_mode == 3 ? P.curv[i] : 0.f;
+            const float cv = GR_OPT(P, curvature_mode) == 3 ? P.curv[i] : 0.f;
             const V3 p{P.px[i], P.py[i], DIM == 3 ? P.pz[i] : 0.f};
             extras_at<DIM>(P, code, i, pid, true, last_s, p, V3{v.x, v.y, v.z}, cv, -1);
             reinterpret_cast<int32_t *>(P.vlast + i)[3] = -1;

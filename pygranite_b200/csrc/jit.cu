@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <utility>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -175,8 +176,13 @@ std::map<std::string, Cached> g_cache;
 
 }  // namespace
 
-std::string jit_source(const Program *progs, int nexpr, int dim) {
-    std::string src;
+std::string jit_source(const Program *progs, const JitOptions &o, int dim) {
+    const int nexpr = o.nexpr;
+    std::string src = "#define GR_JIT_OPTIONS 1\n";
+    const std::pair<const char *, int> opts[] = {{"nvol", o.nvol}, {"nexpr", o.nexpr}, {"ncon", o.ncon},
+                                                 {"volume_mode", o.volume_mode}, {"constants_mode", o.constants_mode},
+                                                 {"curvature_mode", o.curvature_mode}, {"dyn_any", o.dyn_any}};
+    for (const auto &kv : opts) src += "#define GR_JIT_" + std::string(kv.first) + " " + std::to_string(kv.second) + "\n";
     src += "#include \"granite_kernels.cuh\"\nnamespace granite_b200 {\nstruct JitCode {\n";
     src += "    __device__ __forceinline__ float eval(int e, const float (&ref)[19]) const {\n";
     for (int e = 0; e < nexpr; ++e) {
@@ -192,13 +198,13 @@ std::string jit_source(const Program *progs, int nexpr, int dim) {
     return src;
 }
 
-cudaKernel_t jit_deferred_kernel(const Program *progs, int nexpr, int dim, std::string &why) {
+cudaKernel_t jit_deferred_kernel(const Program *progs, const JitOptions &o, int dim, std::string &why) {
     const char *env = std::getenv("GR_JIT");
     if (env && env[0] == '0') {
         why = "GR_JIT=0";
         return nullptr;
     }
-    const std::string src = jit_source(progs, nexpr, dim);
+    const std::string src = jit_source(progs, o, dim);
     if (src.empty()) {
         why = "expression code not translatable";
         return nullptr;
