@@ -1449,7 +1449,7 @@ int make_ctx(gr_engine *e, RunPlan &R, RunCtx &r) {
     // resolved per run (a cache lookup after the first compile): expressions and settings may
     // change between runs
     e->jit_extras = nullptr;
-    if (r.defer && e->nexpr > 0)
+    if (r.defer)
         e->jit_extras = jit_deferred_kernel(e->progs,
                                             JitOptions{r.P.nvol, r.P.nexpr, r.P.ncon, r.P.volume_mode, r.P.constants_mode,
                                                        r.P.curvature_mode, r.P.dyn_any},
