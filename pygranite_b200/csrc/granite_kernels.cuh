@@ -1148,8 +1148,7 @@ __device__ __forceinline__ void advance_particle(const KParams &P, const int64_t
 // 48 cached floats in 128-thread blocks: 4 per SM (128 registers) in the generic variant and the
 // lean ones with volume / expression values or with both Kahan positions and curvature, 5 per SM
 // (96 registers, 20 warps) in the other lean ones, whose state fits there without spills; the
-// extra warps hide more of the sampling and curvature latency.  The 16-bit kernels keep 256 x 2
-// (measured faster than 128 x 5 there).
+// extra warps hide more of the sampling and curvature latency.  The 16-bit kernels: AdvBounds16.
 template <int DIM, typename W, int FT> struct AdvBounds { static constexpr int threads = 256, blocks = GR_ADV_MIN_BLOCKS; };
 #ifndef GR_F32_PAIR_BLOCKS
 #define GR_F32_PAIR_BLOCKS 4
@@ -1157,6 +1156,17 @@ template <int DIM, typename W, int FT> struct AdvBounds { static constexpr int t
 #ifndef GR_F32_LIGHT_BLOCKS
 #define GR_F32_LIGHT_BLOCKS 5
 #endif
+// 16-bit 3D pair kernels: 128 x 5 for the lean variants with curvature or deferred values
+// (measured 5-6% faster than 256 x 2 on the 3D benchmark configuration), 256 x 2 for the rest
+// (the positions-only variant of the batching and serving forms measured 2% slower at 128 x 5).
+template <typename H, int FT> struct AdvBounds16 {
+    static constexpr bool light = (FT & FT_LEAN) != 0 && (FT & FT_EXTRAS) == 0 &&
+                                  (FT & (FT_COMP | FT_CURV)) != (FT_COMP | FT_CURV) &&
+                                  (FT & (FT_CURV | FT_DEFER)) != 0;
+    static constexpr int threads = light ? 128 : 256, blocks = light ? GR_F32_LIGHT_BLOCKS : GR_ADV_MIN_BLOCKS;
+};
+template <int FT> struct AdvBounds<3, Pair<__nv_bfloat16>, FT> : AdvBounds16<__nv_bfloat16, FT> {};
+template <int FT> struct AdvBounds<3, Pair<__half>, FT> : AdvBounds16<__half, FT> {};
 template <int FT> struct AdvBounds<3, Pair<float>, FT> {
     static constexpr bool light = (FT & FT_LEAN) != 0 && (FT & FT_EXTRAS) == 0 &&
                                   (FT & (FT_COMP | FT_CURV)) != (FT_COMP | FT_CURV);
