@@ -52,7 +52,7 @@ def parse():
     p.add_argument("--sim-steps", type=int, default=2000)
     p.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
     p.add_argument("--steps-per-launch", type=int, default=0)
-    p.add_argument("--sort-interval", type=int, default=4,
+    p.add_argument("--sort-interval", type=int, default=8,
                    help="launches between compaction / Morton re-sorts of the live particles (0 = off)")
     p.add_argument("--layout", type=int, default=0, help="0: window-pair wind layout, 1: ring slots")
     p.add_argument("--e2e-steps", type=int, default=5)

@@ -70,7 +70,8 @@ typedef struct gr_settings {
     int32_t compensated;           /* 1: Kahan-compensated float32 position update */
     int32_t ring_slots;            /* device ring depth (>= 3); 0 = 3 */
     int32_t steps_per_launch;      /* steps fused into one launch; 0 = one snapshot window */
-    int32_t sort_interval;         /* launches between Morton re-sorts / compactions; 0 = off */
+    int32_t sort_interval;         /* launches between Morton re-sorts / compactions; 0 = off; negative
+                                    * (the default): every 8 launches from 65,536 particles, else off */
     int32_t block_size;            /* threads per block; 0 = autotuned default; capped at the step
                                       kernel's launch bound (128 for the float32 3D window-pair
                                       kernel, 256 for the others) */

@@ -512,6 +512,13 @@ int ensure_particles(gr_engine *e) {
 
 extern "C" {
 
+// Automatic compaction (sort_interval < 0): a Morton re-sort every 8 launches measured best on
+// the 3D benchmark configuration (1e6 particles: 2.05e10 against 1.99e10 every 4 and 2.03e10
+// every 12); below 65,536 particles the passes cost more than the sorted warps save (the 2D
+// double gyre, 10,000 particles: 1.74e10 with them, 1.95e10 without).
+constexpr int kAutoSortInterval = 8;
+constexpr int64_t kAutoSortMin = 65536;
+
 void gr_settings_default(gr_settings *s) {
     std::memset(s, 0, sizeof *s);
     s->space = 0;
@@ -524,6 +531,7 @@ void gr_settings_default(gr_settings *s) {
     s->offset_len = 3;
     s->save_interval = 1;
     s->maximum_simulation_time = 100.f;
+    s->sort_interval = -1;  // automatic: kAutoSortInterval launches from kAutoSortMin particles, else off
 }
 
 const char *gr_last_error(void) { return g_last_error.c_str(); }
@@ -871,7 +879,7 @@ int alloc_state(gr_engine *e) {
     if (rc) return rc;
     if (e->st[0].vlast.p) CK(e->vrec.alloc(2 * N));
     CK(e->out_status.alloc(N)); CK(e->out_length.alloc(N)); CK(e->out_tc.alloc(N));
-    e->compacting = e->s.sort_interval > 0;
+    e->compacting = e->s.sort_interval > 0 || (e->s.sort_interval < 0 && e->n >= kAutoSortMin);
     CK(e->d_counts.alloc(4));
     if (!e->compacting) return GR_OK;
     rc = alloc_set(e, e->st[1], false);
@@ -1553,7 +1561,7 @@ int after_launch(RunCtx &r, int64_t k_end) {
     gr_engine *e = r.e;
     const RunPlan &R = *r.R;
     if (!e->compacting || k_end >= R.nsteps) return 0;
-    if (++r.since_sort < e->s.sort_interval) return 0;
+    if (++r.since_sort < (e->s.sort_interval > 0 ? e->s.sort_interval : kAutoSortInterval)) return 0;
     r.since_sort = 0;
     if (r.defer) {   // retiring particles take their final values along
         const int q = launch_deferred_extras(r, -1, k_end, false);

@@ -74,7 +74,7 @@ struct IntegratorSettings {
     bool CompensatedPositions{false};
     int32_t RingSlots{0};
     int32_t StepsPerLaunch{0};
-    int32_t SortInterval{0};
+    int32_t SortInterval{-1};
     int32_t BlockSize{0};
     int32_t Device{0};
     int32_t WindLayout{0};
