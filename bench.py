@@ -614,8 +614,7 @@ def run_precision(args, world, rank, local, pg_dist):
              "f16": dict(storage=2, compensated=1, time_mode=1)}
     out, hist = {}, {}
     for name, opt in forms.items():
-        e = capi.Engine(capi.settings_from_reference(settings, ring_slots=n_snap, device=local, sort_interval=4,
-                                                     **opt))
+        e = capi.Engine(capi.settings_from_reference(settings, ring_slots=n_snap, device=local, **opt))
         e.set_seeds(seeds)
         for k in range(n_snap):
             fld.load(e, k)
